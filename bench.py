@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the MLS-MPM step (particle-steps/s) on B200.
+
+Default workload: the two-material drop (128^3 grid, 2,097,152 particles:
+neo-Hookean block + EOS fluid column, slip walls, dt 5e-5), seeded synthetic
+inputs.  One bench "step" = one MPM time step of all particles.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload cfg2|cfg1|cfg3|cfg4|cfg3_adjoint]
+
+Our arm prints ONE JSON line: value = whole-job particle-steps/s with state
+resident in HBM (device time, CUDA events, max over ranks), e2e = the same
+metric through the host-buffer C-ABI call pgmpm_advance_host (pinned host
+memory in and out, copies inside the timed region), roofline of the dominant
+kernel from live per-kernel CUDA events, and the reference's own CPU solver
+timed on the host cores as cpu_baseline.  N > 1 runs independent replicas
+(weak scaling; the MPM step of one scene does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return PEAK_FALLBACK_GBS, "fallback"
+
+
+# ----------------------------------------------------------------- workloads
+def make_workload(name):
+    from physgrad_b200 import workloads as W
+
+    if name == "cfg1":
+        return W.config1()
+    if name == "cfg3" or name == "cfg3_adjoint":
+        return W.config3()
+    if name == "cfg4":
+        return W.config4()
+    if name == "cfg5":
+        return W.config5()
+    return W.config2()
+
+
+def algorithmic_bytes(N, A, multi_mat):
+    """Algorithmic HBM bytes per launch (FP32): P2G 100 B/particle (+4 for a
+    material id) + 16 B/active node; G2P 144 B/particle + 12 B/node; grid
+    update 28 B/node."""
+    return {"p2g": (100 + (4 if multi_mat else 0)) * N + 16 * A, "g2p": 144 * N + 12 * A, "grid": 28 * A}
+
+
+def kernel_launches_per_step(scenes):
+    """Our kernels per step: 3 per radix-sort pass (histogram, scan,
+    scatter) + mark + P2G + grid update + G2P."""
+    cells = sum(((int(s.n[0]) - 3) // 4 + 1) * ((int(s.n[1]) - 3) // 4 + 1) * ((int(s.n[2]) - 3) // 4 + 1)
+                for s in scenes) * 64
+    bits = max(1, int(np.ceil(np.log2(max(2, cells)))))
+    passes = (bits + 7) // 8
+    return 3 * passes + 4
+
+
+# -------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------- reference CPU timing
+def reference_cpu_rate(st, scene, steps_per_thread, warmup=1, threads=None, sample_div=8):
+    """The reference's own CPU solver (physgrad::mpm::MPMSolver<float,64>,
+    single-threaded by design) on `threads` host threads, each an
+    independent instance on a 1/sample_div particle sample of the workload on
+    the full grid.  Returns (particle-steps/s, threads, description)."""
+    import ctypes
+
+    from oracle import pyoracle as O
+
+    R = O.ref_lib()
+    vp = ctypes.c_void_p
+    R.ref_mpm_create.restype = vp
+    R.ref_mpm_create.argtypes = [ctypes.c_int64, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+    R.ref_mpm_step.argtypes = [vp, ctypes.c_int]
+    R.ref_mpm_destroy.argtypes = [vp]
+    T = threads or min(os.cpu_count() or 1, 32)
+    N = st["x"].shape[0]
+    handles, keep = [], []
+    for t in range(T):
+        idx = np.arange(t % sample_div, N, sample_div)
+        x = np.ascontiguousarray(st["x"][idx], np.float32)
+        v = np.ascontiguousarray(st["v"][idx], np.float32)
+        m = np.ascontiguousarray(st["m"][idx], np.float32)
+        V0 = np.ascontiguousarray(st["V0"][idx], np.float32)
+        keep.append((x, v, m, V0))
+        h = R.ref_mpm_create(len(idx), x.ctypes.data, v.ctypes.data, m.ctypes.data, V0.ctypes.data,
+                             int(scene.n[0]), int(scene.n[1]), int(scene.n[2]), float(scene.dx), float(scene.dt),
+                             float(scene.gravity[0]), float(scene.gravity[1]), float(scene.gravity[2]))
+        if not h:
+            raise RuntimeError("ref_mpm_create failed")
+        handles.append(h)
+    ns = len(np.arange(0, N, sample_div))
+
+    def run(h, k):
+        R.ref_mpm_step(h, k)
+
+    def par(k):
+        ths = [threading.Thread(target=run, args=(h, k)) for h in handles]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        return time.perf_counter() - t0
+
+    if warmup:
+        par(warmup)
+    dt = par(steps_per_thread)
+    for h in handles:
+        R.ref_mpm_destroy(h)
+    rate = T * ns * steps_per_thread / dt
+    desc = (f"{T} independent reference MPMSolver<float,64> instances (single-threaded each), "
+            f"{ns} particles each (1/{sample_div} of the workload's particles) on the full "
+            f"{scene.n[0]}^3 grid, {steps_per_thread} steps each, wall {dt:.2f} s")
+    return rate, T, desc
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, device):
+    import torch
+
+    import physgrad_b200 as pg
+    from physgrad_b200 import _capi as C
+
+    torch.cuda.set_device(device)
+    scenes, counts, mats, st, meta = make_workload(args.workload)
+    N = int(sum(counts))
+    sim = pg.Simulator(scenes, counts, mats, device=device)
+    Cm = st["C"].reshape(N, 9)
+    Fm = st["F"].reshape(N, 9)
+    sim.upload(st["x"], st["v"], Cm, Fm, st["m"], st["V0"], st["mat"])
+    if args.autotune:
+        sim.autotune(reps=3)
+        sim.upload(st["x"], st["v"], Cm, Fm, st["m"], st["V0"], st["mat"])
+    stream = torch.cuda.current_stream()
+    # warm-up (also builds the CUDA graph)
+    sim.step(args.warmup, stream=stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        sim.step(args.steps, stream=stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    flags = sim.status()
+    clocks = clk.summary()
+    # per-kernel device times: eager launches bracketed by events on the launching stream
+    sim.set_profiling(True)
+    prof_steps = max(5, min(args.steps, 50))
+    sums = {"sort": 0.0, "p2g": 0.0, "grid": 0.0, "g2p": 0.0}
+    for _ in range(prof_steps):
+        sim.step(1, stream=stream)
+        m = sim.metrics()
+        sums["sort"] += m["sort_ms"]
+        sums["p2g"] += m["p2g_ms"]
+        sums["grid"] += m["grid_ms"]
+        sums["g2p"] += m["g2p_ms"]
+    sim.set_profiling(False)
+    sim.status()
+    A = sim.metrics()["active_nodes"]
+    kern_ms = {k: v / prof_steps for k, v in sums.items()}
+    multi = len(mats) > 1
+    alg = algorithmic_bytes(N, A, multi)
+    hbm, peak_kind = peaks()
+    kernels = {}
+    for k in ("p2g", "g2p", "grid"):
+        gbs = alg[k] / (kern_ms[k] * 1e-3) / 1e9
+        kernels[k] = {"ms": round(kern_ms[k], 5), "alg_bytes": alg[k], "achieved_gbs": round(gbs, 1),
+                      "frac": round(gbs / hbm, 4)}
+    kernels["sort"] = {"ms": round(kern_ms["sort"], 5)}
+    dom = max(("p2g", "g2p"), key=lambda k: kern_ms[k])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        traffic = tj.get(args.workload, {}).get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": kernels[dom]["achieved_gbs"], "peak": hbm,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": kernels[dom]["frac"], "traffic": traffic}
+    value = world * N * args.steps / (ms * 1e-3)
+    launches_per_step = kernel_launches_per_step(scenes)
+
+    # e2e: host-buffer C-ABI call (pinned memory in/out), S steps per call
+    S = min(args.steps, 100)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hx, hv, hC, hF = pin(st["x"]), pin(st["v"]), pin(Cm), pin(Fm)
+    hm, hV = pin(st["m"]), pin(st["V0"])
+    hmat = pin(st["mat"]) if st["mat"] is not None else None
+    ox, ov, oC, oF = (pin(np.empty_like(a)) for a in (hx, hv, hC, hF))
+    L = pg.lib()
+    import ctypes
+
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    e2e_times = []
+    for it in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        C.check(L.pgmpm_advance_host(sim.handle, hx.ctypes.data, hv.ctypes.data, hC.ctypes.data, hF.ctypes.data,
+                                     hm.ctypes.data, hV.ctypes.data, hmat.ctypes.data if hmat is not None else None,
+                                     S, ox.ctypes.data, ov.ctypes.data, oC.ctypes.data, oF.ctypes.data, sh))
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_t = statistics.median(e2e_times[1:])
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_t], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    h2d = sum(a.nbytes for a in (hx, hv, hC, hF, hm, hV)) + (hmat.nbytes if hmat is not None else 0)
+    d2h = sum(a.nbytes for a in (ox, ov, oC, oF))
+    e2e = {"value": world * N * S / e2e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / S,
+           "d2h_bytes_per_step": d2h / S, "steps_per_call": S,
+           "call": "pgmpm_advance_host: state in from pinned host, S steps, state out to pinned host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+
+        if O.ref_available():
+            rate, T, desc = reference_cpu_rate(st, scenes[0], steps_per_thread=3)
+            cpu = {"value": rate, "unit": "particle-steps/s", "cores": T, "kind": "reference",
+                   "sample": desc + "; physics = the reference CPU path (PIC, gravity, no stress)"}
+    cfg = {"workload": meta.get("workload", args.workload), "n_particles": N, "n_scenes": len(scenes),
+           "grid": [int(s.n[0]) for s in scenes][:8], "dt": float(scenes[0].dt), "physics": "MLS",
+           "materials": meta.get("materials", "fixed-corotated"),
+           "l2": f"inputs larger than L2: particle state {N * 104 / 1e6:.0f} MB + grid",
+           "parallelism": "replicas" if world > 1 else "single",
+           "tuning": {k: sim.metrics()[k] for k in ("p2g_block", "p2g_ppt", "g2p_block", "graph_enabled")},
+           "active_nodes": A}
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform positions of the configuration's shapes)", "config": cfg,
+            "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "device_flags": flags}
+    sim.close()
+    return line
+
+
+def run_reference(args):
+    """Reference arm: the reference's own CPU MPM path on the host cores."""
+    from oracle import pyoracle as O
+
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_mpm.so not built (needs the reference tree)"}
+    scenes, counts, mats, st, meta = make_workload(args.workload)
+    N = int(sum(counts))
+    rate_w, T, desc = None, None, None
+    rate, T, desc = reference_cpu_rate(st, scenes[0], steps_per_thread=args.steps, warmup=args.warmup)
+    line = {"impl": "reference", "metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform, same workload)",
+            "config": {"workload": meta.get("workload", args.workload), "n_particles": N,
+                       "physics": "reference CPU path (PIC, gravity)"},
+            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": T, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint"])
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    try:
+        line = run_ours(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,230 @@
+/*
+ * pgmpm.h -- C-ABI of the B200-native MLS-MPM step (libpgmpm.so).
+ *
+ * Plain C: pointers, sizes and an int status.  No torch or C++ types cross
+ * this boundary.  Every entry point returns PGMPM_OK (0) or a negative
+ * PGMPM_ERR_* code; pgmpm_last_error() gives the message of the last failure
+ * on the calling thread.  A solver handle is not thread-safe: use one handle
+ * per host thread.  Streams are explicit (cudaStream_t passed as void*; NULL
+ * is the legacy default stream).
+ *
+ * What each entry point replaces in pedroscortes/physgrad (file:line):
+ *   pgmpm_create / pgmpm_destroy
+ *       physgrad::mpm::MPMSolver<T>(MPMSolverConfig) + initialize() +
+ *       ~MPMSolver()/cleanup()            src/mpm_solver.h:156-187, 506-532
+ *       MPMSolver<T,64>(int3, cell, origin, SimulationParams)
+ *                                         src/material_point_method.h:450-453
+ *       DifferentiableMPMSystem::initializeSystem
+ *                                         src/differentiable_mpm.h:711-728
+ *   pgmpm_upload
+ *       MPMSolver<T>::addParticles        src/mpm_solver.h:190-226
+ *       MPMSolver<T,64>::addParticles     src/material_point_method.h:455-477
+ *   pgmpm_step
+ *       MPMSolver<T>::step / run          src/mpm_solver.h:229-329
+ *       MPMSolver<T,64>::step             src/material_point_method.h:479-500
+ *       G2P2GKernelLauncher::launchG2P2G  src/mpm_g2p2g_kernels.h:494-515
+ *   pgmpm_download / pgmpm_download_grid
+ *       getParticles() / getGrid()        src/mpm_solver.h:322-324,
+ *                                         src/material_point_method.h:503-504
+ *   pgmpm_get_metrics
+ *       MPMSolver<T>::getMetrics          src/mpm_solver.h:324 (struct :72-101)
+ *   pgmpm_forward_checkpointed / pgmpm_backward
+ *       DifferentiableMPMSystem::simulationStep / computeGradients /
+ *       getParticleGradients              src/differentiable_mpm.h:748-797
+ *       (CheckpointStrategy::UNIFORM      src/differentiable_mpm.h:66)
+ *   pgmpm_set_tuning / pgmpm_autotune
+ *       MPMSolverConfig::cuda_block_size  src/mpm_solver.h:51 and
+ *       kernels::KernelConfig             src/mpm_g2p2g_kernels.h:68-75
+ *   launch_mpm_timestep_forward
+ *       same name and arguments as        src/pytorch_autograd.cu:371-382
+ *   pgmpm_radix_sort_pairs
+ *       no reference counterpart (the reference does not sort); exported so
+ *       the integer sort can be checked bit for bit on its own.
+ */
+#ifndef PGMPM_H
+#define PGMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGMPM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PGMPM_API __attribute__((visibility("default")))
+#else
+#define PGMPM_API
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define PGMPM_OK 0
+#define PGMPM_ERR_ARG -1         /* invalid argument */
+#define PGMPM_ERR_CUDA -2        /* CUDA runtime error (message in last_error) */
+#define PGMPM_ERR_STATE -3       /* call not valid in the solver's state */
+#define PGMPM_ERR_UNSUPPORTED -4 /* material / physics combination not built */
+#define PGMPM_ERR_OOM -5         /* device allocation failed */
+#define PGMPM_ERR_SIMULATION -6  /* device flagged escape / non-finite state */
+
+/* ---- device status flags (pgmpm_check_status) ------------------------- */
+#define PGMPM_FLAG_ESCAPE 1u      /* a particle left [0.5dx, (n-2.5)dx) (MLS) */
+#define PGMPM_FLAG_NONFINITE 2u   /* non-finite position seen */
+#define PGMPM_FLAG_TILE_RANGE 4u  /* stencil fell outside its tile (internal) */
+#define PGMPM_FLAG_BAD_MATERIAL 8u /* material id outside [0, n_materials): used 0 */
+
+/* ---- enums ------------------------------------------------------------ */
+#define PGMPM_PHYSICS_MLS 0        /* MLS-MPM + APIC + stress + walls */
+#define PGMPM_PHYSICS_REF_COMPAT 1 /* reference CPU path: PIC, floor stencil, gravity */
+
+#define PGMPM_BC_NONE 0
+#define PGMPM_BC_STICKY 1   /* v = 0 on wall nodes */
+#define PGMPM_BC_SLIP 2     /* normal component = 0 on wall nodes */
+#define PGMPM_BC_SEPARATE 3 /* normal component clamped to leave the wall */
+
+/* MaterialType values of src/mpm_data_structures.h:54-61 */
+#define PGMPM_MAT_ELASTIC 0
+#define PGMPM_MAT_ELASTOPLASTIC 1
+#define PGMPM_MAT_FLUID 2
+#define PGMPM_MAT_SAND 3
+#define PGMPM_MAT_SNOW 4
+#define PGMPM_MAT_JELLY 5
+
+#define PGMPM_MODEL_FIXED_COROTATED 0
+#define PGMPM_MODEL_NEO_HOOKEAN 1
+#define PGMPM_MODEL_EOS_FLUID 2
+
+/* pointer location flags for upload / download / backward */
+#define PGMPM_PTR_HOST 0
+#define PGMPM_PTR_DEVICE 1
+
+typedef struct pgmpm_solver_s* pgmpm_solver;
+
+/* One scene: a dense background grid of n[0] x n[1] x n[2] nodes with
+ * spacing dx starting at origin (node (i,j,k) at origin + (i,j,k) dx). */
+typedef struct {
+    int32_t n[3];
+    int32_t physics;            /* PGMPM_PHYSICS_* */
+    int32_t boundary;           /* PGMPM_BC_* (MLS only; REF_COMPAT has none) */
+    int32_t boundary_thickness; /* wall thickness in nodes */
+    float dx;
+    float origin[3];
+    float dt;
+    float gravity[3];
+} pgmpm_scene_desc;
+
+/* Material (src/mpm_data_structures.h:63-75 MaterialParameters subset). */
+typedef struct {
+    int32_t type;          /* PGMPM_MAT_ELASTIC, PGMPM_MAT_JELLY or PGMPM_MAT_FLUID */
+    int32_t model;         /* PGMPM_MODEL_*; FLUID requires EOS_FLUID */
+    float youngs_modulus;  /* E; the bulk modulus K for FLUID (reference convention) */
+    float poisson_ratio;
+    float density;
+} pgmpm_material;
+
+typedef struct {
+    int64_t total_steps;
+    int64_t num_particles;
+    int64_t active_nodes;      /* grid nodes with mass > 0 in the last step */
+    double last_step_ms;       /* device time of the last timed step (events) */
+    double average_step_ms;
+    double particle_steps_per_s;
+    double sort_ms, p2g_ms, grid_ms, g2p_ms; /* per-kernel device ms, last profiled step */
+    int32_t p2g_block, p2g_ppt, g2p_block, graph_enabled;
+} pgmpm_metrics;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+PGMPM_API const char* pgmpm_last_error(void);
+PGMPM_API int pgmpm_abi_version(void);
+
+/* Create a solver over n_scenes scenes (n_scenes = 1 for a plain solver).
+ * particle_counts[s]: particles of scene s.  materials: table indexed by the
+ * per-particle material id.  device: CUDA ordinal. */
+PGMPM_API int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,
+                 const pgmpm_material* materials, int32_t n_materials, int32_t device, pgmpm_solver* out);
+PGMPM_API int pgmpm_destroy(pgmpm_solver s);
+
+/* Replace the material table (same count), e.g. a new Young's modulus
+ * between optimisation iterations.  Host pointer. */
+PGMPM_API int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t n_materials);
+
+/* Upload particle state, scenes back to back in scene order.
+ * x,v [N][3]; C,F [N][9] row-major (NULL C = 0, NULL F = I); m,V0 [N];
+ * mat [N] (NULL = material 0).  ptr_kind: PGMPM_PTR_HOST / _DEVICE. */
+PGMPM_API int pgmpm_upload(pgmpm_solver s, const float* x, const float* v, const float* C, const float* F,
+                 const float* m, const float* V0, const int32_t* mat, int32_t ptr_kind, void* stream);
+
+/* Download the state in upload order.  Any output pointer may be NULL. */
+PGMPM_API int pgmpm_download(pgmpm_solver s, float* x, float* v, float* C, float* F, int32_t ptr_kind, void* stream);
+
+/* Grid of one scene in the reference layout (index k*nx*ny + j*nx + i):
+ * mass [nodes], velocity [nodes][3] after the last step's grid update. */
+PGMPM_API int pgmpm_download_grid(pgmpm_solver s, int32_t scene, float* mass, float* velocity, int32_t ptr_kind,
+                        void* stream);
+
+/* ---- simulation ------------------------------------------------------------ */
+PGMPM_API int pgmpm_step(pgmpm_solver s, int32_t n_steps, void* stream);
+
+/* One host-buffer call: upload state, advance n_steps, download state.
+ * Pointers are host memory (pinned for full PCIe speed). */
+PGMPM_API int pgmpm_advance_host(pgmpm_solver s, const float* x_in, const float* v_in, const float* C_in,
+                       const float* F_in, const float* m, const float* V0, const int32_t* mat,
+                       int32_t n_steps, float* x_out, float* v_out, float* C_out, float* F_out, void* stream);
+
+/* Device error flags accumulated since the last call (PGMPM_FLAG_*);
+ * synchronises the stream and clears them. */
+PGMPM_API int pgmpm_check_status(pgmpm_solver s, uint32_t* flags, void* stream);
+
+/* ---- tuning ---------------------------------------------------------------- */
+/* p2g_block, g2p_block: threads per block; ppt: particles per P2G chunk.
+ * 0 keeps the current value.  use_graph: capture each step as a CUDA graph. */
+PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p_block, int32_t use_graph);
+/* Time candidate (block, ppt) settings on the solver's own state (restored
+ * afterwards) and keep the fastest. */
+PGMPM_API int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream);
+/* profile != 0: time each kernel group with events on the next steps
+ * (graphs disabled while profiling). */
+PGMPM_API int pgmpm_set_profiling(pgmpm_solver s, int32_t profile);
+PGMPM_API int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out);
+
+/* ---- differentiation (MLS physics) ------------------------------------------ */
+/* Run n_steps from the current state, storing the state every
+ * checkpoint_every steps, so that pgmpm_backward can differentiate them. */
+PGMPM_API int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoint_every, void* stream);
+/* Reverse pass over the last pgmpm_forward_checkpointed call.  g*_out: dL/d
+ * of the final state (upload order, any may be NULL = 0).  g*_in: receives
+ * dL/d of the initial state (any may be NULL).  gE [n_materials]: dL/dE per
+ * material (dL/dK for FLUID); may be NULL. */
+PGMPM_API int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, const float* gC_out,
+                   const float* gF_out, float* gx_in, float* gv_in, float* gC_in, float* gF_in, float* gE,
+                   int32_t ptr_kind, void* stream);
+
+/* ---- inspection ------------------------------------------------------------------ */
+#define PGMPM_ARRAY_USER_INDEX 0   /* physical slot -> upload index */
+#define PGMPM_ARRAY_KEYS 1         /* cell key per physical slot (input of the next sort) */
+#define PGMPM_ARRAY_SORTED_KEYS 2  /* sorted keys of the last step */
+#define PGMPM_ARRAY_SORTED_ORDER 3 /* sorted position -> physical slot, last step */
+/* Copy one u32 array of N entries (see PGMPM_ARRAY_*) for inspection; no
+ * reference counterpart (exposes the integer sort for bit-exact checks). */
+PGMPM_API int pgmpm_get_array(pgmpm_solver s, int32_t which, uint32_t* out, int32_t ptr_kind, void* stream);
+
+/* ---- building blocks ---------------------------------------------------------- */
+/* Stable LSD radix sort of (key, value) pairs by the low key_bits bits of the
+ * key (device pointers; vals_in NULL = 0..n-1).  Bit-identical to a stable
+ * CPU sort. */
+PGMPM_API int pgmpm_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                           uint32_t* vals_out, int64_t n, int32_t key_bits, void* stream);
+
+/* Reference-shaped launcher (src/pytorch_autograd.cu:371-382): one
+ * REF_COMPAT MPM step of num_particles particles on the unit cube with a
+ * grid_resolution^3 grid (dx = 1/grid_resolution).  positions, velocities
+ * [n][3], masses [n], gravity [3] are device pointers; stream is a
+ * cudaStream_t.  Errors are reported through pgmpm_last_error(). */
+PGMPM_API void launch_mpm_timestep_forward(float* positions, float* velocities, const float* masses, int num_particles,
+                                 int grid_resolution, float dt, const float* gravity, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PGMPM_H */

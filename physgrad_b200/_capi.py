@@ -1,0 +1,152 @@
+"""ctypes declarations of the C-ABI in include/pgmpm.h (libpgmpm.so).
+
+The shared library is built in-tree by ``physgrad_b200.build``.  Loading
+fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpgmpm.so")
+
+PGMPM_OK = 0
+PGMPM_ERR_ARG = -1
+PGMPM_ERR_CUDA = -2
+PGMPM_ERR_STATE = -3
+PGMPM_ERR_UNSUPPORTED = -4
+PGMPM_ERR_OOM = -5
+PGMPM_ERR_SIMULATION = -6
+
+FLAG_ESCAPE = 1
+FLAG_NONFINITE = 2
+FLAG_TILE_RANGE = 4
+
+PHYSICS_MLS = 0
+PHYSICS_REF_COMPAT = 1
+
+BC_NONE = 0
+BC_STICKY = 1
+BC_SLIP = 2
+BC_SEPARATE = 3
+
+MAT_ELASTIC = 0
+MAT_ELASTOPLASTIC = 1
+MAT_FLUID = 2
+MAT_SAND = 3
+MAT_SNOW = 4
+MAT_JELLY = 5
+
+MODEL_FIXED_COROTATED = 0
+MODEL_NEO_HOOKEAN = 1
+MODEL_EOS_FLUID = 2
+
+ARRAY_USER_INDEX = 0
+ARRAY_KEYS = 1
+ARRAY_SORTED_KEYS = 2
+ARRAY_SORTED_ORDER = 3
+
+PTR_HOST = 0
+PTR_DEVICE = 1
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32 * 3),
+        ("physics", ctypes.c_int32),
+        ("boundary", ctypes.c_int32),
+        ("boundary_thickness", ctypes.c_int32),
+        ("dx", ctypes.c_float),
+        ("origin", ctypes.c_float * 3),
+        ("dt", ctypes.c_float),
+        ("gravity", ctypes.c_float * 3),
+    ]
+
+
+class Material(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int32),
+        ("model", ctypes.c_int32),
+        ("youngs_modulus", ctypes.c_float),
+        ("poisson_ratio", ctypes.c_float),
+        ("density", ctypes.c_float),
+    ]
+
+
+class Metrics(ctypes.Structure):
+    _fields_ = [
+        ("total_steps", ctypes.c_int64),
+        ("num_particles", ctypes.c_int64),
+        ("active_nodes", ctypes.c_int64),
+        ("last_step_ms", ctypes.c_double),
+        ("average_step_ms", ctypes.c_double),
+        ("particle_steps_per_s", ctypes.c_double),
+        ("sort_ms", ctypes.c_double),
+        ("p2g_ms", ctypes.c_double),
+        ("grid_ms", ctypes.c_double),
+        ("g2p_ms", ctypes.c_double),
+        ("p2g_block", ctypes.c_int32),
+        ("p2g_ppt", ctypes.c_int32),
+        ("g2p_block", ctypes.c_int32),
+        ("graph_enabled", ctypes.c_int32),
+    ]
+
+
+# name -> (restype, argtypes)
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+SIGNATURES = {
+    "pgmpm_last_error": (ctypes.c_char_p, []),
+    "pgmpm_abi_version": (ctypes.c_int, []),
+    "pgmpm_create": (ctypes.c_int, [ctypes.POINTER(SceneDesc), _i32, ctypes.POINTER(_i64), ctypes.POINTER(Material),
+                                    _i32, _i32, ctypes.POINTER(_vp)]),
+    "pgmpm_destroy": (ctypes.c_int, [_vp]),
+    "pgmpm_set_materials": (ctypes.c_int, [_vp, ctypes.POINTER(Material), _i32]),
+    "pgmpm_upload": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "pgmpm_download": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "pgmpm_download_grid": (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
+    "pgmpm_step": (ctypes.c_int, [_vp, _i32, _vp]),
+    "pgmpm_advance_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "pgmpm_check_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint32), _vp]),
+    "pgmpm_set_tuning": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
+    "pgmpm_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
+    "pgmpm_set_profiling": (ctypes.c_int, [_vp, _i32]),
+    "pgmpm_get_metrics": (ctypes.c_int, [_vp, ctypes.POINTER(Metrics)]),
+    "pgmpm_forward_checkpointed": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
+    "pgmpm_backward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "pgmpm_get_array": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
+    "pgmpm_radix_sort_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp]),
+    "launch_mpm_timestep_forward": (None, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp]),
+}
+
+_lib = None
+
+
+class PGMPMError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pgmpm error {code}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Load libpgmpm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m physgrad_b200.build` "
+                               "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != PGMPM_OK:
+        msg = lib().pgmpm_last_error()
+        raise PGMPMError(rc, msg.decode() if msg else "")

@@ -1,0 +1,731 @@
+// pgmpm_capi.cu -- the C-ABI of include/pgmpm.h: solver handle, device
+// memory, step driver (CUDA graph per step), metrics and autotuner.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pgmpm.h"
+#include "pgmpm_internal.h"
+
+using namespace pgmpm;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(expr)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (expr);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(e_ == cudaErrorMemoryAllocation ? PGMPM_ERR_OOM : PGMPM_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #expr, cudaGetErrorString(e_), __FILE__, __LINE__);                             \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t b) {
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    cudaError_t ensure(size_t b) { return bytes >= b ? cudaSuccess : alloc(b); }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+int bits_for(uint64_t v) {
+    int b = 0;
+    while ((1ull << b) < v) ++b;
+    return b < 1 ? 1 : b;
+}
+
+}  // namespace
+
+struct pgmpm_solver_s {
+    int device = 0;
+    int num_sms = 148;
+    int S = 0, M = 0;
+    int64_t N = 0;
+    std::vector<pgmpm_scene_desc> desc;
+    std::vector<SceneDev> scenes;
+    std::vector<pgmpm_material> mats_h;
+    std::vector<int64_t> counts;
+    PhysFlags pf{};
+    int total_ct = 0, total_nt = 0;
+    int key_bits = 1;
+    int sort_which = 0;
+    Tuning tune;
+    bool use_graph = true;
+    bool profiling = false;
+    bool uploaded = false;
+
+    // device buffers
+    DevBuf d_scenes, d_mats, q, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
+    DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, counters, staging;
+    uint32_t* h_counters = nullptr;  // pinned
+
+    // graph
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    cudaGraph_t step_graph = nullptr;
+    cudaEvent_t ev[6] = {};
+
+    // metrics
+    pgmpm_metrics met{};
+
+    // differentiation state (pgmpm_forward_checkpointed / pgmpm_backward)
+    int ck_steps = 0, ck_every = 0;
+    DevBuf ck_states;   // checkpoints: (ceil(steps/every)) x 6N float4
+    DevBuf tape_q, tape_keys, tape_order, tape_grid, adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;
+
+    View view() const {
+        View V;
+        V.N = N;
+        V.S = S;
+        V.M = M;
+        V.scenes = d_scenes.as<SceneDev>();
+        V.mats = d_mats.as<MatDev>();
+        V.q = q.as<float4>();
+        V.mV = mV.as<float2>();
+        V.mat = pf.multi_mat ? mat.as<int32_t>() : nullptr;
+        V.keys = keys.as<uint32_t>();
+        V.skeys = sort_which ? kb.as<uint32_t>() : ka.as<uint32_t>();
+        V.order = sort_which ? vb.as<uint32_t>() : va.as<uint32_t>();
+        V.grid_mp = grid_mp.as<float4>();
+        V.grid_v = grid_v.as<float4>();
+        V.grid_vpre = nullptr;
+        V.tile_flags = tile_flags.as<uint32_t>();
+        V.tile_list = tile_list.as<uint32_t>();
+        V.counters = counters.as<uint32_t>();
+        V.total_ct = total_ct;
+        V.total_nt = total_nt;
+        return V;
+    }
+
+    void drop_graph() {
+        if (step_exec) cudaGraphExecDestroy(step_exec);
+        if (step_graph) cudaGraphDestroy(step_graph);
+        step_exec = nullptr;
+        step_graph = nullptr;
+    }
+
+    ~pgmpm_solver_s() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        drop_graph();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (h_counters) cudaFreeHost(h_counters);
+        cudaSetDevice(prev);
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int material_to_dev(const pgmpm_material& m, MatDev& d) {
+    if (m.type == PGMPM_MAT_FLUID) {
+        if (m.model != PGMPM_MODEL_EOS_FLUID)
+            return fail(PGMPM_ERR_UNSUPPORTED, "FLUID material requires PGMPM_MODEL_EOS_FLUID");
+    } else if (m.type == PGMPM_MAT_ELASTIC || m.type == PGMPM_MAT_JELLY) {
+        if (m.model != PGMPM_MODEL_FIXED_COROTATED && m.model != PGMPM_MODEL_NEO_HOOKEAN)
+            return fail(PGMPM_ERR_UNSUPPORTED, "elastic material requires FIXED_COROTATED or NEO_HOOKEAN");
+    } else {
+        return fail(PGMPM_ERR_UNSUPPORTED, "material type %d (ELASTOPLASTIC/SAND/SNOW) is not built", m.type);
+    }
+    if (!(m.youngs_modulus >= 0.f) || !std::isfinite(m.youngs_modulus))
+        return fail(PGMPM_ERR_ARG, "invalid youngs_modulus");
+    const double E = m.youngs_modulus, nu = m.poisson_ratio;
+    if (m.model != PGMPM_MODEL_EOS_FLUID && !(nu > -1.0 && nu < 0.5))
+        return fail(PGMPM_ERR_ARG, "poisson_ratio must be in (-1, 0.5)");
+    std::memset(&d, 0, sizeof(d));
+    d.model = m.model == PGMPM_MODEL_FIXED_COROTATED ? MODEL_FCR : m.model == PGMPM_MODEL_NEO_HOOKEAN ? MODEL_NH : MODEL_EOS;
+    d.E = (float)E;
+    if (d.model != MODEL_EOS) {
+        d.mu = (float)(E / (2.0 * (1.0 + nu)));
+        d.lam = (float)(E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+        d.dmu_dE = (float)(1.0 / (2.0 * (1.0 + nu)));
+        d.dlam_dE = (float)(nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+    }
+    return PGMPM_OK;
+}
+
+cudaStream_t ST(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int record_step(pgmpm_solver s, cudaStream_t st, bool timed) {
+    View V = s->view();
+    // per-step resets: active tile flags, tile count and active node count
+    CK(cudaMemsetAsync(s->tile_flags.p, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
+    CK(cudaMemsetAsync(s->counters.p, 0, sizeof(uint32_t) * CNT_FLAGS, st));
+    if (timed) CK(cudaEventRecord(s->ev[0], st));
+    int which = 0;
+    CK(radix_sort_pairs(s->keys.as<uint32_t>(), nullptr, s->ka.as<uint32_t>(), s->va.as<uint32_t>(),
+                        s->kb.as<uint32_t>(), s->vb.as<uint32_t>(), s->sort_scratch.as<uint32_t>(), s->N,
+                        s->key_bits, &which, st));
+    if (which != s->sort_which) return fail(PGMPM_ERR_STATE, "internal: sort buffer parity changed");
+    CK(launch_mark(V, st));
+    if (timed) CK(cudaEventRecord(s->ev[1], st));
+    CK(launch_p2g(V, s->pf, s->tune, st));
+    if (timed) CK(cudaEventRecord(s->ev[2], st));
+    CK(launch_grid(V, s->pf, s->tune, s->num_sms, st));
+    if (timed) CK(cudaEventRecord(s->ev[3], st));
+    CK(launch_g2p(V, s->pf, s->tune, st));
+    if (timed) CK(cudaEventRecord(s->ev[4], st));
+    return PGMPM_OK;
+}
+
+int build_graph(pgmpm_solver s) {
+    s->drop_graph();
+    CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = record_step(s, s->cap_stream, false);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
+    if (rc != PGMPM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    CK(e);
+    s->step_graph = g;
+    CK(cudaGraphInstantiate(&s->step_exec, g, 0));
+    return PGMPM_OK;
+}
+
+int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    for (int k = 0; k < n_steps; ++k) {
+        if (s->profiling) {
+            int rc = record_step(s, st, true);
+            if (rc) return rc;
+            CK(cudaEventSynchronize(s->ev[4]));
+            float a, b, c, d;
+            CK(cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
+            CK(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
+            CK(cudaEventElapsedTime(&c, s->ev[2], s->ev[3]));
+            CK(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
+            s->met.sort_ms = a;
+            s->met.p2g_ms = b;
+            s->met.grid_ms = c;
+            s->met.g2p_ms = d;
+            s->met.last_step_ms = a + b + c + d;
+            s->met.average_step_ms =
+                (s->met.average_step_ms * s->met.total_steps + s->met.last_step_ms) / (s->met.total_steps + 1);
+            s->met.particle_steps_per_s = s->met.average_step_ms > 0 ? s->N / (s->met.average_step_ms * 1e-3) : 0;
+        } else if (s->use_graph) {
+            if (!s->step_exec) {
+                int rc = build_graph(s);
+                if (rc) return rc;
+            }
+            CK(cudaGraphLaunch(s->step_exec, st));
+        } else {
+            int rc = record_step(s, st, false);
+            if (rc) return rc;
+        }
+        s->met.total_steps++;
+    }
+    return PGMPM_OK;
+}
+
+}  // namespace
+
+// ============================================================== C-ABI
+extern "C" {
+
+const char* pgmpm_last_error(void) { return g_err.c_str(); }
+int pgmpm_abi_version(void) { return PGMPM_ABI_VERSION; }
+
+int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,
+                 const pgmpm_material* materials, int32_t n_materials, int32_t device, pgmpm_solver* out) {
+    if (!out) return fail(PGMPM_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!scenes || n_scenes < 1 || !particle_counts) return fail(PGMPM_ERR_ARG, "need >= 1 scene and counts");
+    if (!materials || n_materials < 1) return fail(PGMPM_ERR_ARG, "need >= 1 material");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(PGMPM_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev) return fail(PGMPM_ERR_ARG, "device %d out of range", device);
+    DeviceGuard dg(device);
+    auto s = new pgmpm_solver_s();
+    s->device = device;
+    cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+    s->S = n_scenes;
+    s->M = n_materials;
+    s->desc.assign(scenes, scenes + n_scenes);
+    s->counts.assign(particle_counts, particle_counts + n_scenes);
+    s->mats_h.assign(materials, materials + n_materials);
+    int64_t N = 0;
+    int64_t ct_base = 0, nt_base = 0;
+    const int physics = scenes[0].physics;
+    for (int i = 0; i < n_scenes; ++i) {
+        const pgmpm_scene_desc& d = scenes[i];
+        if (d.physics != PGMPM_PHYSICS_MLS && d.physics != PGMPM_PHYSICS_REF_COMPAT) {
+            delete s;
+            return fail(PGMPM_ERR_ARG, "scene %d: unknown physics %d", i, d.physics);
+        }
+        if (d.physics != physics) {
+            delete s;
+            return fail(PGMPM_ERR_ARG, "all scenes of one solver must use the same physics");
+        }
+        if (d.n[0] < 4 || d.n[1] < 4 || d.n[2] < 4 || !(d.dx > 0.f) || !(d.dt > 0.f) || particle_counts[i] < 0) {
+            delete s;
+            return fail(PGMPM_ERR_ARG, "scene %d: need n >= 4 per axis, dx > 0, dt > 0, count >= 0", i);
+        }
+        if (d.boundary < PGMPM_BC_NONE || d.boundary > PGMPM_BC_SEPARATE || d.boundary_thickness < 0) {
+            delete s;
+            return fail(PGMPM_ERR_ARG, "scene %d: invalid boundary", i);
+        }
+        SceneDev sd;
+        std::memset(&sd, 0, sizeof(sd));
+        for (int a = 0; a < 3; ++a) {
+            sd.n[a] = d.n[a];
+            sd.ct[a] = ((d.n[a] - 3) >> 2) + 1;
+            sd.nt[a] = sd.ct[a] + 1;
+            sd.origin[a] = d.origin[a];
+            sd.gravity[a] = d.gravity[a];
+        }
+        sd.ct_base = (int)ct_base;
+        sd.nt_base = (int)nt_base;
+        ct_base += (int64_t)sd.ct[0] * sd.ct[1] * sd.ct[2];
+        nt_base += (int64_t)sd.nt[0] * sd.nt[1] * sd.nt[2];
+        sd.physics = d.physics == PGMPM_PHYSICS_MLS ? PHYS_MLS : PHYS_REF;
+        sd.boundary = d.physics == PGMPM_PHYSICS_MLS ? d.boundary : BC_NONE;
+        sd.bthick = d.boundary_thickness;
+        sd.p_begin = (int)N;
+        N += particle_counts[i];
+        sd.p_end = (int)std::min<int64_t>(N, 0x7FFFFFFF);
+        sd.dx = d.dx;
+        sd.D = 4.f / (d.dx * d.dx);
+        sd.dt = d.dt;
+        s->scenes.push_back(sd);
+        if (ct_base * 64 > 0xFFFFFFFFll || nt_base * 64 > (1ll << 40)) {
+            delete s;
+            return fail(PGMPM_ERR_ARG, "grids too large for 32-bit cell keys");
+        }
+    }
+    if (N >= 0x7FFFFFFF) {
+        delete s;
+        return fail(PGMPM_ERR_ARG, "too many particles (max 2^31-2)");
+    }
+    s->N = N;
+    s->total_ct = (int)ct_base;
+    s->total_nt = (int)nt_base;
+    s->key_bits = bits_for((uint64_t)ct_base * 64);
+    s->pf.physics = physics == PGMPM_PHYSICS_MLS ? PHYS_MLS : PHYS_REF;
+    s->pf.multi_mat = n_materials > 1;
+    s->pf.has_fluid = false;
+    std::vector<MatDev> md(n_materials);
+    for (int i = 0; i < n_materials; ++i) {
+        int rc = material_to_dev(materials[i], md[i]);
+        if (rc) {
+            delete s;
+            return rc;
+        }
+        if (md[i].model == MODEL_EOS) s->pf.has_fluid = true;
+    }
+    int sw = 0;
+    {
+        int passes = radix_passes(s->key_bits);
+        sw = (passes - 1) & 1;
+    }
+    s->sort_which = sw;
+    const size_t n4 = sizeof(uint32_t) * (size_t)std::max<int64_t>(N, 1);
+    cudaError_t e = cudaSuccess;
+#define AL(buf, bytes)                                         \
+    if (e == cudaSuccess) e = (buf).alloc(bytes);
+    AL(s->d_scenes, sizeof(SceneDev) * n_scenes);
+    AL(s->d_mats, sizeof(MatDev) * n_materials);
+    AL(s->q, sizeof(float4) * 6 * (size_t)std::max<int64_t>(N, 1));
+    AL(s->mV, sizeof(float2) * (size_t)std::max<int64_t>(N, 1));
+    if (s->pf.multi_mat) AL(s->mat, n4);
+    AL(s->user_of_phys, n4);
+    AL(s->keys, n4);
+    AL(s->ka, n4);
+    AL(s->va, n4);
+    AL(s->kb, n4);
+    AL(s->vb, n4);
+    AL(s->sort_scratch, sizeof(uint32_t) * (size_t)radix_sort_scratch_words(std::max<int64_t>(N, 1)));
+    AL(s->grid_mp, sizeof(float4) * 64 * (size_t)nt_base);
+    AL(s->grid_v, sizeof(float4) * 64 * (size_t)nt_base);
+    AL(s->tile_flags, sizeof(uint32_t) * (size_t)nt_base);
+    AL(s->tile_list, sizeof(uint32_t) * (size_t)nt_base);
+    AL(s->counters, sizeof(uint32_t) * CNT_WORDS);
+#undef AL
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_scenes.p, s->scenes.data(), sizeof(SceneDev) * n_scenes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(s->grid_mp.p, 0, s->grid_mp.bytes);
+    if (e == cudaSuccess) e = cudaMemset(s->grid_v.p, 0, s->grid_v.bytes);
+    if (e == cudaSuccess) e = cudaMemset(s->tile_flags.p, 0, s->tile_flags.bytes);
+    if (e == cudaSuccess) e = cudaMemset(s->counters.p, 0, s->counters.bytes);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_counters, sizeof(uint32_t) * CNT_WORDS);
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(e == cudaErrorMemoryAllocation ? PGMPM_ERR_OOM : PGMPM_ERR_CUDA, "create: %s",
+                    cudaGetErrorString(e));
+    }
+    s->met.num_particles = N;
+    *out = s;
+    return PGMPM_OK;
+}
+
+int pgmpm_destroy(pgmpm_solver s) {
+    if (!s) return PGMPM_OK;
+    {
+        DeviceGuard dg(s->device);
+        cudaDeviceSynchronize();
+    }
+    delete s;
+    return PGMPM_OK;
+}
+
+int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t n_materials) {
+    if (!s || !materials || n_materials != s->M) return fail(PGMPM_ERR_ARG, "material count must match create()");
+    DeviceGuard dg(s->device);
+    std::vector<MatDev> md(n_materials);
+    bool fluid = false;
+    for (int i = 0; i < n_materials; ++i) {
+        int rc = material_to_dev(materials[i], md[i]);
+        if (rc) return rc;
+        fluid |= md[i].model == MODEL_EOS;
+    }
+    if (fluid != s->pf.has_fluid) {
+        s->pf.has_fluid = fluid;
+        s->drop_graph();
+    }
+    // ordered with prior work on the legacy stream; graphs read the table at run time
+    CK(cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice));
+    s->mats_h.assign(materials, materials + n_materials);
+    return PGMPM_OK;
+}
+
+int pgmpm_upload(pgmpm_solver s, const float* x, const float* v, const float* C, const float* F, const float* m,
+                 const float* V0, const int32_t* mat, int32_t ptr_kind, void* stream) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (s->N > 0 && (!x || !m)) return fail(PGMPM_ERR_ARG, "x and m are required");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const int64_t N = s->N;
+    const float *dx_ = x, *dv = v, *dC = C, *dF = F, *dm = m, *dV0 = V0;
+    const int32_t* dmat = mat;
+    if (ptr_kind == PGMPM_PTR_HOST && N > 0) {
+        const size_t fl = 3 + 3 + 9 + 9 + 1 + 1;
+        CK(s->staging.ensure(sizeof(float) * fl * N + sizeof(int32_t) * N));
+        float* b = s->staging.as<float>();
+        float* sx = b;
+        float* sv = sx + 3 * N;
+        float* sC = sv + 3 * N;
+        float* sF = sC + 9 * N;
+        float* sm = sF + 9 * N;
+        float* sV = sm + N;
+        int32_t* smat = reinterpret_cast<int32_t*>(sV + N);
+        CK(cudaMemcpyAsync(sx, x, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(sm, m, sizeof(float) * N, cudaMemcpyHostToDevice, st));
+        dx_ = sx;
+        dm = sm;
+        dv = v ? sv : nullptr;
+        dC = C ? sC : nullptr;
+        dF = F ? sF : nullptr;
+        dV0 = V0 ? sV : nullptr;
+        dmat = mat ? smat : nullptr;
+        if (v) CK(cudaMemcpyAsync(sv, v, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, st));
+        if (C) CK(cudaMemcpyAsync(sC, C, sizeof(float) * 9 * N, cudaMemcpyHostToDevice, st));
+        if (F) CK(cudaMemcpyAsync(sF, F, sizeof(float) * 9 * N, cudaMemcpyHostToDevice, st));
+        if (V0) CK(cudaMemcpyAsync(sV, V0, sizeof(float) * N, cudaMemcpyHostToDevice, st));
+        if (mat) CK(cudaMemcpyAsync(smat, mat, sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+    } else if (ptr_kind != PGMPM_PTR_DEVICE && ptr_kind != PGMPM_PTR_HOST) {
+        return fail(PGMPM_ERR_ARG, "ptr_kind must be PGMPM_PTR_HOST or PGMPM_PTR_DEVICE");
+    }
+    if (mat && s->M == 1) dmat = nullptr;
+    if (N > 0) {
+        View V = s->view();
+        // 1. identity pack (user order) to compute the keys
+        CK(cudaMemsetAsync(s->keys.p, 0, sizeof(uint32_t) * N, st));
+        // order = identity: use va as a temporary iota through the sort of all-zero keys
+        int w0 = 0;
+        CK(radix_sort_pairs(s->keys.as<uint32_t>(), nullptr, s->ka.as<uint32_t>(), s->va.as<uint32_t>(),
+                            s->kb.as<uint32_t>(), s->vb.as<uint32_t>(), s->sort_scratch.as<uint32_t>(), N, 1, &w0,
+                            st));
+        const uint32_t* iota = w0 ? s->vb.as<uint32_t>() : s->va.as<uint32_t>();
+        CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, iota, s->user_of_phys.as<uint32_t>(), s->mV.as<float2>(),
+                       s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr, st));
+        // 2. keys of the user-order positions, stable sort -> physical order
+        CK(launch_keys(V, s->pf, st));
+        int which = 0;
+        CK(radix_sort_pairs(s->keys.as<uint32_t>(), nullptr, s->ka.as<uint32_t>(), s->va.as<uint32_t>(),
+                            s->kb.as<uint32_t>(), s->vb.as<uint32_t>(), s->sort_scratch.as<uint32_t>(), N,
+                            s->key_bits, &which, st));
+        const uint32_t* ord = which ? s->vb.as<uint32_t>() : s->va.as<uint32_t>();
+        const uint32_t* sk = which ? s->kb.as<uint32_t>() : s->ka.as<uint32_t>();
+        // 3. pack in sorted order; the sorted keys are the keys of the physical order
+        CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, ord, s->user_of_phys.as<uint32_t>(), s->mV.as<float2>(),
+                       s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr, st));
+        CK(cudaMemcpyAsync(s->keys.p, sk, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
+    }
+    s->uploaded = true;
+    return PGMPM_OK;
+}
+
+int pgmpm_download(pgmpm_solver s, float* x, float* v, float* C, float* F, int32_t ptr_kind, void* stream) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const int64_t N = s->N;
+    if (N == 0) return PGMPM_OK;
+    View V = s->view();
+    if (ptr_kind == PGMPM_PTR_DEVICE) {
+        CK(launch_unpack(V, s->user_of_phys.as<uint32_t>(), x, v, C, F, st));
+        return PGMPM_OK;
+    }
+    if (ptr_kind != PGMPM_PTR_HOST) return fail(PGMPM_ERR_ARG, "bad ptr_kind");
+    CK(s->staging.ensure(sizeof(float) * 26 * N + sizeof(int32_t) * N));
+    float* sx = s->staging.as<float>();
+    float* sv = sx + 3 * N;
+    float* sC = sv + 3 * N;
+    float* sF = sC + 9 * N;
+    CK(launch_unpack(V, s->user_of_phys.as<uint32_t>(), x ? sx : nullptr, v ? sv : nullptr, C ? sC : nullptr,
+                     F ? sF : nullptr, st));
+    if (x) CK(cudaMemcpyAsync(x, sx, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
+    if (v) CK(cudaMemcpyAsync(v, sv, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
+    if (C) CK(cudaMemcpyAsync(C, sC, sizeof(float) * 9 * N, cudaMemcpyDeviceToHost, st));
+    if (F) CK(cudaMemcpyAsync(F, sF, sizeof(float) * 9 * N, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PGMPM_OK;
+}
+
+int pgmpm_download_grid(pgmpm_solver s, int32_t scene, float* mass, float* velocity, int32_t ptr_kind,
+                        void* stream) {
+    if (!s || scene < 0 || scene >= s->S) return fail(PGMPM_ERR_ARG, "bad solver or scene");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const SceneDev& sc = s->scenes[scene];
+    const int64_t nodes = (int64_t)sc.n[0] * sc.n[1] * sc.n[2];
+    View V = s->view();
+    if (ptr_kind == PGMPM_PTR_DEVICE) {
+        CK(launch_grid_download(V, scene, sc, mass, velocity, st));
+        return PGMPM_OK;
+    }
+    DevBuf tmp;
+    CK(tmp.alloc(sizeof(float) * 4 * nodes));
+    float* dm = tmp.as<float>();
+    float* dv = dm + nodes;
+    CK(launch_grid_download(V, scene, sc, dm, dv, st));
+    if (mass) CK(cudaMemcpyAsync(mass, dm, sizeof(float) * nodes, cudaMemcpyDeviceToHost, st));
+    if (velocity) CK(cudaMemcpyAsync(velocity, dv, sizeof(float) * 3 * nodes, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PGMPM_OK;
+}
+
+int pgmpm_step(pgmpm_solver s, int32_t n_steps, void* stream) {
+    if (!s || n_steps < 0) return fail(PGMPM_ERR_ARG, "bad arguments");
+    DeviceGuard dg(s->device);
+    return run_steps(s, n_steps, ST(stream));
+}
+
+int pgmpm_advance_host(pgmpm_solver s, const float* x_in, const float* v_in, const float* C_in, const float* F_in,
+                       const float* m, const float* V0, const int32_t* mat, int32_t n_steps, float* x_out,
+                       float* v_out, float* C_out, float* F_out, void* stream) {
+    int rc = pgmpm_upload(s, x_in, v_in, C_in, F_in, m, V0, mat, PGMPM_PTR_HOST, stream);
+    if (rc) return rc;
+    rc = pgmpm_step(s, n_steps, stream);
+    if (rc) return rc;
+    return pgmpm_download(s, x_out, v_out, C_out, F_out, PGMPM_PTR_HOST, stream);
+}
+
+int pgmpm_check_status(pgmpm_solver s, uint32_t* flags, void* stream) {
+    if (!s || !flags) return fail(PGMPM_ERR_ARG, "bad arguments");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    CK(cudaMemcpyAsync(s->h_counters, s->counters.p, sizeof(uint32_t) * CNT_WORDS, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemsetAsync(s->counters.as<uint32_t>() + CNT_FLAGS, 0, sizeof(uint32_t), st));
+    CK(cudaStreamSynchronize(st));
+    *flags = s->h_counters[CNT_FLAGS];
+    uint64_t act;
+    std::memcpy(&act, &s->h_counters[CNT_ACTIVE], sizeof(act));
+    s->met.active_nodes = (int64_t)act;
+    return PGMPM_OK;
+}
+
+int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p_block, int32_t use_graph) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    auto okb = [](int b) { return b == 0 || (b >= 64 && b <= 512 && b % 64 == 0); };
+    if (!okb(p2g_block) || !okb(g2p_block)) return fail(PGMPM_ERR_ARG, "block sizes must be 64..512, multiple of 64");
+    if (ppt != 0 && (ppt < 32 || ppt > (1 << 20))) return fail(PGMPM_ERR_ARG, "ppt must be in [32, 2^20]");
+    if (p2g_block) s->tune.p2g_block = p2g_block;
+    if (ppt) s->tune.ppt = ppt;
+    if (g2p_block) s->tune.g2p_block = g2p_block;
+    if (use_graph >= 0) s->use_graph = use_graph != 0;
+    s->drop_graph();
+    return PGMPM_OK;
+}
+
+int pgmpm_set_profiling(pgmpm_solver s, int32_t profile) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    s->profiling = profile != 0;
+    return PGMPM_OK;
+}
+
+int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out) {
+    if (!s || !out) return fail(PGMPM_ERR_ARG, "bad arguments");
+    s->met.p2g_block = s->tune.p2g_block;
+    s->met.p2g_ppt = s->tune.ppt;
+    s->met.g2p_block = s->tune.g2p_block;
+    s->met.graph_enabled = s->use_graph ? 1 : 0;
+    *out = s->met;
+    return PGMPM_OK;
+}
+
+int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "upload particles before autotuning");
+    if (s->N == 0) return PGMPM_OK;
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    if (reps < 1) reps = 3;
+    // save state (planes + keys) and restore after the trials
+    DevBuf save;
+    const size_t qb = sizeof(float4) * 6 * (size_t)s->N;
+    CK(save.alloc(qb + sizeof(uint32_t) * s->N));
+    CK(cudaMemcpyAsync(save.p, s->q.p, qb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(save.as<char>() + qb, s->keys.p, sizeof(uint32_t) * s->N, cudaMemcpyDeviceToDevice, st));
+    const Tuning keep = s->tune;
+    const bool keep_graph = s->use_graph, keep_prof = s->profiling;
+    s->use_graph = false;
+    s->profiling = false;
+    const int p2g_blocks[] = {128, 256, 512};
+    const int ppts[] = {256, 512, 1024, 2048, 4096};
+    const int g2p_blocks[] = {128, 256, 512};
+    Tuning best = keep;
+    float best_p2g = 1e30f, best_g2p = 1e30f;
+    View V = s->view();
+    auto time_it = [&](auto&& fn, float& ms) -> int {
+        CK(cudaEventRecord(s->ev[0], st));
+        for (int r = 0; r < reps; ++r) CK(fn());
+        CK(cudaEventRecord(s->ev[1], st));
+        CK(cudaEventSynchronize(s->ev[1]));
+        CK(cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]));
+        return PGMPM_OK;
+    };
+    // one real step so the sorted order, tile list and grid velocity exist
+    int rc = record_step(s, st, false);
+    if (rc) return rc;
+    for (int pb : p2g_blocks)
+        for (int ppt : ppts) {
+            if (ppt < pb) continue;
+            Tuning t = keep;
+            t.p2g_block = pb;
+            t.ppt = ppt;
+            float ms = 0.f;
+            rc = time_it([&]() { return launch_p2g(V, s->pf, t, st); }, ms);
+            if (rc) return rc;
+            if (ms < best_p2g) {
+                best_p2g = ms;
+                best.p2g_block = pb;
+                best.ppt = ppt;
+            }
+        }
+    for (int gb : g2p_blocks) {
+        Tuning t = keep;
+        t.g2p_block = gb;
+        float ms = 0.f;
+        rc = time_it([&]() { return launch_g2p(V, s->pf, t, st); }, ms);
+        if (rc) return rc;
+        if (ms < best_g2p) {
+            best_g2p = ms;
+            best.g2p_block = gb;
+        }
+    }
+    // restore: state, keys, clean accumulator grid
+    CK(cudaMemcpyAsync(s->q.p, save.p, qb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->keys.p, save.as<char>() + qb, sizeof(uint32_t) * s->N, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(s->grid_mp.p, 0, s->grid_mp.bytes, st));
+    CK(cudaStreamSynchronize(st));
+    s->tune = best;
+    s->use_graph = keep_graph;
+    s->profiling = keep_prof;
+    s->drop_graph();
+    return PGMPM_OK;
+}
+
+int pgmpm_get_array(pgmpm_solver s, int32_t which, uint32_t* out, int32_t ptr_kind, void* stream) {
+    if (!s || !out) return fail(PGMPM_ERR_ARG, "bad arguments");
+    DeviceGuard dg(s->device);
+    const void* src = nullptr;
+    switch (which) {
+        case PGMPM_ARRAY_USER_INDEX: src = s->user_of_phys.p; break;
+        case PGMPM_ARRAY_KEYS: src = s->keys.p; break;
+        case PGMPM_ARRAY_SORTED_KEYS: src = s->sort_which ? s->kb.p : s->ka.p; break;
+        case PGMPM_ARRAY_SORTED_ORDER: src = s->sort_which ? s->vb.p : s->va.p; break;
+        default: return fail(PGMPM_ERR_ARG, "unknown array %d", which);
+    }
+    if (s->N == 0) return PGMPM_OK;
+    cudaStream_t st = ST(stream);
+    CK(cudaMemcpyAsync(out, src, sizeof(uint32_t) * s->N,
+                       ptr_kind == PGMPM_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PGMPM_OK;
+}
+
+int pgmpm_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                           int64_t n, int32_t key_bits, void* stream) {
+    if (n < 0 || (n > 0 && (!keys_in || !keys_out || !vals_out)) || key_bits < 1 || key_bits > 32)
+        return fail(PGMPM_ERR_ARG, "bad arguments");
+    if (n == 0) return PGMPM_OK;
+    cudaStream_t st = ST(stream);
+    DevBuf a, b, sc;
+    CK(a.alloc(sizeof(uint32_t) * 2 * n));
+    CK(b.alloc(sizeof(uint32_t) * 2 * n));
+    CK(sc.alloc(sizeof(uint32_t) * radix_sort_scratch_words(n)));
+    int which = 0;
+    uint32_t* ka = a.as<uint32_t>();
+    uint32_t* kb = b.as<uint32_t>();
+    CK(radix_sort_pairs(keys_in, vals_in, ka, ka + n, kb, kb + n, sc.as<uint32_t>(), n, key_bits, &which, st));
+    const uint32_t* rk = which ? kb : ka;
+    CK(cudaMemcpyAsync(keys_out, rk, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(vals_out, rk + n, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return PGMPM_OK;
+}
+
+}  // extern "C"

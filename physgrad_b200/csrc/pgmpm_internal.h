@@ -1,0 +1,89 @@
+// pgmpm_internal.h -- declarations shared by the CUDA translation units of
+// libpgmpm.so.  Not installed; the public surface is include/pgmpm.h.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pgmpm_device.cuh"
+
+namespace pgmpm {
+
+// counters[] layout: active tile count, active node count (u64, reset
+// every step) and the sticky error flags.
+enum { CNT_TILES = 0, CNT_ACTIVE = 2, CNT_FLAGS = 4, CNT_WORDS = 8 };
+
+// Everything a step kernel needs, passed by value.
+struct View {
+    int64_t N;
+    int S, M;
+    const SceneDev* scenes;
+    const MatDev* mats;
+    float4* q;                 // 6 planes of N float4
+    const float2* mV;          // (mass, V0)
+    const int32_t* mat;        // material id (null when M == 1)
+    uint32_t* keys;            // cell key per particle (physical order), input of the next sort
+    const uint32_t* skeys;     // sorted keys
+    const uint32_t* order;     // sorted position -> physical particle
+    float4* grid_mp;           // (m, p) accumulator
+    float4* grid_v;            // (v, m) after the grid update
+    float4* grid_vpre;         // optional: (v before walls, m), recorded for the adjoint
+    uint32_t* tile_flags;      // node tile active flags (per global node tile)
+    uint32_t* tile_list;       // active node tiles
+    uint32_t* counters;        // see CNT_*
+    int total_ct, total_nt;
+};
+
+struct Tuning {
+    int p2g_block = 256;
+    int ppt = 1024;
+    int g2p_block = 256;
+    int grid_block = 256;
+};
+
+// pgmpm_sort.cu
+int64_t radix_sort_scratch_words(int64_t n);
+int radix_passes(int key_bits);
+cudaError_t radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uint32_t* va, uint32_t* kb,
+                             uint32_t* vb, uint32_t* scratch, int64_t n, int key_bits, int* which,
+                             cudaStream_t st);
+
+// pgmpm_kernels.cu
+struct PhysFlags {
+    int physics;     // PHYS_MLS / PHYS_REF (same for every scene)
+    bool multi_mat;  // per-particle material ids
+    bool has_fluid;  // some material uses the EOS model
+};
+cudaError_t launch_keys(const View& V, const PhysFlags& pf, cudaStream_t st);
+cudaError_t launch_mark(const View& V, cudaStream_t st);
+cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st);
+cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
+cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st);
+cudaError_t launch_pack(const View& V, const float* x, const float* v, const float* C, const float* F,
+                        const float* m, const float* V0, const int32_t* mat, const uint32_t* order,
+                        uint32_t* user_of_phys, float2* mV_out, int32_t* mat_out, cudaStream_t st);
+cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x, float* v, float* C, float* F,
+                          cudaStream_t st);
+cudaError_t launch_grid_download(const View& V, int scene, const SceneDev& sc, float* mass, float* vel,
+                                 cudaStream_t st);
+
+// pgmpm_adjoint.cu
+struct AdjView {
+    // adjoint of the particle state after the step, overwritten with the
+    // adjoint of the state before it (physical order, same plane packing)
+    float4* g;                 // 6 planes
+    const float4* q_next;      // state after the step (for C' and F'raw)
+    float4* grid_gv;           // (dL/dv_i, -) scatter target, zeroed by the grid adjoint
+    float4* grid_gpm;          // (dL/dp_i, dL/dm_i) per node
+    float* gE;                 // [M] dL/dE accumulators
+};
+cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t,
+                               cudaStream_t st);
+cudaError_t launch_adj_grid(const View& V, const AdjView& A, const Tuning& t, int num_sms, cudaStream_t st);
+cudaError_t launch_adj_gather(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t,
+                              cudaStream_t st);
+cudaError_t launch_state_to_planes(const float* x, const float* v, const float* C, const float* F,
+                                   const uint32_t* user_of_phys, float4* g, int64_t N, cudaStream_t st);
+cudaError_t launch_planes_to_state(const float4* g, const uint32_t* user_of_phys, float* x, float* v, float* C,
+                                   float* F, int64_t N, cudaStream_t st);
+
+}  // namespace pgmpm

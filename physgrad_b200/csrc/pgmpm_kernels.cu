@@ -1,0 +1,581 @@
+// pgmpm_kernels.cu -- the forward MLS-MPM step on sm_100a.
+//
+// Per step (all on one stream, capturable as a CUDA graph):
+//   [sort]   radix sort of the cell keys written by the previous G2P
+//   k_mark   node tiles touched by each occupied cell tile -> active list
+//   k_p2g    one block per chunk of `ppt` sorted particles; for each run of
+//            the chunk that lies in one 4^3 cell tile the block accumulates
+//            into a 6^3-node shared-memory tile (4 channels: m, p) and then
+//            flushes every touched node with ONE vector atomic
+//            (red.global.add.v4.f32) into grid_mp.  Lanes are spread over
+//            the run (lane l of a warp takes particle l*R + r) so that the 32
+//            shared atomics of one instruction fall in different cells.
+//   k_grid   active node tiles only: v = p/m + dt g, walls, (v, m) -> grid_v,
+//            grid_mp cleared for the next step.
+//   k_g2p    one thread per sorted particle: 27-node gather of v, APIC C,
+//            F <- (I + dt C) F, x <- x + dt v, and the particle's next key.
+// HBM-bound: no tensor-core work exists on this path (scatter/gather
+// stencil, not a dense contraction).
+#include "pgmpm_internal.h"
+
+namespace pgmpm {
+
+namespace {
+
+constexpr int TN = 6;              // smem tile edge in nodes (4 cells + 2)
+constexpr int TILE_NODES = TN * TN * TN;
+
+__device__ __forceinline__ const SceneDev& scene_ref(const View& V, int s) { return V.scenes[s]; }
+
+// ------------------------------------------------------------------ keys
+template <int PHYS>
+__global__ void k_keys(View V) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint32_t flags = 0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < V.N; p += stride) {
+        const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
+        const SceneDev& sc = scene_ref(V, s);
+        const float4 q0 = V.q[p];
+        const float x[3] = {q0.x, q0.y, q0.z};
+        int so[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float u;
+            so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+        }
+        V.keys[p] = cell_key(sc, so);
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+// ------------------------------------------------------------------ mark
+__global__ void k_mark(View V) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < V.N; i += stride) {
+        const uint32_t ct = V.skeys[i] >> 6;
+        if (i > 0 && (V.skeys[i - 1] >> 6) == ct) continue;
+        if (ct >= (uint32_t)V.total_ct) {
+            atomicOr(&V.counters[CNT_FLAGS], FLAG_TILE_RANGE);
+            continue;
+        }
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int tx = lt % sc.ct[0], ty = (lt / sc.ct[0]) % sc.ct[1], tz = lt / (sc.ct[0] * sc.ct[1]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int nx = tx + (c & 1), ny = ty + ((c >> 1) & 1), nz = tz + (c >> 2);
+            const uint32_t nt = (uint32_t)(sc.nt_base + (nz * sc.nt[1] + ny) * sc.nt[0] + nx);
+            if (atomicExch(&V.tile_flags[nt], 1u) == 0u) {
+                const uint32_t slot = atomicAdd(&V.counters[CNT_TILES], 1u);
+                V.tile_list[slot] = nt;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------- P2G
+template <int PHYS, bool MULTI>
+__global__ void __launch_bounds__(512) k_p2g(View V, int ppt) {
+    __shared__ float tile[4 * TILE_NODES];
+    for (int i = threadIdx.x; i < 4 * TILE_NODES; i += blockDim.x) tile[i] = 0.f;
+    __syncthreads();
+    const int64_t N = V.N;
+    const int64_t c0 = (int64_t)blockIdx.x * ppt;
+    if (c0 >= N) return;
+    const int64_t cend = min(N, c0 + (int64_t)ppt);
+    uint32_t flags = 0;
+    int64_t seg = c0;
+    while (seg < cend) {
+        const uint32_t ct = V.skeys[seg] >> 6;
+        // end of this cell tile's run inside the chunk (keys are sorted)
+        int64_t lo = seg + 1, hi = cend;
+        const uint32_t target = (ct + 1u) << 6;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (V.skeys[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        const int64_t send = lo;
+        if (ct >= (uint32_t)V.total_ct) {  // corrupt key: skip the run, report
+            flags |= FLAG_TILE_RANGE;
+            seg = send;
+            continue;
+        }
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        const int L = (int)(send - seg);
+        const int R = (L + 31) >> 5;
+        for (int slot = threadIdx.x; slot < 32 * R; slot += blockDim.x) {
+            const int jj = (slot & 31) * R + (slot >> 5);
+            if (jj >= L) continue;
+            const uint32_t p = V.order[seg + jj];
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            const float4 q0 = V.q[p];
+            const float x[3] = {q0.x, q0.y, q0.z};
+            const float2 mv = V.mV[p];
+            Stencil st;
+            make_stencil<PHYS>(sc, x, st, flags);
+            if (PHYS == PHYS_MLS) {
+                const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+                const float4 q3 = V.q[3 * N + p], q4 = V.q[4 * N + p], q5 = V.q[5 * N + p];
+                float xx[3], F[9], v[3], C[9];
+                unpack_xF(q0, q1, q2, xx, F);
+                unpack_vC(q3, q4, q5, v, C);
+                const MatDev mt = V.mats[MULTI ? V.mat[p] : 0];
+                float tau[9];
+                kirchhoff(F, mt, tau);
+                const float kk = -sc.dt * mv.y * sc.D;
+                float A[9];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) A[i] = kk * tau[i] + mv.x * C[i];
+                const int lx = st.s[0] - ox, ly = st.s[1] - oy, lz = st.s[2] - oz;
+                if ((unsigned)lx > 3u || (unsigned)ly > 3u || (unsigned)lz > 3u) {
+                    flags |= FLAG_TILE_RANGE;
+                    continue;
+                }
+                const float dx = sc.dx;
+                float d0[3], d1[3], d2[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    d0[i] = ((float)i - st.f[0]) * dx;
+                    d1[i] = ((float)i - st.f[1]) * dx;
+                    d2[i] = ((float)i - st.f[2]) * dx;
+                }
+                const float m = mv.x;
+                const float mvx = m * v[0], mvy = m * v[1], mvz = m * v[2];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const float wjk = st.w[1][j] * st.w[2][k];
+                        const float bx = mvx + A[1] * d1[j] + A[2] * d2[k];
+                        const float by = mvy + A[4] * d1[j] + A[5] * d2[k];
+                        const float bz = mvz + A[7] * d1[j] + A[8] * d2[k];
+                        const int row = (lx) + TN * (ly + j) + TN * TN * (lz + k);
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            const float w = st.w[0][i] * wjk;
+                            const int nidx = row + i;
+                            atomicAdd(&tile[nidx], w * m);
+                            atomicAdd(&tile[TILE_NODES + nidx], w * (bx + A[0] * d0[i]));
+                            atomicAdd(&tile[2 * TILE_NODES + nidx], w * (by + A[3] * d0[i]));
+                            atomicAdd(&tile[3 * TILE_NODES + nidx], w * (bz + A[6] * d0[i]));
+                        }
+                    }
+                }
+            } else {
+                const float4 q3 = V.q[3 * N + p];
+                const float vel[3] = {q3.x, q3.y, q3.z};
+                const float mass = mv.x;
+                // reference loop order: x outer, z inner (material_point_method.h:535-566)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const int gi = st.b[0] + i;
+                    if (gi < 0 || gi >= sc.n[0]) continue;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const int gj = st.b[1] + j;
+                        if (gj < 0 || gj >= sc.n[1]) continue;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const int gk = st.b[2] + k;
+                            if (gk < 0 || gk >= sc.n[2]) continue;
+                            const float weight = __fmul_rn(__fmul_rn(st.w[0][i], st.w[1][j]), st.w[2][k]);
+                            if (!(weight > 1e-10f)) continue;
+                            const int lx = gi - ox, ly = gj - oy, lz = gk - oz;
+                            if ((unsigned)lx >= (unsigned)TN || (unsigned)ly >= (unsigned)TN ||
+                                (unsigned)lz >= (unsigned)TN) {
+                                flags |= FLAG_TILE_RANGE;
+                                continue;
+                            }
+                            const int nidx = lx + TN * ly + TN * TN * lz;
+                            const float wm = __fmul_rn(weight, mass);
+                            atomicAdd(&tile[nidx], wm);
+                            atomicAdd(&tile[TILE_NODES + nidx], __fmul_rn(wm, vel[0]));
+                            atomicAdd(&tile[2 * TILE_NODES + nidx], __fmul_rn(wm, vel[1]));
+                            atomicAdd(&tile[3 * TILE_NODES + nidx], __fmul_rn(wm, vel[2]));
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // flush: one vector atomic per touched node, then clear the tile
+        for (int nidx = threadIdx.x; nidx < TILE_NODES; nidx += blockDim.x) {
+            const float m = tile[nidx];
+            if (m != 0.f) {
+                const float4 val = make_float4(m, tile[TILE_NODES + nidx], tile[2 * TILE_NODES + nidx],
+                                               tile[3 * TILE_NODES + nidx]);
+                tile[nidx] = 0.f;
+                tile[TILE_NODES + nidx] = 0.f;
+                tile[2 * TILE_NODES + nidx] = 0.f;
+                tile[3 * TILE_NODES + nidx] = 0.f;
+                const int lx = nidx % TN, ly = (nidx / TN) % TN, lz = nidx / (TN * TN);
+                const int gi = ox + lx, gj = oy + ly, gk = oz + lz;
+                if (gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2]) atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], val);
+            }
+        }
+        __syncthreads();
+        seg = send;
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+// ------------------------------------------------------------ grid update
+template <int PHYS>
+__global__ void k_grid(View V) {
+    const uint32_t count = V.counters[CNT_TILES];
+    const int tiles_per_block = blockDim.x >> 6;
+    const int l = threadIdx.x & 63;
+    uint32_t active = 0;
+    for (uint32_t w = blockIdx.x * tiles_per_block + (threadIdx.x >> 6); w < count;
+         w += gridDim.x * tiles_per_block) {
+        const uint32_t nt = V.tile_list[w];
+        if (nt >= (uint32_t)V.total_nt) continue;
+        const int s = V.S == 1 ? 0 : scene_of_node_tile(V.scenes, V.S, (int)nt);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)nt - sc.nt_base;
+        const int i = 4 * (lt % sc.nt[0]) + (l & 3);
+        const int j = 4 * ((lt / sc.nt[0]) % sc.nt[1]) + ((l >> 2) & 3);
+        const int k = 4 * (lt / (sc.nt[0] * sc.nt[1])) + (l >> 4);
+        const int64_t idx = ((int64_t)nt << 6) + l;
+        const float4 mp = V.grid_mp[idx];
+        float v[3] = {0.f, 0.f, 0.f};
+        if (PHYS == PHYS_MLS) {
+            if (mp.x > 0.f) {
+                v[0] = __fdiv_rn(mp.y, mp.x) + sc.dt * sc.gravity[0];
+                v[1] = __fdiv_rn(mp.z, mp.x) + sc.dt * sc.gravity[1];
+                v[2] = __fdiv_rn(mp.w, mp.x) + sc.dt * sc.gravity[2];
+                ++active;
+            }
+            if (V.grid_vpre) V.grid_vpre[idx] = make_float4(v[0], v[1], v[2], mp.x);
+            apply_bc(sc, i, j, k, v);
+        } else {
+            // material_point_method.h:572-597: p += (m g) dt, v = p / m
+            if (mp.x > 1e-10f) {
+                v[0] = __fdiv_rn(__fadd_rn(mp.y, __fmul_rn(__fmul_rn(mp.x, sc.gravity[0]), sc.dt)), mp.x);
+                v[1] = __fdiv_rn(__fadd_rn(mp.z, __fmul_rn(__fmul_rn(mp.x, sc.gravity[1]), sc.dt)), mp.x);
+                v[2] = __fdiv_rn(__fadd_rn(mp.w, __fmul_rn(__fmul_rn(mp.x, sc.gravity[2]), sc.dt)), mp.x);
+            }
+            if (mp.x > 0.f) ++active;
+        }
+        V.grid_v[idx] = make_float4(v[0], v[1], v[2], mp.x);
+        V.grid_mp[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    unsigned long long a = active;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, o);
+    if ((threadIdx.x & 31) == 0 && a) atomicAdd(reinterpret_cast<unsigned long long*>(&V.counters[CNT_ACTIVE]), a);
+}
+
+// ------------------------------------------------------------------- G2P
+template <int PHYS, bool MULTI, bool FLUID>
+__global__ void k_g2p(View V) {
+    const int64_t N = V.N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint32_t flags = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+        const uint32_t p = V.order[i];
+        if (p >= (uint32_t)N) {
+            flags |= FLAG_TILE_RANGE;
+            continue;
+        }
+        const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
+        const SceneDev& sc = scene_ref(V, s);
+        const float4 q0 = V.q[p];
+        float x[3] = {q0.x, q0.y, q0.z};
+        Stencil st;
+        make_stencil<PHYS>(sc, x, st, flags);
+        if (PHYS == PHYS_MLS) {
+            const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+            float xx[3], F[9];
+            unpack_xF(q0, q1, q2, xx, F);
+            const float dx = sc.dx;
+            float nv[3] = {0.f, 0.f, 0.f};
+            float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float dk = ((float)k - st.f[2]) * dx;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const float dj = ((float)j - st.f[1]) * dx;
+                    const float wjk = st.w[1][j] * st.w[2][k];
+                    const int64_t row = node_index(sc, st.s[0], st.s[1] + j, st.s[2] + k);
+                    const int gi0 = st.s[0];
+#pragma unroll
+                    for (int ii = 0; ii < 3; ++ii) {
+                        const float di = ((float)ii - st.f[0]) * dx;
+                        const int gi = gi0 + ii;
+                        // nodes of a row share the tile unless the row crosses x % 4 == 0
+                        const int64_t idx = ((gi >> 2) == (gi0 >> 2)) ? row + ii
+                                                                      : node_index(sc, gi, st.s[1] + j, st.s[2] + k);
+                        const float4 g = __ldg(&V.grid_v[idx]);
+                        const float w = st.w[0][ii] * wjk;
+                        const float wx = w * g.x, wy = w * g.y, wz = w * g.z;
+                        nv[0] += wx; nv[1] += wy; nv[2] += wz;
+                        B[0] += wx * di; B[1] += wx * dj; B[2] += wx * dk;
+                        B[3] += wy * di; B[4] += wy * dj; B[5] += wy * dk;
+                        B[6] += wz * di; B[7] += wz * dj; B[8] += wz * dk;
+                    }
+                }
+            }
+            float C[9], Fn[9], M[9];
+#pragma unroll
+            for (int a = 0; a < 9; ++a) {
+                C[a] = sc.D * B[a];
+                M[a] = sc.dt * C[a] + ((a % 4 == 0) ? 1.f : 0.f);
+            }
+            m3_mul(M, F, Fn);
+            if (FLUID) {
+                const int mid = MULTI ? V.mat[p] : 0;
+                if (V.mats[mid].model == MODEL_EOS) {
+                    const float c = cbrtf(m3_det(Fn));
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) Fn[a] = (a % 4 == 0) ? c : 0.f;
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) x[a] = x[a] + sc.dt * nv[a];
+            float4 o0, o1, o2, o3, o4, o5;
+            pack_xF(x, Fn, o0, o1, o2);
+            pack_vC(nv, C, o3, o4, o5);
+            V.q[p] = o0;
+            V.q[N + p] = o1;
+            V.q[2 * N + p] = o2;
+            V.q[3 * N + p] = o3;
+            V.q[4 * N + p] = o4;
+            V.q[5 * N + p] = o5;
+        } else {
+            // material_point_method.h:599-666 in the same order of operations
+            float nv[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int ii = 0; ii < 3; ++ii) {
+                const int gi = st.b[0] + ii;
+                if (gi < 0 || gi >= sc.n[0]) continue;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int gj = st.b[1] + j;
+                    if (gj < 0 || gj >= sc.n[1]) continue;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int gk = st.b[2] + k;
+                        if (gk < 0 || gk >= sc.n[2]) continue;
+                        const float weight = __fmul_rn(__fmul_rn(st.w[0][ii], st.w[1][j]), st.w[2][k]);
+                        if (!(weight > 1e-10f)) continue;
+                        const float4 g = __ldg(&V.grid_v[node_index(sc, gi, gj, gk)]);
+                        nv[0] = __fadd_rn(nv[0], __fmul_rn(weight, g.x));
+                        nv[1] = __fadd_rn(nv[1], __fmul_rn(weight, g.y));
+                        nv[2] = __fadd_rn(nv[2], __fmul_rn(weight, g.z));
+                    }
+                }
+            }
+            const float4 q3 = V.q[3 * N + p];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) x[a] = __fadd_rn(x[a], __fmul_rn(nv[a], sc.dt));
+            V.q[p] = make_float4(x[0], x[1], x[2], q0.w);
+            V.q[3 * N + p] = make_float4(nv[0], nv[1], nv[2], q3.w);
+        }
+        // key of the new position for the next step's sort
+        int so[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float u;
+            so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+        }
+        V.keys[p] = cell_key(sc, so);
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+// ------------------------------------------------------------ pack / unpack
+__global__ void k_pack(View V, const float* __restrict__ x, const float* __restrict__ v,
+                       const float* __restrict__ C, const float* __restrict__ F, const float* __restrict__ m,
+                       const float* __restrict__ V0, const int32_t* __restrict__ mat,
+                       const uint32_t* __restrict__ order, uint32_t* __restrict__ user_of_phys,
+                       float2* __restrict__ mV_out, int32_t* __restrict__ mat_out) {
+    const int64_t N = V.N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+        const uint32_t u = order[i];
+        if (u >= (uint32_t)N) {
+            atomicOr(&V.counters[CNT_FLAGS], FLAG_TILE_RANGE);
+            continue;
+        }
+        float xx[3], vv[3], CC[9], FF[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            xx[a] = x[3 * (int64_t)u + a];
+            vv[a] = v ? v[3 * (int64_t)u + a] : 0.f;
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) {
+            CC[a] = C ? C[9 * (int64_t)u + a] : 0.f;
+            FF[a] = F ? F[9 * (int64_t)u + a] : ((a % 4 == 0) ? 1.f : 0.f);
+        }
+        float4 o0, o1, o2, o3, o4, o5;
+        pack_xF(xx, FF, o0, o1, o2);
+        pack_vC(vv, CC, o3, o4, o5);
+        V.q[i] = o0;
+        V.q[N + i] = o1;
+        V.q[2 * N + i] = o2;
+        V.q[3 * N + i] = o3;
+        V.q[4 * N + i] = o4;
+        V.q[5 * N + i] = o5;
+        mV_out[i] = make_float2(m[u], V0 ? V0[u] : 0.f);
+        if (mat_out) {
+            int32_t mid = mat ? mat[u] : 0;
+            if (mid < 0 || mid >= V.M) {  // invalid material id: use 0 and report
+                atomicOr(&V.counters[CNT_FLAGS], FLAG_BAD_MATERIAL);
+                mid = 0;
+            }
+            mat_out[i] = mid;
+        }
+        user_of_phys[i] = u;
+    }
+}
+
+__global__ void k_unpack(View V, const uint32_t* __restrict__ user_of_phys, float* __restrict__ x,
+                         float* __restrict__ v, float* __restrict__ C, float* __restrict__ F) {
+    const int64_t N = V.N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+        const int64_t u = user_of_phys[i];
+        if (u >= N) continue;
+        float xx[3], FF[9], vv[3], CC[9];
+        unpack_xF(V.q[i], V.q[N + i], V.q[2 * N + i], xx, FF);
+        unpack_vC(V.q[3 * N + i], V.q[4 * N + i], V.q[5 * N + i], vv, CC);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (x) x[3 * u + a] = xx[a];
+            if (v) v[3 * u + a] = vv[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) {
+            if (C) C[9 * u + a] = CC[a];
+            if (F) F[9 * u + a] = FF[a];
+        }
+    }
+}
+
+__global__ void k_grid_download(View V, SceneDev sc, float* __restrict__ mass, float* __restrict__ vel) {
+    const int64_t nodes = (int64_t)sc.n[0] * sc.n[1] * sc.n[2];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; li < nodes; li += stride) {
+        const int i = (int)(li % sc.n[0]);
+        const int j = (int)((li / sc.n[0]) % sc.n[1]);
+        const int k = (int)(li / ((int64_t)sc.n[0] * sc.n[1]));
+        const int t = ((k >> 2) * sc.nt[1] + (j >> 2)) * sc.nt[0] + (i >> 2);
+        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (V.tile_flags[sc.nt_base + t]) g = V.grid_v[node_index(sc, i, j, k)];
+        if (mass) mass[li] = g.w;
+        if (vel) {
+            vel[3 * li] = g.x;
+            vel[3 * li + 1] = g.y;
+            vel[3 * li + 2] = g.z;
+        }
+    }
+}
+
+inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    return (int)(g < cap ? g : cap);
+}
+
+}  // namespace
+
+cudaError_t launch_keys(const View& V, const PhysFlags& pf, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    if (pf.physics == PHYS_MLS)
+        k_keys<PHYS_MLS><<<grid_for(V.N, 256), 256, 0, st>>>(V);
+    else
+        k_keys<PHYS_REF><<<grid_for(V.N, 256), 256, 0, st>>>(V);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mark(const View& V, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    k_mark<<<grid_for(V.N, 256), 256, 0, st>>>(V);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    const int64_t nb = (V.N + t.ppt - 1) / t.ppt;
+    if (nb > 0x7FFFFFFF) return cudaErrorInvalidValue;
+    if (pf.physics == PHYS_MLS) {
+        if (pf.multi_mat)
+            k_p2g<PHYS_MLS, true><<<(int)nb, t.p2g_block, 0, st>>>(V, t.ppt);
+        else
+            k_p2g<PHYS_MLS, false><<<(int)nb, t.p2g_block, 0, st>>>(V, t.ppt);
+    } else {
+        k_p2g<PHYS_REF, false><<<(int)nb, t.p2g_block, 0, st>>>(V, t.ppt);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    const int tiles_per_block = t.grid_block / 64;
+    int64_t nb = ((int64_t)V.total_nt + tiles_per_block - 1) / tiles_per_block;
+    const int cap = num_sms * 8;
+    if (nb > cap) nb = cap;
+    if (nb < 1) nb = 1;
+    if (pf.physics == PHYS_MLS)
+        k_grid<PHYS_MLS><<<(int)nb, t.grid_block, 0, st>>>(V);
+    else
+        k_grid<PHYS_REF><<<(int)nb, t.grid_block, 0, st>>>(V);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
+    if (pf.physics == PHYS_MLS) {
+        if (pf.multi_mat) {
+            if (pf.has_fluid)
+                k_g2p<PHYS_MLS, true, true><<<nb, t.g2p_block, 0, st>>>(V);
+            else
+                k_g2p<PHYS_MLS, true, false><<<nb, t.g2p_block, 0, st>>>(V);
+        } else {
+            if (pf.has_fluid)
+                k_g2p<PHYS_MLS, false, true><<<nb, t.g2p_block, 0, st>>>(V);
+            else
+                k_g2p<PHYS_MLS, false, false><<<nb, t.g2p_block, 0, st>>>(V);
+        }
+    } else {
+        k_g2p<PHYS_REF, false, false><<<nb, t.g2p_block, 0, st>>>(V);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const View& V, const float* x, const float* v, const float* C, const float* F,
+                        const float* m, const float* V0, const int32_t* mat, const uint32_t* order,
+                        uint32_t* user_of_phys, float2* mV_out, int32_t* mat_out, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    k_pack<<<grid_for(V.N, 256), 256, 0, st>>>(V, x, v, C, F, m, V0, mat, order, user_of_phys, mV_out, mat_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x, float* v, float* C, float* F,
+                          cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    k_unpack<<<grid_for(V.N, 256), 256, 0, st>>>(V, user_of_phys, x, v, C, F);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid_download(const View& V, int scene, const SceneDev& sc, float* mass, float* vel,
+                                 cudaStream_t st) {
+    (void)scene;
+    const int64_t nodes = (int64_t)sc.n[0] * sc.n[1] * sc.n[2];
+    k_grid_download<<<grid_for(nodes, 256), 256, 0, st>>>(V, sc, mass, vel);
+    return cudaGetLastError();
+}
+
+}  // namespace pgmpm

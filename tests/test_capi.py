@@ -1,0 +1,118 @@
+"""The C-ABI library loads, exports every entry point of include/pgmpm.h and
+its structs match the ctypes mirror (CPU only: no compute calls)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pgmpm.h")
+
+
+def header_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n.startswith(("pgmpm_", "launch_"))))
+
+
+def test_library_exports_every_header_symbol(built_lib):
+    names = header_functions()
+    assert "pgmpm_create" in names and "launch_mpm_timestep_forward" in names
+    L = ctypes.CDLL(built_lib)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", built_lib], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if " T " in l)
+    assert set(names) <= exported
+    # nothing but the C entry points is exported
+    extra = [e for e in exported if not e.startswith(("pgmpm_", "launch_")) and not e.startswith("_")]
+    assert not extra, extra
+
+
+def test_ctypes_mirror_covers_header(built_lib):
+    from physgrad_b200 import _capi
+
+    assert set(header_functions()) == set(_capi.SIGNATURES)
+
+
+def test_struct_layout_matches_c(tmp_path):
+    """sizeof/offsetof of the C structs == the ctypes mirror."""
+    from physgrad_b200 import _capi as C
+
+    prog = tmp_path / "layout.c"
+    prog.write_text(r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "pgmpm.h"
+int main(void){
+ printf("%zu %zu %zu %zu\n", sizeof(pgmpm_scene_desc), offsetof(pgmpm_scene_desc, dx), offsetof(pgmpm_scene_desc, gravity), offsetof(pgmpm_scene_desc, dt));
+ printf("%zu %zu\n", sizeof(pgmpm_material), offsetof(pgmpm_material, density));
+ printf("%zu %zu %zu\n", sizeof(pgmpm_metrics), offsetof(pgmpm_metrics, p2g_block), offsetof(pgmpm_metrics, g2p_ms));
+ return 0;}
+''')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    got = [int(g) for g in got]
+    exp = [ctypes.sizeof(C.SceneDesc), C.SceneDesc.dx.offset, C.SceneDesc.gravity.offset, C.SceneDesc.dt.offset,
+           ctypes.sizeof(C.Material), C.Material.density.offset,
+           ctypes.sizeof(C.Metrics), C.Metrics.p2g_block.offset, C.Metrics.g2p_ms.offset]
+    assert got == exp
+
+
+def test_header_compiles_as_c_and_cxx(tmp_path):
+    for comp, ext in (("gcc", "c"), ("g++", "cpp")):
+        f = tmp_path / f"h.{ext}"
+        f.write_text('#include "pgmpm.h"\nint main(void){ return PGMPM_ABI_VERSION == 1 ? 0 : 1; }\n')
+        subprocess.run([comp, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(f), "-o",
+                        str(tmp_path / f"h_{ext}")], check=True)
+
+
+def test_errors_without_gpu_are_reported_not_raised(built_lib):
+    """On a machine without a GPU, create() fails with a status and message."""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("machine has a GPU")
+    except Exception:
+        pass
+    from physgrad_b200 import _capi as C
+    from physgrad_b200.solver import Scene, Simulator, createElasticMaterial
+
+    with pytest.raises(C.PGMPMError) as ei:
+        Simulator([Scene()], [10], [createElasticMaterial(1000, 1e4, 0.3)])
+    assert ei.value.code in (C.PGMPM_ERR_CUDA, C.PGMPM_ERR_ARG)
+    assert "device" in str(ei.value).lower() or "cuda" in str(ei.value).lower()
+
+
+def test_argument_validation_without_gpu(built_lib):
+    from physgrad_b200 import _capi as C
+
+    L = C.lib()
+    h = ctypes.c_void_p()
+    assert L.pgmpm_create(None, 0, None, None, 0, 0, ctypes.byref(h)) == C.PGMPM_ERR_ARG
+    assert b"scene" in L.pgmpm_last_error()
+    assert L.pgmpm_step(None, 1, None) == C.PGMPM_ERR_ARG
+    assert L.pgmpm_radix_sort_pairs(None, None, None, None, 10, 8, None) == C.PGMPM_ERR_ARG
+    assert L.pgmpm_abi_version() == 1
+
+
+def test_workloads_are_seeded_and_shaped():
+    from physgrad_b200 import workloads as W
+
+    s1, c1, m1, st1, meta1 = W.config1(seed=0)
+    s1b, _, _, st1b, _ = W.config1(seed=0)
+    assert np.array_equal(st1["x"], st1b["x"])
+    assert st1["x"].shape == (32768, 3) and c1 == [32768] and s1[0].n == (64, 64, 64)
+    assert st1["x"].min() >= 0.3 and st1["x"].max() <= 0.6
+    sc, counts, mats, st, meta = W.config4(seed=0)
+    assert len(sc) == 64 and len(counts) == 64 and len(mats) == 64
+    assert min(counts) >= 4096 and max(counts) <= 262144
+    assert all(s.n[0] == (32 if c < 16384 else 64 if c < 131072 else 128) for s, c in zip(sc, counts))
+    assert st["x"].shape[0] == sum(counts)
+    assert np.array_equal(np.unique(st["mat"]), np.arange(64))

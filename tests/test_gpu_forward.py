@@ -1,0 +1,345 @@
+"""GPU parity of the forward step through the C-ABI (libpgmpm.so).
+
+Tolerances (FP32 kernels vs checkers):
+  * integer work (cell keys, radix sort, physical order): bit-exact;
+  * REF_COMPAT vs the reference's own CPU solver: max |err| / max |ref| <= 1e-4
+    on positions and velocities (F is the identity in both);
+  * MLS vs the FP64 oracle: positions max abs err <= 2e-5 (domain size 1),
+    velocities <= 1e-3 * max|v| + 1e-5, F <= 2e-4 absolute.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _sim(pg, scenes, counts, mats, st, **tune):
+    sim = pg.Simulator(scenes, counts, mats)
+    if tune:
+        sim.set_tuning(**tune)
+    sim.upload(st["x"], st["v"], st.get("C").reshape(-1, 9) if st.get("C") is not None else None,
+               st.get("F").reshape(-1, 9) if st.get("F") is not None else None, st["m"], st["V0"], st.get("mat"))
+    return sim
+
+
+def _oracle_state(st):
+    N = st["x"].shape[0]
+    d = dict(x=st["x"].astype(np.float64), v=st["v"].astype(np.float64),
+             C=st["C"].reshape(N, 9).astype(np.float64), F=st["F"].reshape(N, 9).astype(np.float64),
+             m=st["m"].astype(np.float64), V0=st["V0"].astype(np.float64))
+    if st.get("mat") is not None:
+        d["mat"] = st["mat"]
+    return d
+
+
+def _oracle_scene(oracle, s):
+    return oracle.make_scene(tuple(s.n), s.dx, s.dt, gravity=tuple(s.gravity), origin=tuple(s.origin),
+                             physics=s.physics, boundary=s.boundary, bthick=s.boundary_thickness)
+
+
+# ------------------------------------------------------------------ sort
+@pytest.mark.parametrize("n,bits,kind", [(0, 8, "rand"), (1, 8, "rand"), (2047, 11, "rand"), (2048, 21, "rand"),
+                                         (2049, 24, "rand"), (100003, 21, "nearly"), (65536, 9, "equal"),
+                                         (1 << 20, 32, "rand"), (300001, 17, "dup")])
+def test_radix_sort_bit_exact(gpu, oracle, n, bits, kind):
+    import torch
+
+    rng = np.random.default_rng(n + bits)
+    if kind == "rand":
+        k = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+    elif kind == "nearly":
+        k = np.sort(rng.integers(0, 1 << bits, n)).astype(np.uint32)
+        sw = rng.integers(0, n - 1, n // 100)
+        k[sw], k[sw + 1] = k[sw + 1].copy(), k[sw].copy()
+    elif kind == "equal":
+        k = np.full(n, 7, np.uint32)
+    else:
+        k = rng.integers(0, 50, n).astype(np.uint32)
+    vals = rng.integers(0, 1 << 31, n).astype(np.uint32)
+    kt = torch.from_numpy(k.view(np.int32)).cuda()
+    vt = torch.from_numpy(vals.view(np.int32)).cuda()
+    ko, vo = gpu.radix_sort_pairs(kt, vt, key_bits=bits)
+    ek, ev = oracle.stable_sort(k, vals)
+    assert np.array_equal(ko.cpu().numpy().view(np.uint32), ek)
+    assert np.array_equal(vo.cpu().numpy().view(np.uint32), ev)
+
+
+def test_radix_sort_golden_fixture(gpu):
+    import torch
+
+    g = np.load(os.path.join(GOLDEN, "sort_small.npz"))
+    kt = torch.from_numpy(g["keys"].view(np.int32)).cuda()
+    ko, vo = gpu.radix_sort_pairs(kt, None, key_bits=12)
+    assert np.array_equal(ko.cpu().numpy().view(np.uint32), g["sorted_keys"])
+    assert np.array_equal(vo.cpu().numpy().view(np.uint32), g["order"])
+
+
+def test_upload_order_and_step_sort_bit_exact(gpu, oracle):
+    from physgrad_b200 import _capi as C
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=20000, n=32, v_sigma=0.5, seed=3)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    osc = _oracle_scene(oracle, scenes[0])
+    keys_user = oracle.keys(osc, st["x"])
+    ek, ev = oracle.stable_sort(keys_user)
+    assert np.array_equal(sim.get_array(C.ARRAY_USER_INDEX), ev)
+    assert np.array_equal(sim.get_array(C.ARRAY_KEYS), ek)
+    for _ in range(3):
+        keys_before = sim.get_array(C.ARRAY_KEYS)
+        sim.step(1)
+        sk, so = oracle.stable_sort(keys_before)
+        assert np.array_equal(sim.get_array(C.ARRAY_SORTED_KEYS), sk)
+        assert np.array_equal(sim.get_array(C.ARRAY_SORTED_ORDER), so)
+        # keys written by G2P == keys of the new positions (physical order)
+        x_user = sim.download()["x"]
+        x_phys = x_user[sim.get_array(C.ARRAY_USER_INDEX)]
+        assert np.array_equal(sim.get_array(C.ARRAY_KEYS), oracle.keys(osc, x_phys))
+
+
+# ------------------------------------------------------------- REF_COMPAT
+def test_ref_compat_golden_fixture(gpu):
+    """GPU REF_COMPAT vs the reference's own CPU solver output (fixture)."""
+    with open(os.path.join(GOLDEN, "ref_cpu_small.json")) as f:
+        meta = json.load(f)
+    g = np.load(os.path.join(GOLDEN, "ref_cpu_small.npz"))
+    s = gpu.RefCompatSolver(tuple(meta["n"]), np.float32(meta["dx"]), (0, 0, 0),
+                            gpu.RefCompatSolver.SimulationParams(np.float32(meta["dt"]), tuple(meta["gravity"])))
+    s.addParticles(g["x0"], g["v0"], g["m"], g["vol"])
+    s.step(meta["steps"])
+    out = s.getParticles()
+    ex = np.abs(out["x"] - g["x"]).max() / np.abs(g["x"]).max()
+    ev = np.abs(out["v"] - g["v"]).max() / np.abs(g["v"]).max()
+    assert ex <= 1e-4 and ev <= 1e-4, (ex, ev)
+    gr = s.getGrid()
+    em = np.abs(gr["mass"] - g["grid_m"]).max() / np.abs(g["grid_m"]).max()
+    egv = np.abs(gr["velocity"] - g["grid_v"]).max() / np.abs(g["grid_v"]).max()
+    assert em <= 1e-4 and egv <= 1e-4, (em, egv)
+    assert np.array_equal(out["F"], np.tile(np.eye(3, dtype=np.float32), (g["x0"].shape[0], 1, 1)))
+
+
+def test_ref_compat_config1_vs_reference_live(gpu, oracle):
+    """Config-1 geometry, 200 steps: GPU vs the reference's CPU solver."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, meta = W.elastic_cube(physics=1, boundary=0)
+    dx = np.float32(scenes[0].dx)
+    r = oracle.ref_run(st["x"], st["v"], st["m"], st["V0"], (64, 64, 64), dx, np.float32(1e-4),
+                       (0.0, np.float32(-9.8), 0.0), 200)
+    s = gpu.RefCompatSolver((64, 64, 64), dx, (0, 0, 0), gpu.RefCompatSolver.SimulationParams(1e-4, (0.0, -9.8, 0.0)))
+    s.addParticles(st["x"], st["v"], st["m"], st["V0"])
+    s.step(200)
+    out = s.getParticles()
+    ex = np.abs(out["x"] - r["x"]).max() / np.abs(r["x"]).max()
+    ev = np.abs(out["v"] - r["v"]).max() / np.abs(r["v"]).max()
+    print(f"REF_COMPAT config1 200 steps: rel err x {ex:.3e} v {ev:.3e}")
+    assert ex <= 1e-4 and ev <= 1e-4, (ex, ev)
+
+
+# -------------------------------------------------------------------- MLS
+def _mls_errors(out, ref):
+    ex = np.abs(out["x"] - ref["x"]).max()
+    ev = np.abs(out["v"] - ref["v"]).max()
+    vmax = np.abs(ref["v"]).max()
+    eF = np.abs(out["F"].reshape(-1, 9) - ref["F"].reshape(-1, 9)).max()
+    eC = np.abs(out["C"].reshape(-1, 9) - ref["C"].reshape(-1, 9)).max()
+    return ex, ev, vmax, eF, eC
+
+
+def _assert_mls(out, ref, label):
+    ex, ev, vmax, eF, eC = _mls_errors(out, ref)
+    print(f"{label}: |dx| {ex:.2e} |dv| {ev:.2e} (vmax {vmax:.2e}) |dF| {eF:.2e} |dC| {eC:.2e}")
+    assert ex <= 2e-5, ex
+    assert ev <= 1e-3 * vmax + 1e-5, (ev, vmax)
+    assert eF <= 2e-4, eF
+
+
+def test_mls_golden_fixture(gpu):
+    """Three materials (FCR, neo-Hookean, EOS), sticky walls, 20 steps vs FP64."""
+    with open(os.path.join(GOLDEN, "mls_small.json")) as f:
+        meta = json.load(f)
+    g = np.load(os.path.join(GOLDEN, "mls_small.npz"))
+    N = g["x0"].shape[0]
+    scene = gpu.Scene(tuple(meta["n"]), meta["dx"], meta["dt"], tuple(meta["gravity"]), (0, 0, 0), 0, 1, 3)
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3), gpu.createElasticMaterial(1000, 3e4, 0.25, 1),
+            gpu.createFluidMaterial(1000, 1e4)]
+    V0 = np.full(N, (meta["dx"] / 2) ** 3, np.float32)
+    st = dict(x=g["x0"], v=g["v0"], C=np.zeros((N, 9), np.float32), F=np.tile(np.eye(3, dtype=np.float32).ravel(), (N, 1)),
+              m=(1000 * V0).astype(np.float32), V0=V0, mat=g["mat"])
+    sim = _sim(gpu, [scene], [N], mats, st)
+    sim.step(meta["steps"])
+    out = sim.download()
+    _assert_mls(out, {"x": g["x"], "v": g["v"], "F": g["F"], "C": g["C"]}, "mls_small")
+
+
+@pytest.mark.parametrize("case", ["cfg1", "cfg3_small", "cfg2_small", "separate"])
+def test_mls_vs_fp64_oracle(gpu, oracle, case):
+    from physgrad_b200 import workloads as W
+
+    if case == "cfg1":
+        scenes, counts, mats, st, meta = W.config1()
+        steps = 200
+    elif case == "cfg3_small":
+        scenes, counts, mats, st, meta = W.elastic_cube(n_particles=65536, n=64, v_sigma=0.1, seed=1)
+        steps = 64
+    elif case == "cfg2_small":
+        scenes, counts, mats, st, meta = W.two_material_drop(n_particles=131072, n=64, seed=2)
+        steps = 100
+    else:
+        scenes, counts, mats, st, meta = W.elastic_cube(n_particles=8192, n=32, v_sigma=2.0, seed=4,
+                                                        boundary=3, lo=0.1, hi=0.9)
+        steps = 40
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(steps)
+    out = sim.download()
+    osc = _oracle_scene(oracle, scenes[0])
+    omats = oracle.make_materials([(int(m.model), float(m.youngs_modulus), float(m.poisson_ratio)) for m in mats])
+    ref = oracle.run(osc, omats, _oracle_state(st), steps, prec=64)
+    _assert_mls(out, ref, case)
+    assert sim.status() & 2 == 0
+
+
+def test_mls_grid_download_matches_oracle(gpu, oracle):
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=4096, n=32, v_sigma=0.3, seed=8)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(5)
+    m, v = sim.grid(0)
+    osc = _oracle_scene(oracle, scenes[0])
+    omats = oracle.make_materials([(0, 1e4, 0.3)])
+    ref = oracle.run(osc, omats, _oracle_state(st), 5, prec=64, want_grid=True)
+    assert np.abs(m - ref["grid_m"]).max() <= 1e-5 * ref["grid_m"].max()
+    assert np.abs(v - ref["grid_v"]).max() <= 1e-4 * np.abs(ref["grid_v"]).max() + 1e-6
+
+
+# --------------------------------------------------------- batching / misc
+def test_batched_scenes_equal_single_scenes(gpu):
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.batched_scenes(n_scenes=5, lo=500, hi=20000, seed=6, v_sigma=0.3)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(20)
+    out = sim.download()
+    off = 0
+    for s, c in enumerate(counts):
+        sl = slice(off, off + c)
+        one = {k: (None if v is None else v[sl]) for k, v in st.items()}
+        one["mat"] = None
+        sim1 = _sim(gpu, [scenes[s]], [c], [mats[s]], one)
+        sim1.step(20)
+        o1 = sim1.download()
+        assert np.abs(out["x"][sl] - o1["x"]).max() <= 1e-6
+        assert np.abs(out["v"][sl] - o1["v"]).max() <= 1e-4 * (np.abs(o1["v"]).max() + 1e-3)
+        assert np.abs(out["F"][sl] - o1["F"]).max() <= 1e-5
+        off += c
+
+
+def test_graph_and_eager_agree(gpu):
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=30000, n=64, v_sigma=0.2, seed=9)
+    a = _sim(gpu, scenes, counts, mats, st, use_graph=1)
+    b = _sim(gpu, scenes, counts, mats, st, use_graph=0)
+    a.step(30)
+    b.step(30)
+    oa, ob = a.download(), b.download()
+    assert np.abs(oa["x"] - ob["x"]).max() <= 1e-6
+    assert np.abs(oa["F"] - ob["F"]).max() <= 1e-5
+
+
+def test_autotune_restores_state(gpu):
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=50000, n=64, v_sigma=0.2, seed=10)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(3)
+    before = sim.download()
+    best = sim.autotune(reps=2)
+    after = sim.download()
+    for k in ("x", "v", "C", "F"):
+        assert np.array_equal(before[k], after[k])
+    assert best["p2g_block"] in (128, 256, 512) and best["ppt"] >= 256
+    ref = _sim(gpu, scenes, counts, mats, st)
+    ref.step(5)
+    sim.step(2)
+    assert np.abs(sim.download()["x"] - ref.download()["x"]).max() <= 1e-6
+
+
+def test_empty_scene_and_single_particle(gpu):
+    s = gpu.Scene((16, 16, 16), 1 / 16, 1e-4)
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3)]
+    sim = gpu.Simulator([s], [0], mats)
+    sim.upload(np.zeros((0, 3), np.float32), None, None, None, np.zeros(0, np.float32))
+    sim.step(3)
+    assert sim.download()["x"].shape == (0, 3)
+    one = gpu.Simulator([s], [1], mats)
+    one.upload(np.array([[0.5, 0.5, 0.5]], np.float32), np.zeros((1, 3), np.float32), None, None,
+               np.array([1e-3], np.float32), np.array([1e-6], np.float32))
+    one.step(10)
+    out = one.download()
+    assert abs(out["v"][0, 1] - (-9.8 * 10 * 1e-4)) < 1e-6
+    # mixed sizes in one batch, one scene empty
+    b = gpu.Simulator([s, s, s], [5, 0, 7], mats)
+    x = np.random.default_rng(0).uniform(0.4, 0.6, (12, 3)).astype(np.float32)
+    b.upload(x, None, None, None, np.full(12, 1e-3, np.float32), np.full(12, 1e-6, np.float32))
+    b.step(2)
+    assert np.isfinite(b.download()["x"]).all()
+
+
+def test_escape_and_nonfinite_flags(gpu):
+    from physgrad_b200 import _capi as C
+
+    s = gpu.Scene((16, 16, 16), 1 / 16, 1e-3, boundary=C.BC_NONE)
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3)]
+    sim = gpu.Simulator([s], [2], mats)
+    x = np.array([[0.5, 0.5, 0.5], [0.5, 0.5, 0.5]], np.float32)
+    v = np.array([[0, 0, 0], [0, 0, 300.0]], np.float32)  # leaves the grid in a few steps
+    sim.upload(x, v, None, None, np.full(2, 1e-3, np.float32), np.full(2, 1e-6, np.float32))
+    sim.step(30)
+    f = sim.status()
+    assert f & C.FLAG_ESCAPE
+    assert np.isfinite(sim.download()["x"]).all()
+    nan = gpu.Simulator([s], [2], mats)
+    x[1, 0] = np.nan
+    nan.upload(x, None, None, None, np.full(2, 1e-3, np.float32), np.full(2, 1e-6, np.float32))
+    nan.step(1)
+    assert nan.status() & C.FLAG_NONFINITE
+
+
+def test_invalid_material_rejected(gpu):
+    from physgrad_b200 import _capi as C
+
+    s = gpu.Scene((16, 16, 16), 1 / 16, 1e-4)
+    bad = gpu.MaterialParameters(1000, 1e4, 0.3, gpu.MaterialType.SAND)
+    with pytest.raises(C.PGMPMError) as ei:
+        gpu.Simulator([s], [1], [bad])
+    assert ei.value.code == C.PGMPM_ERR_UNSUPPORTED
+
+
+def test_reference_shaped_solver_api(gpu):
+    cfg = gpu.MPMSolverConfig(grid_dimensions=(32, 32, 32), grid_spacing=(1 / 32,) * 3, time_step=1e-4,
+                              gravity=(0, -9.8, 0), max_particles=1000)
+    solver = gpu.MPMSolver(cfg)
+    rng = np.random.default_rng(0)
+    solver.addParticles(rng.uniform(0.4, 0.6, (500, 3)), np.zeros((500, 3)), np.full(500, 1e-3))
+    with pytest.raises(RuntimeError):
+        solver.step()
+    with pytest.raises(RuntimeError):
+        solver.addParticles(np.zeros((600, 3)), np.zeros((600, 3)), np.ones(600))
+    solver.initialize()
+    solver.step()
+    solver.run(9)
+    assert solver.getCurrentStep() == 10
+    p = solver.getParticles()
+    assert p["x"].shape == (500, 3) and np.isfinite(p["x"]).all()
+    g = solver.getGrid()
+    assert g["mass"].sum() > 0
+    assert solver.getMetrics()["total_steps"] == 10

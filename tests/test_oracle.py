@@ -1,0 +1,137 @@
+"""The CPU oracle, pinned before it is trusted (CPU only)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load_golden(name):
+    with open(os.path.join(GOLDEN, name + ".json")) as f:
+        meta = json.load(f)
+    arrs = np.load(os.path.join(GOLDEN, name + ".npz"))
+    return meta, arrs
+
+
+def test_ref_compat_matches_reference_golden(oracle):
+    """Oracle REF_COMPAT (float) is bit-identical to the reference's own CPU
+    solver (src/material_point_method.h:479-666) on the committed fixture."""
+    meta, g = _load_golden("ref_cpu_small")
+    n = tuple(meta["n"])
+    sc = oracle.make_scene(n, np.float32(meta["dx"]), np.float32(meta["dt"]),
+                           gravity=tuple(np.float32(a) for a in meta["gravity"]), physics=oracle.REF_COMPAT,
+                           boundary=oracle.BC_NONE)
+    mats = oracle.make_materials([(0, 1e4, 0.3)])
+    N = g["x0"].shape[0]
+    st = dict(x=g["x0"].astype(np.float64), v=g["v0"].astype(np.float64), C=np.zeros((N, 9)),
+              F=np.tile(np.eye(3).ravel(), (N, 1)), m=g["m"].astype(np.float64), V0=g["vol"].astype(np.float64))
+    out = oracle.run(sc, mats, st, meta["steps"], prec=32, want_grid=True)
+    assert np.array_equal(out["x"].astype(np.float32), g["x"])
+    assert np.array_equal(out["v"].astype(np.float32), g["v"])
+    assert np.array_equal(out["grid_m"].astype(np.float32), g["grid_m"])
+    assert np.array_equal(out["grid_v"].astype(np.float32), g["grid_v"])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref",
+                                                    "libref_mpm.so")), reason="reference build absent")
+def test_ref_compat_matches_reference_live(oracle):
+    """Same pin, live against oracle/_ref on config-1 geometry (20 steps)."""
+    rng = np.random.default_rng(7)
+    N, n, dx = 32768, (64, 64, 64), np.float32(1 / 64)
+    x = rng.uniform(0.3, 0.6, (N, 3)).astype(np.float32)
+    v = rng.normal(0, 0.05, (N, 3)).astype(np.float32)
+    vol = np.full(N, dx ** 3 / 8, np.float32)
+    m = (1000 * vol).astype(np.float32)
+    r = oracle.ref_run(x, v, m, vol, n, dx, np.float32(1e-4), (0, np.float32(-9.8), 0), 20)
+    sc = oracle.make_scene(n, dx, np.float32(1e-4), gravity=(0, np.float32(-9.8), 0), physics=oracle.REF_COMPAT,
+                           boundary=oracle.BC_NONE)
+    st = dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)),
+              F=np.tile(np.eye(3).ravel(), (N, 1)), m=m.astype(np.float64), V0=vol.astype(np.float64))
+    o = oracle.run(sc, oracle.make_materials([(0, 1e4, 0.3)]), st, 20, prec=32)
+    assert np.array_equal(o["x"].astype(np.float32), r["x"])
+    assert np.array_equal(o["v"].astype(np.float32), r["v"])
+
+
+def test_stable_sort_and_keys(oracle):
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 50, 5000).astype(np.uint32)
+    ok, ov = oracle.stable_sort(keys)
+    ref = np.argsort(keys, kind="stable")
+    assert np.array_equal(ov, ref.astype(np.uint32))
+    assert np.array_equal(ok, keys[ref])
+    # keys: stencil origin floor(u - 0.5) clamped, tile-major
+    sc = oracle.make_scene((16, 16, 16), 1 / 16, 1e-4)
+    x = np.array([[0.5, 0.5, 0.5], [0.0, 0.0, 0.0], [0.99, 0.99, 0.99], [0.2, 0.3, 0.4]], np.float32)
+    k = oracle.keys(sc, x)
+    def key(s):
+        ct = ((16 - 3) >> 2) + 1
+        t = ((s[2] >> 2) * ct + (s[1] >> 2)) * ct + (s[0] >> 2)
+        return t * 64 + (s[2] & 3) * 16 + (s[1] & 3) * 4 + (s[0] & 3)
+    exp = []
+    for p in x:
+        s = [int(min(max(np.floor(np.float32(np.float32(a) / np.float32(1 / 16)) - np.float32(0.5)), 0), 13)) for a in p]
+        exp.append(key(s))
+    assert k.tolist() == exp
+
+
+def _small_state(rng, N, dx, spread=0.05):
+    x = rng.uniform(0.35, 0.6, (N, 3))
+    return dict(x=x, v=rng.normal(0, 0.3, (N, 3)), C=rng.normal(0, 0.5, (N, 9)),
+                F=np.tile(np.eye(3).ravel(), (N, 1)) + rng.normal(0, spread, (N, 9)),
+                m=np.full(N, 1000 * (dx / 2) ** 3), V0=np.full(N, (dx / 2) ** 3), mat=(np.arange(N) % 3).astype(np.int32))
+
+
+@pytest.mark.parametrize("bc", [1, 2, 3])
+def test_oracle_adjoint_matches_central_differences(oracle, bc):
+    """FP64 oracle adjoint vs central FD, three materials, each wall type."""
+    rng = np.random.default_rng(11 + bc)
+    N, dx, steps = 200, 1 / 16, 3
+    st = _small_state(rng, N, dx)
+    sc = oracle.make_scene((16, 16, 16), dx, 2e-3, physics=oracle.MLS, boundary=bc, bthick=3)
+    mlist = [(oracle.FIXED_COROTATED, 1e4, 0.3), (oracle.NEO_HOOKEAN, 3e4, 0.25), (oracle.EOS_FLUID, 1e4, 0.0)]
+    mats = oracle.make_materials(mlist)
+    tgt = np.array([0.5, 0.3, 0.5])
+
+    def loss(s, mt=mats):
+        o = oracle.run(sc, mt, s, steps, prec=64)
+        return ((o["x"].mean(0) - tgt) ** 2).sum() + 0.1 * (o["v"] ** 2).sum() + 0.01 * (o["F"] ** 2).sum()
+
+    o = oracle.run(sc, mats, st, steps, prec=64)
+    g = oracle.adjoint(sc, mats, st, steps, dict(x=np.tile(2 * (o["x"].mean(0) - tgt) / N, (N, 1)), v=0.2 * o["v"],
+                                                 F=0.02 * o["F"].reshape(N, 9)))
+    eps = 1e-6
+    num, ana = [], []
+    for key, cols in (("x", 3), ("v", 3), ("C", 9), ("F", 9)):
+        for _ in range(4):
+            i, j = rng.integers(N), rng.integers(cols)
+            sp = {k: (a.copy() if isinstance(a, np.ndarray) else a) for k, a in st.items()}
+            sm = {k: (a.copy() if isinstance(a, np.ndarray) else a) for k, a in st.items()}
+            sp[key] = sp[key].reshape(N, cols)
+            sm[key] = sm[key].reshape(N, cols)
+            sp[key][i, j] += eps
+            sm[key][i, j] -= eps
+            num.append((loss(sp) - loss(sm)) / (2 * eps))
+            ana.append(g[key].reshape(N, -1)[i, j])
+    for mi in range(3):
+        hi = [(a, b + (1e-2 if k == mi else 0), c) for k, (a, b, c) in enumerate(mlist)]
+        lo = [(a, b - (1e-2 if k == mi else 0), c) for k, (a, b, c) in enumerate(mlist)]
+        num.append((loss(st, oracle.make_materials(hi)) - loss(st, oracle.make_materials(lo))) / 2e-2)
+        ana.append(g["E"][mi])
+    num, ana = np.array(num), np.array(ana)
+    # relative to the largest gradient entry of the set (tolerance 1e-4)
+    assert np.abs(num - ana).max() <= 1e-4 * np.abs(num).max() + 1e-10
+
+
+def test_oracle_fp32_mirror_close_to_fp64(oracle):
+    rng = np.random.default_rng(5)
+    N, dx = 1000, 1 / 32
+    st = _small_state(rng, N, dx, spread=0.02)
+    st["mat"] = np.zeros(N, np.int32)
+    sc = oracle.make_scene((32, 32, 32), dx, 1e-4)
+    mats = oracle.make_materials([(oracle.FIXED_COROTATED, 1e4, 0.3)])
+    a = oracle.run(sc, mats, st, 10, prec=64)
+    b = oracle.run(sc, mats, st, 10, prec=32)
+    assert np.abs(a["x"] - b["x"]).max() < 1e-6
+    assert np.abs(a["F"] - b["F"]).max() < 1e-5
