@@ -132,6 +132,7 @@ typedef struct {
     double particle_steps_per_s;
     double sort_ms, p2g_ms, grid_ms, g2p_ms; /* per-kernel device ms, last profiled step */
     int32_t p2g_block, p2g_ppt, g2p_block, graph_enabled;
+    int32_t p2g_variant, g2p_variant, p2g_tiles_per_sm, g2p_tiles_per_sm;
 } pgmpm_metrics;
 
 /* ---- lifecycle ---------------------------------------------------------- */
@@ -180,6 +181,13 @@ PGMPM_API int pgmpm_check_status(pgmpm_solver s, uint32_t* flags, void* stream);
 /* p2g_block, g2p_block: threads per block; ppt: particles per P2G chunk.
  * 0 keeps the current value.  use_graph: capture each step as a CUDA graph. */
 PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p_block, int32_t use_graph);
+/* Kernel variants.  p2g_variant 0: per-cell register accumulation over
+ * occupied 4^3 cell tiles (persistent, p2g_tiles_per_sm blocks per SM);
+ * 1: per-particle shared-memory atomics over chunks of ppt particles.
+ * g2p_variant 0: tile-staged gather (g2p_tiles_per_sm blocks per SM);
+ * 1: direct gather, one thread per particle.  Negative keeps a value. */
+PGMPM_API int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant,
+                                        int32_t p2g_tiles_per_sm, int32_t g2p_tiles_per_sm);
 /* Time candidate (block, ppt) settings on the solver's own state (restored
  * afterwards) and keep the fastest. */
 PGMPM_API int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream);

@@ -419,8 +419,12 @@ template <class T> inline void mls_stencil(const oracle_scene& sc, const Grid& g
         if (b < 0) b = 0;
         if (b > T(g.n[a] - 3)) b = T(g.n[a] - 3);
         s.base[a] = (int)b;
-        s.f[a] = u - b;
+        // f clamped to the support: an escaped particle transfers as if at
+        // the wall (zero weight derivative there)
+        T f = u - b;
+        s.f[a] = f < T(0.5) ? T(0.5) : (f > T(1.5) ? T(1.5) : f);
         mls_w(s.f[a], s.w[a], s.dw[a]);
+        if (f < T(0.5) || f > T(1.5)) s.dw[a][0] = s.dw[a][1] = s.dw[a][2] = T(0);
     }
 }
 

@@ -90,6 +90,10 @@ class Metrics(ctypes.Structure):
         ("p2g_ppt", ctypes.c_int32),
         ("g2p_block", ctypes.c_int32),
         ("graph_enabled", ctypes.c_int32),
+        ("p2g_variant", ctypes.c_int32),
+        ("g2p_variant", ctypes.c_int32),
+        ("p2g_tiles_per_sm", ctypes.c_int32),
+        ("g2p_tiles_per_sm", ctypes.c_int32),
     ]
 
 
@@ -112,6 +116,7 @@ SIGNATURES = {
     "pgmpm_check_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint32), _vp]),
     "pgmpm_set_tuning": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
     "pgmpm_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
+    "pgmpm_set_kernel_variants": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
     "pgmpm_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "pgmpm_get_metrics": (ctypes.c_int, [_vp, ctypes.POINTER(Metrics)]),
     "pgmpm_forward_checkpointed": (ctypes.c_int, [_vp, _i32, _i32, _vp]),

@@ -88,7 +88,7 @@ struct pgmpm_solver_s {
 
     // device buffers
     DevBuf d_scenes, d_mats, q, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
-    DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, counters, staging;
+    DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
     uint32_t* h_counters = nullptr;  // pinned
 
     // graph
@@ -123,6 +123,8 @@ struct pgmpm_solver_s {
         V.grid_vpre = nullptr;
         V.tile_flags = tile_flags.as<uint32_t>();
         V.tile_list = tile_list.as<uint32_t>();
+        V.ctile_list = ctile_list.as<uint32_t>();
+        V.ctile_range = ctile_range.as<uint2>();
         V.counters = counters.as<uint32_t>();
         V.total_ct = total_ct;
         V.total_nt = total_nt;
@@ -194,10 +196,15 @@ int material_to_dev(const pgmpm_material& m, MatDev& d) {
 cudaStream_t ST(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 int record_step(pgmpm_solver s, cudaStream_t st, bool timed) {
+    if (s->N == 0) {  // nothing to move; keep the timing events consistent
+        if (timed)
+            for (int i = 0; i < 5; ++i) CK(cudaEventRecord(s->ev[i], st));
+        return PGMPM_OK;
+    }
     View V = s->view();
     // per-step resets: active tile flags, tile count and active node count
     CK(cudaMemsetAsync(s->tile_flags.p, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
-    CK(cudaMemsetAsync(s->counters.p, 0, sizeof(uint32_t) * CNT_FLAGS, st));
+    CK(cudaMemsetAsync(s->counters.p, 0, sizeof(uint32_t) * CNT_RESET, st));
     if (timed) CK(cudaEventRecord(s->ev[0], st));
     int which = 0;
     CK(radix_sort_pairs(s->keys.as<uint32_t>(), nullptr, s->ka.as<uint32_t>(), s->va.as<uint32_t>(),
@@ -206,11 +213,11 @@ int record_step(pgmpm_solver s, cudaStream_t st, bool timed) {
     if (which != s->sort_which) return fail(PGMPM_ERR_STATE, "internal: sort buffer parity changed");
     CK(launch_mark(V, st));
     if (timed) CK(cudaEventRecord(s->ev[1], st));
-    CK(launch_p2g(V, s->pf, s->tune, st));
+    CK(launch_p2g(V, s->pf, s->tune, s->num_sms, st));
     if (timed) CK(cudaEventRecord(s->ev[2], st));
     CK(launch_grid(V, s->pf, s->tune, s->num_sms, st));
     if (timed) CK(cudaEventRecord(s->ev[3], st));
-    CK(launch_g2p(V, s->pf, s->tune, st));
+    CK(launch_g2p(V, s->pf, s->tune, s->num_sms, st));
     if (timed) CK(cudaEventRecord(s->ev[4], st));
     return PGMPM_OK;
 }
@@ -388,6 +395,8 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->grid_v, sizeof(float4) * 64 * (size_t)nt_base);
     AL(s->tile_flags, sizeof(uint32_t) * (size_t)nt_base);
     AL(s->tile_list, sizeof(uint32_t) * (size_t)nt_base);
+    AL(s->ctile_list, sizeof(uint32_t) * (size_t)ct_base);
+    AL(s->ctile_range, sizeof(uint2) * (size_t)ct_base);
     AL(s->counters, sizeof(uint32_t) * CNT_WORDS);
 #undef AL
     if (e == cudaSuccess) e = cudaMemcpy(s->d_scenes.p, s->scenes.data(), sizeof(SceneDev) * n_scenes, cudaMemcpyHostToDevice);
@@ -600,6 +609,19 @@ int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p
     return PGMPM_OK;
 }
 
+int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant, int32_t p2g_tiles_per_sm,
+                              int32_t g2p_tiles_per_sm) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (p2g_variant > 1 || g2p_variant > 1 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
+        return fail(PGMPM_ERR_ARG, "variants are 0 or 1; tiles per SM at most 16");
+    if (p2g_variant >= 0) s->tune.p2g_variant = p2g_variant;
+    if (g2p_variant >= 0) s->tune.g2p_variant = g2p_variant;
+    if (p2g_tiles_per_sm > 0) s->tune.tile_blocks_per_sm = p2g_tiles_per_sm;
+    if (g2p_tiles_per_sm > 0) s->tune.g2p_tiles_per_sm = g2p_tiles_per_sm;
+    s->drop_graph();
+    return PGMPM_OK;
+}
+
 int pgmpm_set_profiling(pgmpm_solver s, int32_t profile) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
     s->profiling = profile != 0;
@@ -612,6 +634,10 @@ int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out) {
     s->met.p2g_ppt = s->tune.ppt;
     s->met.g2p_block = s->tune.g2p_block;
     s->met.graph_enabled = s->use_graph ? 1 : 0;
+    s->met.p2g_variant = s->tune.p2g_variant;
+    s->met.g2p_variant = s->tune.g2p_variant;
+    s->met.p2g_tiles_per_sm = s->tune.tile_blocks_per_sm;
+    s->met.g2p_tiles_per_sm = s->tune.g2p_tiles_per_sm;
     *out = s->met;
     return PGMPM_OK;
 }
@@ -633,47 +659,65 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
     const bool keep_graph = s->use_graph, keep_prof = s->profiling;
     s->use_graph = false;
     s->profiling = false;
-    const int p2g_blocks[] = {128, 256, 512};
-    const int ppts[] = {256, 512, 1024, 2048, 4096};
-    const int g2p_blocks[] = {128, 256, 512};
+    // candidates: the tile kernels at several resident blocks per SM, and the
+    // chunked / direct variants over (block size, particles per chunk)
+    struct Cand {
+        int variant, block, ppt, tiles_per_sm;
+    };
+    const Cand p2g_c[] = {{0, 192, 0, 2}, {0, 192, 0, 3}, {0, 192, 0, 4}, {0, 192, 0, 6},
+                          {1, 256, 512, 0}, {1, 256, 1024, 0}, {1, 512, 2048, 0}};
+    const Cand g2p_c[] = {{0, 256, 0, 1}, {0, 256, 0, 2}, {0, 256, 0, 3},
+                          {1, 128, 0, 0}, {1, 256, 0, 0}, {1, 512, 0, 0}};
     Tuning best = keep;
     float best_p2g = 1e30f, best_g2p = 1e30f;
     View V = s->view();
-    auto time_it = [&](auto&& fn, float& ms) -> int {
+    auto time_it = [&](auto&& fn, int cursor, float& ms) -> int {
         CK(cudaEventRecord(s->ev[0], st));
-        for (int r = 0; r < reps; ++r) CK(fn());
+        for (int r = 0; r < reps; ++r) {
+            CK(cudaMemsetAsync(s->counters.as<uint32_t>() + cursor, 0, sizeof(uint32_t), st));
+            CK(fn());
+        }
         CK(cudaEventRecord(s->ev[1], st));
         CK(cudaEventSynchronize(s->ev[1]));
         CK(cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]));
         return PGMPM_OK;
     };
-    // one real step so the sorted order, tile list and grid velocity exist
+    // one real step so the sorted order, tile lists and grid velocity exist
     int rc = record_step(s, st, false);
     if (rc) return rc;
-    for (int pb : p2g_blocks)
-        for (int ppt : ppts) {
-            if (ppt < pb) continue;
-            Tuning t = keep;
-            t.p2g_block = pb;
-            t.ppt = ppt;
-            float ms = 0.f;
-            rc = time_it([&]() { return launch_p2g(V, s->pf, t, st); }, ms);
-            if (rc) return rc;
-            if (ms < best_p2g) {
-                best_p2g = ms;
-                best.p2g_block = pb;
-                best.ppt = ppt;
-            }
-        }
-    for (int gb : g2p_blocks) {
+    for (const Cand& c : p2g_c) {
         Tuning t = keep;
-        t.g2p_block = gb;
+        t.p2g_variant = c.variant;
+        if (c.variant == 0) {
+            t.tile_blocks_per_sm = c.tiles_per_sm;
+        } else {
+            t.p2g_block = c.block;
+            t.ppt = c.ppt;
+        }
         float ms = 0.f;
-        rc = time_it([&]() { return launch_g2p(V, s->pf, t, st); }, ms);
+        rc = time_it([&]() { return launch_p2g(V, s->pf, t, s->num_sms, st); }, CNT_P2G_CURSOR, ms);
+        if (rc) return rc;
+        if (ms < best_p2g) {
+            best_p2g = ms;
+            best.p2g_variant = t.p2g_variant;
+            best.tile_blocks_per_sm = t.tile_blocks_per_sm;
+            best.p2g_block = t.p2g_block;
+            best.ppt = t.ppt;
+        }
+    }
+    for (const Cand& c : g2p_c) {
+        Tuning t = best;
+        t.g2p_variant = c.variant;
+        t.g2p_block = c.block;
+        if (c.variant == 0) t.g2p_tiles_per_sm = c.tiles_per_sm;
+        float ms = 0.f;
+        rc = time_it([&]() { return launch_g2p(V, s->pf, t, s->num_sms, st); }, CNT_G2P_CURSOR, ms);
         if (rc) return rc;
         if (ms < best_g2p) {
             best_g2p = ms;
-            best.g2p_block = gb;
+            best.g2p_variant = t.g2p_variant;
+            best.g2p_block = t.g2p_block;
+            best.g2p_tiles_per_sm = t.g2p_tiles_per_sm;
         }
     }
     // restore: state, keys, clean accumulator grid

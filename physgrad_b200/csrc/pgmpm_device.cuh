@@ -162,7 +162,10 @@ __device__ __forceinline__ void make_stencil(const SceneDev& sc, const float x[3
         float u;
         st.s[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
         if (PHYS == PHYS_MLS) {
-            st.f[a] = __fsub_rn(u, (float)st.s[a]);
+            // f is clamped to the stencil's support so that a particle that
+            // left the grid (flagged ESCAPE) transfers as if at the wall
+            // instead of with extrapolated, negative weights.
+            st.f[a] = fminf(fmaxf(__fsub_rn(u, (float)st.s[a]), 0.5f), 1.5f);
             st.b[a] = st.s[a];
             mls_weights(st.f[a], st.w[a]);
         } else {

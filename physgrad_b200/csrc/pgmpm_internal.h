@@ -8,9 +8,20 @@
 
 namespace pgmpm {
 
-// counters[] layout: active tile count, active node count (u64, reset
-// every step) and the sticky error flags.
-enum { CNT_TILES = 0, CNT_ACTIVE = 2, CNT_FLAGS = 4, CNT_WORDS = 8 };
+// counters[] layout.  Words [0, CNT_RESET) are cleared every step:
+// active node tiles, occupied cell tiles, active node count (u64), and the
+// work cursors of the tile kernels.  CNT_FLAGS (sticky error flags) is
+// cleared only by pgmpm_check_status.
+enum {
+    CNT_TILES = 0,
+    CNT_CTILES = 1,
+    CNT_ACTIVE = 2,
+    CNT_P2G_CURSOR = 4,
+    CNT_G2P_CURSOR = 5,
+    CNT_RESET = 6,
+    CNT_FLAGS = 6,
+    CNT_WORDS = 8
+};
 
 // Everything a step kernel needs, passed by value.
 struct View {
@@ -29,15 +40,24 @@ struct View {
     float4* grid_vpre;         // optional: (v before walls, m), recorded for the adjoint
     uint32_t* tile_flags;      // node tile active flags (per global node tile)
     uint32_t* tile_list;       // active node tiles
+    uint32_t* ctile_list;      // occupied cell tiles (global cell tile ids)
+    uint2* ctile_range;        // per global cell tile: [begin, end) in sorted order
     uint32_t* counters;        // see CNT_*
     int total_ct, total_nt;
 };
 
+// P2G variants: 0 = per-cell register accumulation over occupied cell tiles
+// (default), 1 = per-particle shared-memory atomics over fixed chunks.
+// G2P variants: 0 = node tile staged in shared memory, 1 = direct gather.
 struct Tuning {
-    int p2g_block = 256;
-    int ppt = 1024;
+    int p2g_block = 192;   // variant 0 uses exactly 192 threads (64 cells x 3 z-slices)
+    int ppt = 1024;        // variant 1: particles per chunk; variant 0: sub-chunk staged at once is fixed
     int g2p_block = 256;
     int grid_block = 256;
+    int p2g_variant = 0;
+    int g2p_variant = 1;
+    int tile_blocks_per_sm = 3;  // persistent P2G tile kernel: blocks per SM
+    int g2p_tiles_per_sm = 2;    // persistent G2P tile kernel: blocks per SM (256 threads)
 };
 
 // pgmpm_sort.cu
@@ -55,9 +75,9 @@ struct PhysFlags {
 };
 cudaError_t launch_keys(const View& V, const PhysFlags& pf, cudaStream_t st);
 cudaError_t launch_mark(const View& V, cudaStream_t st);
-cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st);
+cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
-cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st);
+cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_pack(const View& V, const float* x, const float* v, const float* C, const float* F,
                         const float* m, const float* V0, const int32_t* mat, const uint32_t* order,
                         uint32_t* user_of_phys, float2* mV_out, int32_t* mat_out, cudaStream_t st);

@@ -58,6 +58,19 @@ __global__ void k_mark(View V) {
             atomicOr(&V.counters[CNT_FLAGS], FLAG_TILE_RANGE);
             continue;
         }
+        // this thread found the first particle of cell tile ct: record the
+        // tile's sorted range and list it as occupied
+        {
+            int64_t lo = i + 1, hi = V.N;
+            const uint32_t target = (ct + 1u) << 6;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (V.skeys[mid] < target) lo = mid + 1; else hi = mid;
+            }
+            V.ctile_range[ct] = make_uint2((uint32_t)i, (uint32_t)lo);
+            const uint32_t slot = atomicAdd(&V.counters[CNT_CTILES], 1u);
+            V.ctile_list[slot] = ct;
+        }
         const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
         const SceneDev& sc = scene_ref(V, s);
         const int lt = (int)ct - sc.ct_base;
@@ -227,6 +240,229 @@ __global__ void __launch_bounds__(512) k_p2g(View V, int ppt) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// ---------------------------------------------------- P2G over cell tiles
+// One block per occupied 4^3 cell tile (work taken from an atomic cursor).
+// Thread t owns cell t/3 and z-slice oz = t%3 of that cell's 3x3x3 stencil:
+// 9 nodes x (m, p) = 36 register accumulators.  Per sub-chunk of P2G_SC
+// sorted particles:
+//   phase A (thread = particle, coalesced): stress, affine matrix, axis
+//            weights -> shared-memory payload (SoA);
+//   phase B (thread = (cell, oz)): loop over the cell's particles of the
+//            sub-chunk, accumulate its 9 nodes in registers.
+// Flush: accumulators are transposed through shared memory (plain stores,
+// no atomics), each of the 6^3 tile nodes sums the <= 27 cells that touch
+// it, and non-empty nodes get ONE vector atomic (red.global.add.v4.f32).
+constexpr int P2G_T = 192;
+constexpr int P2G_SC = 256;
+constexpr int PAY_W = 0;    // wx0..2, wy0..2, wz0..2
+constexpr int PAY_M = 9;
+constexpr int PAY_B = 10;   // MLS: m v - (A dx) f ;  REF: v
+constexpr int PAY_A = 13;   // MLS: A dx (row-major)
+constexpr int PAY_MLS = 22;
+
+template <int PHYS, bool MULTI>
+__global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V) {
+    __shared__ float sm[27 * 4 * 64];  // payload [22][P2G_SC], then transpose [27][4][64]
+    __shared__ uint32_t cb[64], ce[64];
+    __shared__ uint32_t s_work;
+    static_assert(PAY_MLS * P2G_SC <= 27 * 4 * 64, "payload must fit the transpose buffer");
+    const int t = threadIdx.x;
+    const int cell = t / 3, oz = t - 3 * (t / 3);
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    for (;;) {
+        if (t == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+        if (t < 64) {
+            cb[t] = 0u;
+            ce[t] = 0u;
+        }
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= ntiles) break;
+        const uint32_t ct = V.ctile_list[w];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        // per-cell sorted ranges inside the tile (keys are sorted by local cell)
+        for (uint32_t i = rg.x + t; i < rg.y; i += P2G_T) {
+            const uint32_t k = V.skeys[i] & 63u;
+            if (i == rg.x || (V.skeys[i - 1] & 63u) != k) cb[k] = i;
+            if (i + 1 == rg.y || (V.skeys[i + 1] & 63u) != k) ce[k] = i + 1;
+        }
+        __syncthreads();
+        const uint32_t my_b = cb[cell], my_e = ce[cell];
+        float am[3][3], apx[3][3], apy[3][3], apz[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) am[a][b] = apx[a][b] = apy[a][b] = apz[a][b] = 0.f;
+        for (uint32_t s0 = rg.x; s0 < rg.y; s0 += P2G_SC) {
+            const uint32_t s1 = min(rg.y, s0 + (uint32_t)P2G_SC);
+            // ---- phase A: per-particle payload
+            for (uint32_t i = s0 + t; i < s1; i += P2G_T) {
+                const int j = (int)(i - s0);
+                const uint32_t p = V.order[i];
+                if (p >= (uint32_t)N) {
+                    flags |= FLAG_TILE_RANGE;
+#pragma unroll
+                    for (int f = 0; f < PAY_MLS; ++f) sm[f * P2G_SC + j] = 0.f;
+                    continue;
+                }
+                const float4 q0 = V.q[p];
+                const float x[3] = {q0.x, q0.y, q0.z};
+                const float2 mv = V.mV[p];
+                Stencil st;
+                make_stencil<PHYS>(sc, x, st, flags);
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) sm[(PAY_W + 3 * a + k) * P2G_SC + j] = st.w[a][k];
+                if (PHYS == PHYS_MLS) {
+                    const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+                    const float4 q3 = V.q[3 * N + p], q4 = V.q[4 * N + p], q5 = V.q[5 * N + p];
+                    float xx[3], F[9], v[3], C[9];
+                    unpack_xF(q0, q1, q2, xx, F);
+                    unpack_vC(q3, q4, q5, v, C);
+                    const MatDev mt = V.mats[MULTI ? V.mat[p] : 0];
+                    float tau[9];
+                    kirchhoff(F, mt, tau);
+                    const float kk = -sc.dt * mv.y * sc.D;
+                    float Ad[9];
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) Ad[a] = (kk * tau[a] + mv.x * C[a]) * sc.dx;
+                    sm[PAY_M * P2G_SC + j] = mv.x;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        sm[(PAY_B + a) * P2G_SC + j] =
+                            mv.x * v[a] - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) sm[(PAY_A + a) * P2G_SC + j] = Ad[a];
+                } else {
+                    const float4 q3 = V.q[3 * N + p];
+                    const bool regular = st.b[0] == st.s[0] && st.b[1] == st.s[1] && st.b[2] == st.s[2];
+                    sm[PAY_M * P2G_SC + j] = regular ? mv.x : 0.f;
+                    sm[(PAY_B + 0) * P2G_SC + j] = q3.x;
+                    sm[(PAY_B + 1) * P2G_SC + j] = q3.y;
+                    sm[(PAY_B + 2) * P2G_SC + j] = q3.z;
+                    if (!regular) {
+                        // stencil partly outside the grid: scatter this particle
+                        // directly (per-node bounds checks as the reference)
+                        const float vel[3] = {q3.x, q3.y, q3.z};
+                        for (int ii = 0; ii < 3; ++ii) {
+                            const int gi = st.b[0] + ii;
+                            if (gi < 0 || gi >= sc.n[0]) continue;
+                            for (int jj = 0; jj < 3; ++jj) {
+                                const int gj = st.b[1] + jj;
+                                if (gj < 0 || gj >= sc.n[1]) continue;
+                                for (int kq = 0; kq < 3; ++kq) {
+                                    const int gk = st.b[2] + kq;
+                                    if (gk < 0 || gk >= sc.n[2]) continue;
+                                    const float wgt = __fmul_rn(__fmul_rn(st.w[0][ii], st.w[1][jj]), st.w[2][kq]);
+                                    if (!(wgt > 1e-10f)) continue;
+                                    const float wm = __fmul_rn(wgt, mv.x);
+                                    float* g = reinterpret_cast<float*>(&V.grid_mp[node_index(sc, gi, gj, gk)]);
+                                    atomicAdd(g, wm);
+                                    atomicAdd(g + 1, __fmul_rn(wm, vel[0]));
+                                    atomicAdd(g + 2, __fmul_rn(wm, vel[1]));
+                                    atomicAdd(g + 3, __fmul_rn(wm, vel[2]));
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- phase B: this thread's cell, slice oz
+            const uint32_t ib = max(my_b, s0), ie = min(my_e, s1);
+            for (uint32_t i = ib; i < ie; ++i) {
+                const int j = (int)(i - s0);
+                const float wz = sm[(PAY_W + 6 + oz) * P2G_SC + j];
+                const float m = sm[PAY_M * P2G_SC + j];
+                const float wx[3] = {sm[(PAY_W + 0) * P2G_SC + j], sm[(PAY_W + 1) * P2G_SC + j],
+                                     sm[(PAY_W + 2) * P2G_SC + j]};
+                const float wy[3] = {sm[(PAY_W + 3) * P2G_SC + j], sm[(PAY_W + 4) * P2G_SC + j],
+                                     sm[(PAY_W + 5) * P2G_SC + j]};
+                const float b0 = sm[(PAY_B + 0) * P2G_SC + j], b1 = sm[(PAY_B + 1) * P2G_SC + j],
+                            b2 = sm[(PAY_B + 2) * P2G_SC + j];
+                if (PHYS == PHYS_MLS) {
+                    float Ad[9];
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) Ad[a] = sm[(PAY_A + a) * P2G_SC + j];
+                    const float fz = (float)oz;
+                    const float bz0 = b0 + Ad[2] * fz, bz1 = b1 + Ad[5] * fz, bz2 = b2 + Ad[8] * fz;
+#pragma unroll
+                    for (int yy = 0; yy < 3; ++yy) {
+                        const float wyz = wy[yy] * wz;
+                        float v0 = bz0 + Ad[1] * (float)yy, v1 = bz1 + Ad[4] * (float)yy,
+                              v2 = bz2 + Ad[7] * (float)yy;
+#pragma unroll
+                        for (int xx = 0; xx < 3; ++xx) {
+                            const float wgt = wx[xx] * wyz;
+                            am[yy][xx] += wgt * m;
+                            apx[yy][xx] += wgt * v0;
+                            apy[yy][xx] += wgt * v1;
+                            apz[yy][xx] += wgt * v2;
+                            v0 += Ad[0];
+                            v1 += Ad[3];
+                            v2 += Ad[6];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int yy = 0; yy < 3; ++yy)
+#pragma unroll
+                        for (int xx = 0; xx < 3; ++xx) {
+                            const float wgt = __fmul_rn(__fmul_rn(wx[xx], wy[yy]), wz);
+                            if (wgt > 1e-10f) {
+                                const float wm = __fmul_rn(wgt, m);
+                                am[yy][xx] += wm;
+                                apx[yy][xx] += __fmul_rn(wm, b0);
+                                apy[yy][xx] += __fmul_rn(wm, b1);
+                                apz[yy][xx] += __fmul_rn(wm, b2);
+                            }
+                        }
+                }
+            }
+            __syncthreads();
+        }
+        // ---- flush: transpose through shared memory, one vector atomic per node
+#pragma unroll
+        for (int yy = 0; yy < 3; ++yy)
+#pragma unroll
+            for (int xx = 0; xx < 3; ++xx) {
+                const int o = xx + 3 * yy + 9 * oz;
+                sm[(o * 4 + 0) * 64 + cell] = am[yy][xx];
+                sm[(o * 4 + 1) * 64 + cell] = apx[yy][xx];
+                sm[(o * 4 + 2) * 64 + cell] = apy[yy][xx];
+                sm[(o * 4 + 3) * 64 + cell] = apz[yy][xx];
+            }
+        __syncthreads();
+        for (int n = t; n < TILE_NODES; n += P2G_T) {
+            const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int zz = max(0, nz - 3); zz <= min(2, nz); ++zz)
+                for (int yy = max(0, ny - 3); yy <= min(2, ny); ++yy)
+                    for (int xx = max(0, nx - 3); xx <= min(2, nx); ++xx) {
+                        const int c = (nx - xx) + 4 * (ny - yy) + 16 * (nz - zz);
+                        const int o = xx + 3 * yy + 9 * zz;
+                        acc.x += sm[(o * 4 + 0) * 64 + c];
+                        acc.y += sm[(o * 4 + 1) * 64 + c];
+                        acc.z += sm[(o * 4 + 2) * 64 + c];
+                        acc.w += sm[(o * 4 + 3) * 64 + c];
+                    }
+            const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
+            if (acc.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], acc);
+        }
+        __syncthreads();
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
 // ------------------------------------------------------------ grid update
 template <int PHYS>
 __global__ void k_grid(View V) {
@@ -275,6 +511,110 @@ __global__ void k_grid(View V) {
 }
 
 // ------------------------------------------------------------------- G2P
+// Per-particle G2P update shared by both G2P variants; `fetch(i, j, k)`
+// returns the (v, m) float4 of grid node (i, j, k) of scene sc.
+template <int PHYS, bool MULTI, bool FLUID, class Fetch>
+__device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, uint32_t p, const Fetch& fetch,
+                                             uint32_t& flags) {
+    const int64_t N = V.N;
+    const float4 q0 = V.q[p];
+    float x[3] = {q0.x, q0.y, q0.z};
+    Stencil st;
+    make_stencil<PHYS>(sc, x, st, flags);
+    if (PHYS == PHYS_MLS) {
+        const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+        float xx[3], F[9];
+        unpack_xF(q0, q1, q2, xx, F);
+        const float dx = sc.dx;
+        float nv[3] = {0.f, 0.f, 0.f};
+        float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float dk = ((float)k - st.f[2]) * dx;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float dj = ((float)j - st.f[1]) * dx;
+                const float wjk = st.w[1][j] * st.w[2][k];
+#pragma unroll
+                for (int ii = 0; ii < 3; ++ii) {
+                    const float di = ((float)ii - st.f[0]) * dx;
+                    const float4 g = fetch(st.s[0] + ii, st.s[1] + j, st.s[2] + k);
+                    const float w = st.w[0][ii] * wjk;
+                    const float wx = w * g.x, wy = w * g.y, wz = w * g.z;
+                    nv[0] += wx; nv[1] += wy; nv[2] += wz;
+                    B[0] += wx * di; B[1] += wx * dj; B[2] += wx * dk;
+                    B[3] += wy * di; B[4] += wy * dj; B[5] += wy * dk;
+                    B[6] += wz * di; B[7] += wz * dj; B[8] += wz * dk;
+                }
+            }
+        }
+        float C[9], Fn[9], M[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) {
+            C[a] = sc.D * B[a];
+            M[a] = sc.dt * C[a] + ((a % 4 == 0) ? 1.f : 0.f);
+        }
+        m3_mul(M, F, Fn);
+        if (FLUID) {
+            const int mid = MULTI ? V.mat[p] : 0;
+            if (V.mats[mid].model == MODEL_EOS) {
+                const float c = cbrtf(m3_det(Fn));
+#pragma unroll
+                for (int a = 0; a < 9; ++a) Fn[a] = (a % 4 == 0) ? c : 0.f;
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) x[a] = x[a] + sc.dt * nv[a];
+        float4 o0, o1, o2, o3, o4, o5;
+        pack_xF(x, Fn, o0, o1, o2);
+        pack_vC(nv, C, o3, o4, o5);
+        V.q[p] = o0;
+        V.q[N + p] = o1;
+        V.q[2 * N + p] = o2;
+        V.q[3 * N + p] = o3;
+        V.q[4 * N + p] = o4;
+        V.q[5 * N + p] = o5;
+    } else {
+        // material_point_method.h:599-666 in the same order of operations
+        float nv[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii) {
+            const int gi = st.b[0] + ii;
+            if (gi < 0 || gi >= sc.n[0]) continue;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int gj = st.b[1] + j;
+                if (gj < 0 || gj >= sc.n[1]) continue;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const int gk = st.b[2] + k;
+                    if (gk < 0 || gk >= sc.n[2]) continue;
+                    const float weight = __fmul_rn(__fmul_rn(st.w[0][ii], st.w[1][j]), st.w[2][k]);
+                    if (!(weight > 1e-10f)) continue;
+                    const float4 g = fetch(gi, gj, gk);
+                    nv[0] = __fadd_rn(nv[0], __fmul_rn(weight, g.x));
+                    nv[1] = __fadd_rn(nv[1], __fmul_rn(weight, g.y));
+                    nv[2] = __fadd_rn(nv[2], __fmul_rn(weight, g.z));
+                }
+            }
+        }
+        const float4 q3 = V.q[3 * N + p];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) x[a] = __fadd_rn(x[a], __fmul_rn(nv[a], sc.dt));
+        V.q[p] = make_float4(x[0], x[1], x[2], q0.w);
+        V.q[3 * N + p] = make_float4(nv[0], nv[1], nv[2], q3.w);
+    }
+    // key of the new position for the next step's sort
+    int so[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float u;
+        so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+    }
+    V.keys[p] = cell_key(sc, so);
+}
+
+// G2P variant 1: one thread per sorted particle, 27 gathers through L1.
 template <int PHYS, bool MULTI, bool FLUID>
 __global__ void k_g2p(View V) {
     const int64_t N = V.N;
@@ -288,107 +628,56 @@ __global__ void k_g2p(View V) {
         }
         const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
         const SceneDev& sc = scene_ref(V, s);
-        const float4 q0 = V.q[p];
-        float x[3] = {q0.x, q0.y, q0.z};
-        Stencil st;
-        make_stencil<PHYS>(sc, x, st, flags);
-        if (PHYS == PHYS_MLS) {
-            const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
-            float xx[3], F[9];
-            unpack_xF(q0, q1, q2, xx, F);
-            const float dx = sc.dx;
-            float nv[3] = {0.f, 0.f, 0.f};
-            float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float dk = ((float)k - st.f[2]) * dx;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const float dj = ((float)j - st.f[1]) * dx;
-                    const float wjk = st.w[1][j] * st.w[2][k];
-                    const int64_t row = node_index(sc, st.s[0], st.s[1] + j, st.s[2] + k);
-                    const int gi0 = st.s[0];
-#pragma unroll
-                    for (int ii = 0; ii < 3; ++ii) {
-                        const float di = ((float)ii - st.f[0]) * dx;
-                        const int gi = gi0 + ii;
-                        // nodes of a row share the tile unless the row crosses x % 4 == 0
-                        const int64_t idx = ((gi >> 2) == (gi0 >> 2)) ? row + ii
-                                                                      : node_index(sc, gi, st.s[1] + j, st.s[2] + k);
-                        const float4 g = __ldg(&V.grid_v[idx]);
-                        const float w = st.w[0][ii] * wjk;
-                        const float wx = w * g.x, wy = w * g.y, wz = w * g.z;
-                        nv[0] += wx; nv[1] += wy; nv[2] += wz;
-                        B[0] += wx * di; B[1] += wx * dj; B[2] += wx * dk;
-                        B[3] += wy * di; B[4] += wy * dj; B[5] += wy * dk;
-                        B[6] += wz * di; B[7] += wz * dj; B[8] += wz * dk;
-                    }
-                }
-            }
-            float C[9], Fn[9], M[9];
-#pragma unroll
-            for (int a = 0; a < 9; ++a) {
-                C[a] = sc.D * B[a];
-                M[a] = sc.dt * C[a] + ((a % 4 == 0) ? 1.f : 0.f);
-            }
-            m3_mul(M, F, Fn);
-            if (FLUID) {
-                const int mid = MULTI ? V.mat[p] : 0;
-                if (V.mats[mid].model == MODEL_EOS) {
-                    const float c = cbrtf(m3_det(Fn));
-#pragma unroll
-                    for (int a = 0; a < 9; ++a) Fn[a] = (a % 4 == 0) ? c : 0.f;
-                }
-            }
-#pragma unroll
-            for (int a = 0; a < 3; ++a) x[a] = x[a] + sc.dt * nv[a];
-            float4 o0, o1, o2, o3, o4, o5;
-            pack_xF(x, Fn, o0, o1, o2);
-            pack_vC(nv, C, o3, o4, o5);
-            V.q[p] = o0;
-            V.q[N + p] = o1;
-            V.q[2 * N + p] = o2;
-            V.q[3 * N + p] = o3;
-            V.q[4 * N + p] = o4;
-            V.q[5 * N + p] = o5;
-        } else {
-            // material_point_method.h:599-666 in the same order of operations
-            float nv[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int ii = 0; ii < 3; ++ii) {
-                const int gi = st.b[0] + ii;
-                if (gi < 0 || gi >= sc.n[0]) continue;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const int gj = st.b[1] + j;
-                    if (gj < 0 || gj >= sc.n[1]) continue;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const int gk = st.b[2] + k;
-                        if (gk < 0 || gk >= sc.n[2]) continue;
-                        const float weight = __fmul_rn(__fmul_rn(st.w[0][ii], st.w[1][j]), st.w[2][k]);
-                        if (!(weight > 1e-10f)) continue;
-                        const float4 g = __ldg(&V.grid_v[node_index(sc, gi, gj, gk)]);
-                        nv[0] = __fadd_rn(nv[0], __fmul_rn(weight, g.x));
-                        nv[1] = __fadd_rn(nv[1], __fmul_rn(weight, g.y));
-                        nv[2] = __fadd_rn(nv[2], __fmul_rn(weight, g.z));
-                    }
-                }
-            }
-            const float4 q3 = V.q[3 * N + p];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) x[a] = __fadd_rn(x[a], __fmul_rn(nv[a], sc.dt));
-            V.q[p] = make_float4(x[0], x[1], x[2], q0.w);
-            V.q[3 * N + p] = make_float4(nv[0], nv[1], nv[2], q3.w);
+        const float4* gv = V.grid_v;
+        auto fetch = [&](int gi, int gj, int gk) { return __ldg(&gv[node_index(sc, gi, gj, gk)]); };
+        g2p_particle<PHYS, MULTI, FLUID>(V, sc, p, fetch, flags);
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+// G2P variant 0: one block per occupied cell tile; the tile's 6^3 node
+// velocities are staged in shared memory once and every particle of the tile
+// gathers its 27 nodes from there.
+template <int PHYS, bool MULTI, bool FLUID>
+__global__ void __launch_bounds__(256) k_g2p_tiles(View V) {
+    __shared__ float4 gsm[TILE_NODES];
+    __shared__ uint32_t s_work;
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    for (;;) {
+        if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_G2P_CURSOR], 1u);
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= ntiles) break;
+        const uint32_t ct = V.ctile_list[w];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        for (int n = threadIdx.x; n < TILE_NODES; n += blockDim.x) {
+            const int gi = ox + n % TN, gj = oy + (n / TN) % TN, gk = oz + n / (TN * TN);
+            gsm[n] = (gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2]) ? V.grid_v[node_index(sc, gi, gj, gk)]
+                                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        // key of the new position for the next step's sort
-        int so[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float u;
-            so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+        __syncthreads();
+        const float4* gv = V.grid_v;
+        auto fetch = [&](int gi, int gj, int gk) {
+            const unsigned lx = (unsigned)(gi - ox), ly = (unsigned)(gj - oy), lz = (unsigned)(gk - oz);
+            if (lx < (unsigned)TN && ly < (unsigned)TN && lz < (unsigned)TN) return gsm[lx + TN * (ly + TN * lz)];
+            return __ldg(&gv[node_index(sc, gi, gj, gk)]);
+        };
+        for (uint32_t i = rg.x + threadIdx.x; i < rg.y; i += blockDim.x) {
+            const uint32_t p = V.order[i];
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            g2p_particle<PHYS, MULTI, FLUID>(V, sc, p, fetch, flags);
         }
-        V.keys[p] = cell_key(sc, so);
+        __syncthreads();
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
@@ -505,8 +794,20 @@ cudaError_t launch_mark(const View& V, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st) {
+cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
+    if (t.p2g_variant == 0) {
+        const int nb = num_sms * t.tile_blocks_per_sm;
+        if (pf.physics == PHYS_MLS) {
+            if (pf.multi_mat)
+                k_p2g_tiles<PHYS_MLS, true><<<nb, P2G_T, 0, st>>>(V);
+            else
+                k_p2g_tiles<PHYS_MLS, false><<<nb, P2G_T, 0, st>>>(V);
+        } else {
+            k_p2g_tiles<PHYS_REF, false><<<nb, P2G_T, 0, st>>>(V);
+        }
+        return cudaGetLastError();
+    }
     const int64_t nb = (V.N + t.ppt - 1) / t.ppt;
     if (nb > 0x7FFFFFFF) return cudaErrorInvalidValue;
     if (pf.physics == PHYS_MLS) {
@@ -534,23 +835,33 @@ cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, cudaStream_t st) {
+#define PGMPM_G2P_DISPATCH(KERNEL, GRID, BLOCK)                                  \
+    do {                                                                         \
+        if (pf.physics == PHYS_MLS) {                                            \
+            if (pf.multi_mat) {                                                  \
+                if (pf.has_fluid)                                                \
+                    KERNEL<PHYS_MLS, true, true><<<GRID, BLOCK, 0, st>>>(V);     \
+                else                                                             \
+                    KERNEL<PHYS_MLS, true, false><<<GRID, BLOCK, 0, st>>>(V);    \
+            } else {                                                             \
+                if (pf.has_fluid)                                                \
+                    KERNEL<PHYS_MLS, false, true><<<GRID, BLOCK, 0, st>>>(V);    \
+                else                                                             \
+                    KERNEL<PHYS_MLS, false, false><<<GRID, BLOCK, 0, st>>>(V);   \
+            }                                                                    \
+        } else {                                                                 \
+            KERNEL<PHYS_REF, false, false><<<GRID, BLOCK, 0, st>>>(V);           \
+        }                                                                        \
+    } while (0)
+
+cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
-    const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
-    if (pf.physics == PHYS_MLS) {
-        if (pf.multi_mat) {
-            if (pf.has_fluid)
-                k_g2p<PHYS_MLS, true, true><<<nb, t.g2p_block, 0, st>>>(V);
-            else
-                k_g2p<PHYS_MLS, true, false><<<nb, t.g2p_block, 0, st>>>(V);
-        } else {
-            if (pf.has_fluid)
-                k_g2p<PHYS_MLS, false, true><<<nb, t.g2p_block, 0, st>>>(V);
-            else
-                k_g2p<PHYS_MLS, false, false><<<nb, t.g2p_block, 0, st>>>(V);
-        }
+    if (t.g2p_variant == 0) {
+        const int nb = num_sms * t.g2p_tiles_per_sm;
+        PGMPM_G2P_DISPATCH(k_g2p_tiles, nb, 256);
     } else {
-        k_g2p<PHYS_REF, false, false><<<nb, t.g2p_block, 0, st>>>(V);
+        const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
+        PGMPM_G2P_DISPATCH(k_g2p, nb, t.g2p_block);
     }
     return cudaGetLastError();
 }

@@ -247,10 +247,15 @@ class Simulator:
     def set_tuning(self, p2g_block=0, ppt=0, g2p_block=0, use_graph=-1):
         check(lib().pgmpm_set_tuning(self._h, int(p2g_block), int(ppt), int(g2p_block), int(use_graph)))
 
+    def set_variants(self, p2g_variant=-1, g2p_variant=-1, p2g_tiles_per_sm=0, g2p_tiles_per_sm=0):
+        check(lib().pgmpm_set_kernel_variants(self._h, int(p2g_variant), int(g2p_variant), int(p2g_tiles_per_sm),
+                                              int(g2p_tiles_per_sm)))
+
     def autotune(self, reps: int = 3, stream=None) -> dict:
         check(lib().pgmpm_autotune(self._h, int(reps), _stream_handle(stream)))
         m = self.metrics()
-        return {"p2g_block": m["p2g_block"], "ppt": m["p2g_ppt"], "g2p_block": m["g2p_block"]}
+        return {k: m[k] for k in ("p2g_variant", "p2g_block", "p2g_ppt", "p2g_tiles_per_sm", "g2p_variant",
+                                  "g2p_block", "g2p_tiles_per_sm")}
 
     def get_array(self, which: int) -> np.ndarray:
         """u32 array of N entries (C.ARRAY_*): physical order, keys, last sort."""
