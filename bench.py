@@ -85,18 +85,29 @@ class ClockSampler:
         self.path = None
 
     def __enter__(self):
+        self.t0 = self.t1 = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "--query-gpu=timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            t_end = time.time() + 5.0  # wait for the first sample
+            while time.time() < t_end and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(0.25)  # let the sampler record the tail of the window
 
     def __exit__(self, *exc):
         if self.proc:
@@ -109,22 +120,32 @@ class ClockSampler:
     def summary(self):
         if not self.path or not os.path.exists(self.path):
             return None
+        import datetime
+
         rows = []
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 7:
+            if len(parts) < 8:
                 continue
             try:
-                rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[1]), float(parts[2]), parts[4:8]))
             except ValueError:
                 continue
         os.unlink(self.path)
         if not rows:
             return None
+        win = rows
+        if self.t0 is not None and self.t1 is not None:
+            # nvidia-smi timestamps are local wall-clock; compare in the same clock
+            win = [r for r in rows if self.t0 - 0.05 <= r[0] <= self.t1 + 0.05]
+            if not win:  # window shorter than the sampling period: nearest sample after start
+                after = [r for r in rows if r[0] >= self.t0]
+                win = after[:1] or rows[-1:]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({names[i] for _, _, _, r in win for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[1] for r in win), "sm_max_mhz": max(r[2] for r in win),
+                "reasons": reasons, "samples": len(win)}
 
 
 # ------------------------------------------------------- reference CPU timing
@@ -214,10 +235,12 @@ def run_ours(args, rank, world, device):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(device) as clk:
         torch.cuda.synchronize()
+        clk.mark_start()
         ev0.record(stream)
         sim.step(args.steps, stream=stream)
         ev1.record(stream)
         torch.cuda.synchronize()
+        clk.mark_end()
     ms = ev0.elapsed_time(ev1)
     if world > 1:
         import torch.distributed as dist
@@ -345,8 +368,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint"])
     ap.add_argument("--autotune", action="store_true")
