@@ -224,6 +224,21 @@ PGMPM_API int pgmpm_get_array(pgmpm_solver s, int32_t which, uint32_t* out, int3
 PGMPM_API int pgmpm_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                            uint32_t* vals_out, int64_t n, int32_t key_bits, void* stream);
 
+/* Same stable sort, for callers that may not allocate device memory (a host
+ * framework that owns the GPU memory budget, or a loop that cannot afford
+ * cudaMalloc's device-wide synchronisation).  No reference counterpart: the
+ * reference has no sort.  It calls no allocator.  Its scratch is a fixed
+ * array in the library's device image (about 8.9 MB per GPU that loads the
+ * library, held until exit), so n is limited to PGMPM_NOALLOC_MAX_PAIRS
+ * (larger n returns PGMPM_ERR_ARG).  keys_out/vals_out must not alias the
+ * inputs.  The first call on a device looks up the array's address and may
+ * load the module: make it before any stream capture.  Calls share the
+ * array, so calls that overlap on the GPU race; the caller orders them.
+ * Asynchronous on `stream`. */
+#define PGMPM_NOALLOC_MAX_PAIRS (1 << 20)
+PGMPM_API int pgmpm_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                             uint32_t* vals_out, int64_t n, int32_t key_bits, void* stream);
+
 /* Reference-shaped launcher (src/pytorch_autograd.cu:371-382): one
  * REF_COMPAT MPM step of num_particles particles on the unit cube with a
  * grid_resolution^3 grid (dx = 1/grid_resolution).  positions, velocities

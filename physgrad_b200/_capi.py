@@ -50,6 +50,8 @@ ARRAY_SORTED_ORDER = 3
 PTR_HOST = 0
 PTR_DEVICE = 1
 
+NOALLOC_MAX_PAIRS = 1 << 20
+
 
 class SceneDesc(ctypes.Structure):
     _fields_ = [
@@ -123,6 +125,7 @@ SIGNATURES = {
     "pgmpm_backward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "pgmpm_get_array": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
     "pgmpm_radix_sort_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp]),
+    "pgmpm_radix_sort_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp]),
     "launch_mpm_timestep_forward": (None, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp]),
 }
 

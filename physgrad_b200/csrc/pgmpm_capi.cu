@@ -19,8 +19,17 @@
 using namespace pgmpm;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+// Sets the message returned by pgmpm_last_error() (shared with the other
+// translation units of the library) and returns code.
+int pgmpm_set_error(int code, const char* msg) {
+    g_err = msg ? msg : "";
+    return code;
+}
+
+namespace {
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];

@@ -61,6 +61,12 @@ struct Tuning {
 };
 
 // pgmpm_sort.cu
+constexpr int RADIX_TILE = 2048;  // keys per block of the sort kernels
+constexpr int RADIX_MAX_DIGITS = 256;
+// u32 words of histogram scratch the sort needs for n pairs
+constexpr int64_t radix_scratch_words_for(int64_t n) {
+    return ((n + RADIX_TILE - 1) / RADIX_TILE) * RADIX_MAX_DIGITS + RADIX_MAX_DIGITS;
+}
 int64_t radix_sort_scratch_words(int64_t n);
 int radix_passes(int key_bits);
 cudaError_t radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uint32_t* va, uint32_t* kb,

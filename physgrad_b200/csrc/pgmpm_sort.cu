@@ -24,6 +24,7 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_ITEMS = 8;  // keys per thread per tile
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_MAXD = 256;
+static_assert(RS_TILE == RADIX_TILE && RS_MAXD == RADIX_MAX_DIGITS, "scratch sizing must match the kernels");
 
 __global__ void __launch_bounds__(RS_THREADS) rs_hist(const uint32_t* __restrict__ keys, int64_t n, int shift,
                                                       int bits, uint32_t* __restrict__ hist, int nblocks) {
@@ -176,10 +177,7 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
 }
 }  // namespace
 
-int64_t radix_sort_scratch_words(int64_t n) {
-    const int64_t nb = (n + RS_TILE - 1) / RS_TILE;
-    return nb * RS_MAXD + RS_MAXD;
-}
+int64_t radix_sort_scratch_words(int64_t n) { return radix_scratch_words_for(n); }
 
 int radix_passes(int key_bits) { return key_bits <= 0 ? 0 : (key_bits + 7) / 8; }
 
