@@ -344,6 +344,161 @@ def run_ours(args, rank, world, device):
     return line
 
 
+def _events():
+    import torch
+
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_adjoint(args, device=0):
+    """Config 3: forward+adjoint (checkpoint every 16) vs plain forward."""
+    import torch
+
+    import physgrad_b200 as pg
+
+    torch.cuda.set_device(device)
+    scenes, counts, mats, st, meta = make_workload("cfg3")
+    N = int(sum(counts))
+    steps, k = meta["steps"], 16
+    sim = pg.Simulator(scenes, counts, mats, device=device)
+    up = lambda s: s.upload(st["x"], st["v"], None, None, st["m"], st["V0"])
+    up(sim)
+    sim.step(args.warmup)
+    up(sim)
+    e0, e1 = _events()
+    torch.cuda.synchronize()
+    e0.record()
+    sim.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1)
+    tgt = np.array([0.5, 0.3, 0.5])
+    gx = torch.empty(N, 3, device="cuda")
+
+    def fwd_adj():
+        up(sim)
+        torch.cuda.synchronize()
+        e0.record()
+        sim.forward_checkpointed(steps, k)
+        out = {"x": torch.empty(N, 3, device="cuda"), "v": torch.empty(N, 3, device="cuda"),
+               "C": torch.empty(N, 3, 3, device="cuda"), "F": torch.empty(N, 3, 3, device="cuda")}
+        sim.download(out)
+        com = out["x"].double().mean(0)
+        gx.copy_((2 * (com - torch.tensor(tgt, device="cuda")) / N).float().expand(N, 3))
+        g = sim.backward({"x": gx})
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), float(((com.cpu().numpy() - tgt) ** 2).sum()), g
+
+    fwd_adj()  # warm-up (allocates the tape)
+    t_fa, L, g = fwd_adj()
+    # FD along a uniform v0 shift in y (full size, FP32 forward)
+    eps = 1e-3
+
+    def loss_at(v0):
+        s2 = pg.Simulator(scenes, counts, mats, device=device)
+        s2.upload(st["x"], v0, None, None, st["m"], st["V0"])
+        s2.step(steps)
+        x = s2.download()["x"].astype(np.float64)
+        s2.close()
+        return float(((x.mean(0) - tgt) ** 2).sum())
+
+    d = np.zeros_like(st["v"])
+    d[:, 1] = 1.0
+    fd = (loss_at(st["v"] + eps * d) - loss_at(st["v"] - eps * d)) / (2 * eps)
+    ad = float(g["v"][:, 1].sum().item())
+    line = {"metric": "particle-steps/s (forward+adjoint)", "value": N * steps / (t_fa * 1e-3),
+            "unit": "particle-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": t_fa / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "differentiable elastic cube (config 3)", "n_particles": N, "grid": 64,
+                       "steps": steps, "checkpoint_every": k, "loss": "||COM - (0.5,0.3,0.5)||^2"},
+            "plain_forward_ms": t_plain, "forward_adjoint_ms": t_fa, "ratio_vs_plain_forward": t_fa / t_plain,
+            "loss": L, "grad_check": {"direction": "uniform v0_y shift", "fd": fd, "adjoint": ad,
+                                      "rel_err": abs(fd - ad) / abs(fd)},
+            "dL_dE": float(g["E"][0].item()),
+            "note": "dL/dE of a centre-of-mass loss is ~0: momentum-conserving transfers, no wall contact"}
+    sim.close()
+    return line
+
+
+def run_batched(args, device=0, adjoint=False):
+    """Config 4 (or 5 with adjoint): all scenes in one solver vs a loop of
+    single-scene solvers (one launch sequence per scene per step)."""
+    import torch
+
+    import physgrad_b200 as pg
+
+    torch.cuda.set_device(device)
+    scenes, counts, mats, st, meta = make_workload("cfg5" if adjoint else "cfg4")
+    N = int(sum(counts))
+    steps = min(args.steps, meta["steps"])
+    off = np.concatenate([[0], np.cumsum(counts)])
+    sl = lambda a, s: None if a is None else a[off[s]:off[s + 1]]
+    big = pg.Simulator(scenes, counts, mats, device=device)
+    big.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st["mat"])
+    singles = []
+    for s in range(len(scenes)):
+        one = pg.Simulator([scenes[s]], [counts[s]], [mats[s]], device=device)
+        one.upload(sl(st["x"], s), sl(st["v"], s), None, None, sl(st["m"], s), sl(st["V0"], s))
+        singles.append(one)
+    e0, e1 = _events()
+    k = 8
+    gxs = None
+    if adjoint:
+        gxb = torch.full((N, 3), 1.0 / N, device="cuda")
+
+        def go_big():
+            big.forward_checkpointed(steps, k)
+            big.backward({"x": gxb})
+
+        def go_loop():
+            for s, one in enumerate(singles):
+                one.forward_checkpointed(steps, k)
+                one.backward({"x": gxb[off[s]:off[s + 1]]})
+    else:
+        def go_big():
+            big.step(steps)
+
+        def go_loop():
+            for _ in range(steps):
+                for one in singles:
+                    one.step(1)
+
+    # warm-up both (graphs, tapes)
+    big.step(args.warmup)
+    for one in singles:
+        one.step(args.warmup)
+    if adjoint:
+        go_big()
+        go_loop()
+    torch.cuda.synchronize()
+    e0.record()
+    go_big()
+    e1.record()
+    torch.cuda.synchronize()
+    t_big = e0.elapsed_time(e1)
+    e0.record()
+    go_loop()
+    e1.record()
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1)
+    name = "batched forward+adjoint (config 5)" if adjoint else "batched forward (config 4)"
+    line = {"metric": "particle-steps/s" + (" (forward+adjoint)" if adjoint else ""),
+            "value": N * steps / (t_big * 1e-3), "unit": "particle-steps/s", "n_gpus": 1, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": t_big / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": name, "n_scenes": len(scenes), "n_particles": N, "counts_min": int(min(counts)),
+                       "counts_max": int(max(counts)), "grids": sorted(set(int(s.n[0]) for s in scenes)),
+                       "checkpoint_every": k if adjoint else None},
+            "loop_of_single_scene_value": N * steps / (t_loop * 1e-3), "batched_ms": t_big, "loop_ms": t_loop,
+            "speedup_vs_loop": t_loop / t_big}
+    big.close()
+    for one in singles:
+        one.close()
+    return line
+
+
 def run_reference(args):
     """Reference arm: the reference's own CPU MPM path on the host cores."""
     from oracle import pyoracle as O
@@ -374,6 +529,7 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint"])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="cfg4/cfg5: plain bench line instead of the batched comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -392,7 +548,12 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     try:
-        line = run_ours(args, rank, world, local)
+        if args.workload == "cfg3_adjoint" and world == 1:
+            line = run_adjoint(args, local)
+        elif args.workload in ("cfg4", "cfg5") and world == 1 and not args.plain:
+            line = run_batched(args, local, adjoint=args.workload == "cfg5")
+        else:
+            line = run_ours(args, rank, world, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

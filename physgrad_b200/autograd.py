@@ -1,0 +1,66 @@
+"""torch.autograd.Function over the checkpointed MLS-MPM forward/backward.
+
+Replaces the reference's PhysicsSimulationFunction pattern
+(src/pytorch_autograd.h:146-226: save inputs, run forward, backward by the
+adjoint) for the MPM path, whose reference adjoint records an empty backward
+(src/differentiable_mpm.h:871-876).  Device tensors cross the C-ABI by
+pointer (no copies); work runs on torch's current stream.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Optional
+
+import torch
+
+from .solver import Simulator
+
+
+class MPMSimulate(torch.autograd.Function):
+    """(x0, v0, C0, F0, E) -> (x, v, C, F) after ``n_steps`` steps.
+
+    ``E`` is a float32 tensor [n_materials] of Young's moduli (bulk modulus
+    for FLUID materials); gradients flow to x0, v0, C0, F0 and E.  m, V0 and
+    the material ids are constants of the simulation."""
+
+    @staticmethod
+    def forward(ctx, sim: Simulator, n_steps: int, checkpoint_every: int, x0, v0, C0, F0, E, m, V0,
+                mat: Optional[torch.Tensor] = None):
+        if not x0.is_cuda:
+            raise ValueError("MPMSimulate expects CUDA tensors")
+        N = x0.shape[0]
+        Evals = E.detach().float().cpu().tolist()
+        if len(Evals) != len(sim.materials):
+            raise ValueError("E must have one entry per material")
+        sim.set_materials([dataclasses.replace(mt, youngs_modulus=float(e)) for mt, e in zip(sim.materials, Evals)])
+        stream = torch.cuda.current_stream()
+        f32 = lambda t: t.detach().to(torch.float32).contiguous()
+        sim.upload(f32(x0), f32(v0), f32(C0).reshape(N, 9), f32(F0).reshape(N, 9), f32(m), f32(V0),
+                   mat.detach().to(torch.int32).contiguous() if mat is not None else None, stream=stream)
+        sim.forward_checkpointed(int(n_steps), int(checkpoint_every), stream=stream)
+        out = {"x": torch.empty(N, 3, device=x0.device), "v": torch.empty(N, 3, device=x0.device),
+               "C": torch.empty(N, 3, 3, device=x0.device), "F": torch.empty(N, 3, 3, device=x0.device)}
+        sim.download(out, stream=stream)
+        ctx.sim = sim
+        ctx.N = N
+        return out["x"], out["v"], out["C"], out["F"]
+
+    @staticmethod
+    def backward(ctx, gx, gv, gC, gF):
+        sim, N = ctx.sim, ctx.N
+        c = lambda t: None if t is None else t.detach().to(torch.float32).contiguous()
+        stream = torch.cuda.current_stream()
+        grads = sim.backward({"x": c(gx), "v": c(gv), "C": None if gC is None else c(gC).reshape(N, 9),
+                              "F": None if gF is None else c(gF).reshape(N, 9)}, stream=stream)
+        return (None, None, None, grads["x"], grads["v"], grads["C"].reshape(N, 3, 3), grads["F"].reshape(N, 3, 3),
+                grads["E"], None, None, None)
+
+
+def simulate(sim: Simulator, x0, v0, E, m, V0, n_steps: int, checkpoint_every: int = 16, C0=None, F0=None, mat=None):
+    """Differentiable rollout: returns (x, v, C, F) after n_steps."""
+    N = x0.shape[0]
+    if C0 is None:
+        C0 = torch.zeros(N, 3, 3, device=x0.device)
+    if F0 is None:
+        F0 = torch.eye(3, device=x0.device).expand(N, 3, 3).contiguous()
+    return MPMSimulate.apply(sim, n_steps, checkpoint_every, x0, v0, C0, F0, E, m, V0, mat)

@@ -1,0 +1,313 @@
+// pgmpm_adjoint.cu -- reverse-mode kernels of one MLS-MPM step.
+//
+// Forward step (per particle p, node i, weights w_pi of x_p):
+//   P2G   m_i = sum w m_p,  p_i = sum w (m_p v_p + A_p d_i),  d_i = x_i - x_p,
+//         A_p = -dt V0_p D tau(F_p) + m_p C_p
+//   grid  vpre_i = p_i/m_i + dt g,  v_i = walls(vpre_i)
+//   G2P   v'_p = sum w v_i,  C'_p = D sum w v_i d_i^T,  F'_p = (I + dt C') F,
+//         x'_p = x_p + dt v'_p   (fluid: F' = cbrt(det F') I)
+// Reverse, given the adjoint of (x', v', C', F'):
+//   1. scatter (k_p2g_tiles, MODE_ADJ): gv_i += w (gv' + dt gx' + D gC d_i)
+//      with gC = gC' + dt gF'raw F^T   -- the "cell-sorted scatter"
+//   2. k_adj_grid: walls^T, gp_i = gv_i / m_i, gm_i = -gv_i . (p_i/m_i) / m_i
+//   3. k_adj_gather: per particle, gather v_i, gp_i, gm_i over the stencil and
+//      form gx, gv, gC, gF (with the stress adjoint) and dL/dE -- the gather
+//      that is the reverse of P2G.
+#include "pgmpm_internal.h"
+
+namespace pgmpm {
+namespace {
+
+__device__ __forceinline__ const SceneDev& scene_ref(const View& V, int s) { return V.scenes[s]; }
+
+__global__ void k_adj_grid(View V, AdjView A) {
+    const uint32_t count = V.counters[CNT_TILES];
+    const int tiles_per_block = blockDim.x >> 6;
+    const int l = threadIdx.x & 63;
+    for (uint32_t w = blockIdx.x * tiles_per_block + (threadIdx.x >> 6); w < count;
+         w += gridDim.x * tiles_per_block) {
+        const uint32_t nt = V.tile_list[w];
+        if (nt >= (uint32_t)V.total_nt) continue;
+        const int s = V.S == 1 ? 0 : scene_of_node_tile(V.scenes, V.S, (int)nt);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)nt - sc.nt_base;
+        const int i = 4 * (lt % sc.nt[0]) + (l & 3);
+        const int j = 4 * ((lt / sc.nt[0]) % sc.nt[1]) + ((l >> 2) & 3);
+        const int k = 4 * (lt / (sc.nt[0] * sc.nt[1])) + (l >> 4);
+        const int64_t idx = ((int64_t)nt << 6) + l;
+        const float4 g = A.grid_gv[idx];
+        const float4 vp = V.grid_vpre[idx];
+        float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (vp.w > 0.f) {
+            float gv[3] = {g.y, g.z, g.w};
+            float v[3] = {vp.x, vp.y, vp.z};
+            const uint32_t zeroed = apply_bc(sc, i, j, k, v);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (zeroed & (1u << a)) gv[a] = 0.f;
+            const float im = 1.f / vp.w;
+            const float pm0 = vp.x - sc.dt * sc.gravity[0], pm1 = vp.y - sc.dt * sc.gravity[1],
+                        pm2 = vp.z - sc.dt * sc.gravity[2];
+            out = make_float4(gv[0] * im, gv[1] * im, gv[2] * im, -(gv[0] * pm0 + gv[1] * pm1 + gv[2] * pm2) * im);
+        }
+        A.grid_gpm[idx] = out;
+        A.grid_gv[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+constexpr int GATHER_T = 128;
+constexpr int MAX_SMEM_MATS = 64;
+
+template <bool MULTI, bool FLUID>
+__global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
+    __shared__ float sE[MAX_SMEM_MATS];
+    const bool smem_e = V.M <= MAX_SMEM_MATS;
+    for (int m = threadIdx.x; m < MAX_SMEM_MATS; m += blockDim.x) sE[m] = 0.f;
+    __syncthreads();
+    const int64_t N = V.N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint32_t flags = 0;
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < N; ii += stride) {
+        const uint32_t p = V.order[ii];
+        if (p >= (uint32_t)N) {
+            flags |= FLAG_TILE_RANGE;
+            continue;
+        }
+        const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
+        const SceneDev& sc = scene_ref(V, s);
+        const int mid = MULTI ? V.mat[p] : 0;
+        const MatDev mt = V.mats[mid];
+        float x[3], F[9], v[3], C[9], Cn[9], vdum[3];
+        unpack_xF(V.q[p], V.q[N + p], V.q[2 * N + p], x, F);
+        unpack_vC(V.q[3 * N + p], V.q[4 * N + p], V.q[5 * N + p], v, C);
+        unpack_vC(A.q_next[3 * N + p], A.q_next[4 * N + p], A.q_next[5 * N + p], vdum, Cn);
+        float gx[3], gF[9], gv[3], gC[9];
+        unpack_xF(A.g[p], A.g[N + p], A.g[2 * N + p], gx, gF);
+        unpack_vC(A.g[3 * N + p], A.g[4 * N + p], A.g[5 * N + p], gv, gC);
+        const float2 mv = V.mV[p];
+        const float m = mv.x;
+        Stencil st;
+        make_stencil<PHYS_MLS>(sc, x, st, flags);
+        float dw[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            mls_dweights(st.f[a], dw[a]);
+            // a clamped (escaped) coordinate has zero weight derivative
+            const float raw = __fsub_rn(__fdiv_rn(__fsub_rn(x[a], sc.origin[a]), sc.dx), (float)st.s[a]);
+            if (raw < 0.5f || raw > 1.5f) dw[a][0] = dw[a][1] = dw[a][2] = 0.f;
+        }
+        // adjoint through the fluid reset and the F update
+        float M[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) M[a] = sc.dt * Cn[a] + ((a % 4 == 0) ? 1.f : 0.f);
+        if (FLUID && mt.model == MODEL_EOS) {
+            float Fr[9], cof[9];
+            m3_mul(M, F, Fr);
+            m3_cof(Fr, cof);
+            const float J = Fr[0] * cof[0] + Fr[1] * cof[1] + Fr[2] * cof[2];
+            const float c = cbrtf(J) / (3.f * J) * (gF[0] + gF[4] + gF[8]);
+#pragma unroll
+            for (int a = 0; a < 9; ++a) gF[a] = c * cof[a];
+        }
+        float gvt[3], gCt[9], gFFt[9];
+        m3_mulT(gF, F, gFFt);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) gvt[a] = gv[a] + sc.dt * gx[a];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) gCt[a] = gC[a] + sc.dt * gFFt[a];
+        // forward affine matrix
+        float tau[9], Am[9];
+        kirchhoff(F, mt, tau);
+        const float kk = -sc.dt * mv.y * sc.D;
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Am[a] = kk * tau[a] + m * C[a];
+        const float dx = sc.dx, D = sc.D, idx_ = 1.f / dx;
+        float ox[3] = {gx[0], gx[1], gx[2]};
+        float ogv[3] = {0.f, 0.f, 0.f};
+        float Ab[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float dk = ((float)k - st.f[2]) * dx;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float dj = ((float)j - st.f[1]) * dx;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const float di = ((float)i - st.f[0]) * dx;
+                    const int64_t n = node_index(sc, st.s[0] + i, st.s[1] + j, st.s[2] + k);
+                    const float4 vi = __ldg(&V.grid_v[n]);
+                    const float4 gpm = A.grid_gpm[n];
+                    const float w = st.w[0][i] * st.w[1][j] * st.w[2][k];
+                    const float d[3] = {di, dj, dk};
+                    const float vv[3] = {vi.x, vi.y, vi.z};
+                    const float gp[3] = {gpm.x, gpm.y, gpm.z};
+                    float wb = gpm.w * m;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float Cd = gCt[3 * a] * d[0] + gCt[3 * a + 1] * d[1] + gCt[3 * a + 2] * d[2];
+                        const float Ad = Am[3 * a] * d[0] + Am[3 * a + 1] * d[1] + Am[3 * a + 2] * d[2];
+                        wb += gvt[a] * vv[a] + D * vv[a] * Cd + gp[a] * (m * v[a] + Ad);
+                    }
+                    const float gw[3] = {dw[0][i] * st.w[1][j] * st.w[2][k] * idx_,
+                                         st.w[0][i] * dw[1][j] * st.w[2][k] * idx_,
+                                         st.w[0][i] * st.w[1][j] * dw[2][k] * idx_};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float t1 = gCt[a] * vv[0] + gCt[3 + a] * vv[1] + gCt[6 + a] * vv[2];
+                        const float t2 = Am[a] * gp[0] + Am[3 + a] * gp[1] + Am[6 + a] * gp[2];
+                        ox[a] += wb * gw[a] - w * (D * t1 + t2);
+                        ogv[a] += w * m * gp[a];
+#pragma unroll
+                        for (int b = 0; b < 3; ++b) Ab[3 * a + b] += w * gp[a] * d[b];
+                    }
+                }
+            }
+        }
+        // F' = M F  ->  gF_in = M^T gF'raw, plus the stress adjoint
+        float oF[9];
+        m3_Tmul(M, gF, oF);
+        float tb[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) tb[a] = kk * Ab[a];
+        const float dE = kirchhoff_adjoint(F, mt, tb, oF);
+        float oC[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) oC[a] = m * Ab[a];
+        float4 g0, g1, g2, g3, g4, g5;
+        pack_xF(ox, oF, g0, g1, g2);
+        pack_vC(ogv, oC, g3, g4, g5);
+        A.g[p] = g0;
+        A.g[N + p] = g1;
+        A.g[2 * N + p] = g2;
+        A.g[3 * N + p] = g3;
+        A.g[4 * N + p] = g4;
+        A.g[5 * N + p] = g5;
+        if (smem_e) {
+            // lanes of one material combine before one shared atomic
+            const unsigned peers = __match_any_sync(__activemask(), mid);
+            const float e = dE;
+            const int leader = __ffs(peers) - 1;
+            // every peer reads every peer's value; the leader adds the sum once
+            float sum = 0.f;
+            unsigned rest = peers;
+            while (rest) {
+                const int src = __ffs(rest) - 1;
+                rest &= rest - 1;
+                sum += __shfl_sync(peers, e, src);
+            }
+            if ((int)(threadIdx.x & 31) == leader) atomicAdd(&sE[mid], sum);
+        } else {
+            atomicAdd(&A.gE[mid], dE);
+        }
+    }
+    __syncthreads();
+    if (smem_e)
+        for (int m = threadIdx.x; m < V.M; m += blockDim.x)
+            if (sE[m] != 0.f) atomicAdd(&A.gE[m], sE[m]);
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+__global__ void k_state_to_planes(const float* __restrict__ x, const float* __restrict__ v,
+                                  const float* __restrict__ C, const float* __restrict__ F,
+                                  const uint32_t* __restrict__ user_of_phys, float4* __restrict__ g, int64_t N) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+        const int64_t u = user_of_phys[i];
+        if (u >= N) continue;
+        float xx[3], vv[3], CC[9], FF[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            xx[a] = x ? x[3 * u + a] : 0.f;
+            vv[a] = v ? v[3 * u + a] : 0.f;
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) {
+            CC[a] = C ? C[9 * u + a] : 0.f;
+            FF[a] = F ? F[9 * u + a] : 0.f;
+        }
+        float4 o0, o1, o2, o3, o4, o5;
+        pack_xF(xx, FF, o0, o1, o2);
+        pack_vC(vv, CC, o3, o4, o5);
+        g[i] = o0;
+        g[N + i] = o1;
+        g[2 * N + i] = o2;
+        g[3 * N + i] = o3;
+        g[4 * N + i] = o4;
+        g[5 * N + i] = o5;
+    }
+}
+
+__global__ void k_planes_to_state(const float4* __restrict__ g, const uint32_t* __restrict__ user_of_phys,
+                                  float* __restrict__ x, float* __restrict__ v, float* __restrict__ C,
+                                  float* __restrict__ F, int64_t N) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+        const int64_t u = user_of_phys[i];
+        if (u >= N) continue;
+        float xx[3], FF[9], vv[3], CC[9];
+        unpack_xF(g[i], g[N + i], g[2 * N + i], xx, FF);
+        unpack_vC(g[3 * N + i], g[4 * N + i], g[5 * N + i], vv, CC);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (x) x[3 * u + a] = xx[a];
+            if (v) v[3 * u + a] = vv[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) {
+            if (C) C[9 * u + a] = CC[a];
+            if (F) F[9 * u + a] = FF[a];
+        }
+    }
+}
+
+inline int blocks_for(int64_t n, int block) {
+    int64_t g = (n + block - 1) / block;
+    return (int)(g < 1 ? 1 : (g > 148 * 64 ? 148 * 64 : g));
+}
+
+}  // namespace
+
+cudaError_t launch_adj_grid(const View& V, const AdjView& A, const Tuning& t, int num_sms, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    const int tiles_per_block = t.grid_block / 64;
+    int64_t nb = ((int64_t)V.total_nt + tiles_per_block - 1) / tiles_per_block;
+    if (nb > num_sms * 8) nb = num_sms * 8;
+    if (nb < 1) nb = 1;
+    k_adj_grid<<<(int)nb, t.grid_block, 0, st>>>(V, A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_gather(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t,
+                              cudaStream_t st) {
+    (void)t;
+    if (V.N == 0) return cudaSuccess;
+    const int nb = blocks_for(V.N, GATHER_T);
+    if (pf.multi_mat) {
+        if (pf.has_fluid)
+            k_adj_gather<true, true><<<nb, GATHER_T, 0, st>>>(V, A);
+        else
+            k_adj_gather<true, false><<<nb, GATHER_T, 0, st>>>(V, A);
+    } else {
+        if (pf.has_fluid)
+            k_adj_gather<false, true><<<nb, GATHER_T, 0, st>>>(V, A);
+        else
+            k_adj_gather<false, false><<<nb, GATHER_T, 0, st>>>(V, A);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_state_to_planes(const float* x, const float* v, const float* C, const float* F,
+                                   const uint32_t* user_of_phys, float4* g, int64_t N, cudaStream_t st) {
+    if (N == 0) return cudaSuccess;
+    k_state_to_planes<<<blocks_for(N, 256), 256, 0, st>>>(x, v, C, F, user_of_phys, g, N);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_state(const float4* g, const uint32_t* user_of_phys, float* x, float* v, float* C,
+                                   float* F, int64_t N, cudaStream_t st) {
+    if (N == 0) return cudaSuccess;
+    k_planes_to_state<<<blocks_for(N, 256), 256, 0, st>>>(g, user_of_phys, x, v, C, F, N);
+    return cudaGetLastError();
+}
+
+}  // namespace pgmpm

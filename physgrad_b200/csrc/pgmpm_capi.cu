@@ -16,6 +16,8 @@
 #include "../../include/pgmpm.h"
 #include "pgmpm_internal.h"
 
+#include "pgmpm_solver_impl.h"
+
 using namespace pgmpm;
 
 namespace {
@@ -29,7 +31,7 @@ int pgmpm_set_error(int code, const char* msg) {
     return code;
 }
 
-namespace {
+namespace pgmpm {
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -40,140 +42,6 @@ int fail(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
-
-#define CK(expr)                                                                                        \
-    do {                                                                                                \
-        cudaError_t e_ = (expr);                                                                        \
-        if (e_ != cudaSuccess)                                                                          \
-            return fail(e_ == cudaErrorMemoryAllocation ? PGMPM_ERR_OOM : PGMPM_ERR_CUDA, "%s: %s (%s:%d)", \
-                        #expr, cudaGetErrorString(e_), __FILE__, __LINE__);                             \
-    } while (0)
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    cudaError_t alloc(size_t b) {
-        release();
-        if (b == 0) b = 16;
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e == cudaSuccess) bytes = b;
-        return e;
-    }
-    cudaError_t ensure(size_t b) { return bytes >= b ? cudaSuccess : alloc(b); }
-    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
-};
-
-int bits_for(uint64_t v) {
-    int b = 0;
-    while ((1ull << b) < v) ++b;
-    return b < 1 ? 1 : b;
-}
-
-}  // namespace
-
-struct pgmpm_solver_s {
-    int device = 0;
-    int num_sms = 148;
-    int S = 0, M = 0;
-    int64_t N = 0;
-    std::vector<pgmpm_scene_desc> desc;
-    std::vector<SceneDev> scenes;
-    std::vector<pgmpm_material> mats_h;
-    std::vector<int64_t> counts;
-    PhysFlags pf{};
-    int total_ct = 0, total_nt = 0;
-    int key_bits = 1;
-    int sort_which = 0;
-    Tuning tune;
-    bool use_graph = true;
-    bool profiling = false;
-    bool uploaded = false;
-
-    // device buffers
-    DevBuf d_scenes, d_mats, q, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
-    DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
-    uint32_t* h_counters = nullptr;  // pinned
-
-    // graph
-    cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t step_exec = nullptr;
-    cudaGraph_t step_graph = nullptr;
-    cudaEvent_t ev[6] = {};
-
-    // metrics
-    pgmpm_metrics met{};
-
-    // differentiation state (pgmpm_forward_checkpointed / pgmpm_backward)
-    int ck_steps = 0, ck_every = 0;
-    DevBuf ck_states;   // checkpoints: (ceil(steps/every)) x 6N float4
-    DevBuf tape_q, tape_keys, tape_order, tape_grid, adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;
-
-    View view() const {
-        View V;
-        V.N = N;
-        V.S = S;
-        V.M = M;
-        V.scenes = d_scenes.as<SceneDev>();
-        V.mats = d_mats.as<MatDev>();
-        V.q = q.as<float4>();
-        V.mV = mV.as<float2>();
-        V.mat = pf.multi_mat ? mat.as<int32_t>() : nullptr;
-        V.keys = keys.as<uint32_t>();
-        V.skeys = sort_which ? kb.as<uint32_t>() : ka.as<uint32_t>();
-        V.order = sort_which ? vb.as<uint32_t>() : va.as<uint32_t>();
-        V.grid_mp = grid_mp.as<float4>();
-        V.grid_v = grid_v.as<float4>();
-        V.grid_vpre = nullptr;
-        V.tile_flags = tile_flags.as<uint32_t>();
-        V.tile_list = tile_list.as<uint32_t>();
-        V.ctile_list = ctile_list.as<uint32_t>();
-        V.ctile_range = ctile_range.as<uint2>();
-        V.counters = counters.as<uint32_t>();
-        V.total_ct = total_ct;
-        V.total_nt = total_nt;
-        return V;
-    }
-
-    void drop_graph() {
-        if (step_exec) cudaGraphExecDestroy(step_exec);
-        if (step_graph) cudaGraphDestroy(step_graph);
-        step_exec = nullptr;
-        step_graph = nullptr;
-    }
-
-    ~pgmpm_solver_s() {
-        int prev = 0;
-        cudaGetDevice(&prev);
-        cudaSetDevice(device);
-        drop_graph();
-        if (cap_stream) cudaStreamDestroy(cap_stream);
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-        if (h_counters) cudaFreeHost(h_counters);
-        cudaSetDevice(prev);
-    }
-};
-
-namespace {
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int d) {
-        cudaGetDevice(&prev);
-        if (prev != d) cudaSetDevice(d);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 int material_to_dev(const pgmpm_material& m, MatDev& d) {
     if (m.type == PGMPM_MAT_FLUID) {
@@ -202,24 +70,21 @@ int material_to_dev(const pgmpm_material& m, MatDev& d) {
     return PGMPM_OK;
 }
 
-cudaStream_t ST(void* s) { return reinterpret_cast<cudaStream_t>(s); }
-
-int record_step(pgmpm_solver s, cudaStream_t st, bool timed) {
+int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) {
     if (s->N == 0) {  // nothing to move; keep the timing events consistent
         if (timed)
             for (int i = 0; i < 5; ++i) CK(cudaEventRecord(s->ev[i], st));
         return PGMPM_OK;
     }
-    View V = s->view();
-    // per-step resets: active tile flags, tile count and active node count
-    CK(cudaMemsetAsync(s->tile_flags.p, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
-    CK(cudaMemsetAsync(s->counters.p, 0, sizeof(uint32_t) * CNT_RESET, st));
+    View V = s->view_for(b);
+    // per-step resets: active tile flags, tile counts, active node count, work cursors
+    CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
+    CK(cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * CNT_RESET, st));
     if (timed) CK(cudaEventRecord(s->ev[0], st));
     int which = 0;
-    CK(radix_sort_pairs(s->keys.as<uint32_t>(), nullptr, s->ka.as<uint32_t>(), s->va.as<uint32_t>(),
-                        s->kb.as<uint32_t>(), s->vb.as<uint32_t>(), s->sort_scratch.as<uint32_t>(), s->N,
+    CK(radix_sort_pairs(b.keys_in, nullptr, b.ka, b.va, b.kb, b.vb, s->sort_scratch.as<uint32_t>(), s->N,
                         s->key_bits, &which, st));
-    if (which != s->sort_which) return fail(PGMPM_ERR_STATE, "internal: sort buffer parity changed");
+    if (which != b.which) return fail(PGMPM_ERR_STATE, "internal: sort buffer parity changed");
     CK(launch_mark(V, st));
     if (timed) CK(cudaEventRecord(s->ev[1], st));
     CK(launch_p2g(V, s->pf, s->tune, s->num_sms, st));
@@ -231,10 +96,14 @@ int record_step(pgmpm_solver s, cudaStream_t st, bool timed) {
     return PGMPM_OK;
 }
 
+}  // namespace pgmpm
+
+namespace {
+
 int build_graph(pgmpm_solver s) {
     s->drop_graph();
     CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
-    int rc = record_step(s, s->cap_stream, false);
+    int rc = record_step(s, s->live_bufs(), s->cap_stream, false);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
     if (rc != PGMPM_OK) {
@@ -247,11 +116,14 @@ int build_graph(pgmpm_solver s) {
     return PGMPM_OK;
 }
 
+}  // namespace
+
+namespace pgmpm {
 int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
     if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
     for (int k = 0; k < n_steps; ++k) {
         if (s->profiling) {
-            int rc = record_step(s, st, true);
+            int rc = record_step(s, s->live_bufs(), st, true);
             if (rc) return rc;
             CK(cudaEventSynchronize(s->ev[4]));
             float a, b, c, d;
@@ -274,7 +146,7 @@ int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
             }
             CK(cudaGraphLaunch(s->step_exec, st));
         } else {
-            int rc = record_step(s, st, false);
+            int rc = record_step(s, s->live_bufs(), st, false);
             if (rc) return rc;
         }
         s->met.total_steps++;
@@ -692,7 +564,7 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
         return PGMPM_OK;
     };
     // one real step so the sorted order, tile lists and grid velocity exist
-    int rc = record_step(s, st, false);
+    int rc = record_step(s, s->live_bufs(), st, false);
     if (rc) return rc;
     for (const Cand& c : p2g_c) {
         Tuning t = keep;

@@ -1,8 +1,260 @@
-// pgmpm_diff.cu -- differentiation entry points (filled in below).
-#include "../../include/pgmpm.h"
+// pgmpm_diff.cu -- checkpointed differentiation of the MLS-MPM step
+// (pgmpm_forward_checkpointed / pgmpm_backward) and the reference-shaped
+// launcher launch_mpm_timestep_forward.
+//
+// Forward: the state (6 planes + keys) is copied to a checkpoint every k
+// steps (CheckpointStrategy::UNIFORM of src/differentiable_mpm.h:66).
+// Backward, segment by segment from the last: the segment is replayed from
+// its checkpoint into per-step tape slots (state j and j+1, keys, the sort's
+// order, tile lists, grid v and v before the walls) using the same step
+// kernels pointed at the tape, then the three reverse kernels run for each
+// step from the last to the first.  Tape depth = k steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "pgmpm_solver_impl.h"
+
+using namespace pgmpm;
+
+namespace {
+
+size_t nodes_of(pgmpm_solver s) { return (size_t)s->total_nt * 64; }
+
+int ensure_tape(pgmpm_solver s, int slots) {
+    if (s->tape_slots >= slots && s->tape_q.p) return PGMPM_OK;
+    const size_t N = (size_t)std::max<int64_t>(s->N, 1);
+    const size_t nodes = nodes_of(s);
+    s->tape_slots = 0;
+    CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1)));
+    CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1)));
+    CK(s->tape_sk.alloc(sizeof(uint32_t) * N * slots));
+    CK(s->tape_ord.alloc(sizeof(uint32_t) * N * slots));
+    CK(s->tape_gv.alloc(sizeof(float4) * nodes * slots));
+    CK(s->tape_gvpre.alloc(sizeof(float4) * nodes * slots));
+    CK(s->tape_flags.alloc(sizeof(uint32_t) * (size_t)s->total_nt * slots));
+    CK(s->tape_tiles.alloc(sizeof(uint32_t) * (size_t)s->total_nt * slots));
+    CK(s->tape_ctiles.alloc(sizeof(uint32_t) * (size_t)s->total_ct * slots));
+    CK(s->tape_crange.alloc(sizeof(uint2) * (size_t)s->total_ct * slots));
+    CK(s->tape_counters.alloc(sizeof(uint32_t) * CNT_WORDS * slots));
+    s->tape_slots = slots;
+    return PGMPM_OK;
+}
+
+// Buffers of tape slot j: the step from state j (tape_q[j]) to state j+1.
+StepBufs tape_bufs(pgmpm_solver s, int j) {
+    const size_t N = (size_t)std::max<int64_t>(s->N, 1);
+    const size_t nodes = nodes_of(s);
+    StepBufs b;
+    b.q = s->tape_q.as<float4>() + 6 * N * j;
+    b.q_out = s->tape_q.as<float4>() + 6 * N * (j + 1);
+    b.keys_in = s->tape_keys.as<uint32_t>() + N * j;
+    b.keys_out = s->tape_keys.as<uint32_t>() + N * (j + 1);
+    uint32_t* sk = s->tape_sk.as<uint32_t>() + N * j;
+    uint32_t* so = s->tape_ord.as<uint32_t>() + N * j;
+    // the sort's last pass must land in the slot: pair a when which == 0
+    b.which = s->sort_which;
+    if (b.which == 0) {
+        b.ka = sk;
+        b.va = so;
+        b.kb = s->kb.as<uint32_t>();
+        b.vb = s->vb.as<uint32_t>();
+    } else {
+        b.ka = s->ka.as<uint32_t>();
+        b.va = s->va.as<uint32_t>();
+        b.kb = sk;
+        b.vb = so;
+    }
+    b.grid_v = s->tape_gv.as<float4>() + nodes * j;
+    b.grid_vpre = s->tape_gvpre.as<float4>() + nodes * j;
+    b.tile_flags = s->tape_flags.as<uint32_t>() + (size_t)s->total_nt * j;
+    b.tile_list = s->tape_tiles.as<uint32_t>() + (size_t)s->total_nt * j;
+    b.ctile_list = s->tape_ctiles.as<uint32_t>() + (size_t)s->total_ct * j;
+    b.ctile_range = s->tape_crange.as<uint2>() + (size_t)s->total_ct * j;
+    b.counters = s->tape_counters.as<uint32_t>() + CNT_WORDS * j;
+    return b;
+}
+
+}  // namespace
+
 extern "C" {
-int pgmpm_forward_checkpointed(pgmpm_solver, int32_t, int32_t, void*) { return PGMPM_ERR_UNSUPPORTED; }
-int pgmpm_backward(pgmpm_solver, const float*, const float*, const float*, const float*, float*, float*, float*,
-                   float*, float*, int32_t, void*) { return PGMPM_ERR_UNSUPPORTED; }
-void launch_mpm_timestep_forward(float*, float*, const float*, int, int, float, const float*, void*) {}
+
+int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoint_every, void* stream) {
+    if (!s || n_steps < 1 || checkpoint_every < 1) return fail(PGMPM_ERR_ARG, "need n_steps >= 1, checkpoint_every >= 1");
+    if (s->pf.physics != PHYS_MLS) return fail(PGMPM_ERR_UNSUPPORTED, "differentiation needs PGMPM_PHYSICS_MLS");
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const int k = std::min(checkpoint_every, n_steps);
+    const int nseg = (n_steps + k - 1) / k;
+    const size_t N = (size_t)std::max<int64_t>(s->N, 1);
+    CK(s->ck_q.ensure(sizeof(float4) * 6 * N * nseg));
+    CK(s->ck_keys.ensure(sizeof(uint32_t) * N * nseg));
+    s->ck_valid = false;
+    for (int seg = 0; seg < nseg; ++seg) {
+        CK(cudaMemcpyAsync(s->ck_q.as<float4>() + 6 * N * seg, s->q.p, sizeof(float4) * 6 * N,
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->ck_keys.as<uint32_t>() + N * seg, s->keys.p, sizeof(uint32_t) * N,
+                           cudaMemcpyDeviceToDevice, st));
+        const int len = std::min(k, n_steps - seg * k);
+        int rc = run_steps(s, len, st);
+        if (rc) return rc;
+    }
+    s->ck_steps = n_steps;
+    s->ck_every = k;
+    s->ck_count = nseg;
+    s->ck_valid = true;
+    return PGMPM_OK;
+}
+
+int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, const float* gC_out, const float* gF_out,
+                   float* gx_in, float* gv_in, float* gC_in, float* gF_in, float* gE, int32_t ptr_kind, void* stream) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (!s->ck_valid) return fail(PGMPM_ERR_STATE, "call pgmpm_forward_checkpointed first");
+    if (ptr_kind != PGMPM_PTR_HOST && ptr_kind != PGMPM_PTR_DEVICE) return fail(PGMPM_ERR_ARG, "bad ptr_kind");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const int64_t N = s->N;
+    const size_t Nz = (size_t)std::max<int64_t>(N, 1);
+    const int M = s->M;
+    int rc = ensure_tape(s, s->ck_every);
+    if (rc) return rc;
+    CK(s->adj_g.ensure(sizeof(float4) * 6 * Nz));
+    CK(s->adj_grid_gv.ensure(sizeof(float4) * nodes_of(s)));
+    CK(s->adj_grid_gpm.ensure(sizeof(float4) * nodes_of(s)));
+    CK(s->adj_gE.ensure(sizeof(float) * M));
+    CK(cudaMemsetAsync(s->adj_grid_gv.p, 0, s->adj_grid_gv.bytes, st));
+    CK(cudaMemsetAsync(s->adj_gE.p, 0, sizeof(float) * M, st));
+    // output adjoint (upload order) -> physical planes
+    const float *dx = gx_out, *dv = gv_out, *dC = gC_out, *dF = gF_out;
+    if (ptr_kind == PGMPM_PTR_HOST && N > 0) {
+        CK(s->adj_stage.ensure(sizeof(float) * 24 * Nz));
+        float* b = s->adj_stage.as<float>();
+        float *sx = b, *sv = b + 3 * N, *sC = b + 6 * N, *sF = b + 15 * N;
+        if (gx_out) CK(cudaMemcpyAsync(sx, gx_out, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, st));
+        if (gv_out) CK(cudaMemcpyAsync(sv, gv_out, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, st));
+        if (gC_out) CK(cudaMemcpyAsync(sC, gC_out, sizeof(float) * 9 * N, cudaMemcpyHostToDevice, st));
+        if (gF_out) CK(cudaMemcpyAsync(sF, gF_out, sizeof(float) * 9 * N, cudaMemcpyHostToDevice, st));
+        dx = gx_out ? sx : nullptr;
+        dv = gv_out ? sv : nullptr;
+        dC = gC_out ? sC : nullptr;
+        dF = gF_out ? sF : nullptr;
+    }
+    CK(launch_state_to_planes(dx, dv, dC, dF, s->user_of_phys.as<uint32_t>(), s->adj_g.as<float4>(), N, st));
+    AdjView A;
+    A.g = s->adj_g.as<float4>();
+    A.grid_gv = s->adj_grid_gv.as<float4>();
+    A.grid_gpm = s->adj_grid_gpm.as<float4>();
+    A.gE = s->adj_gE.as<float>();
+    const int k = s->ck_every;
+    for (int seg = s->ck_count - 1; seg >= 0 && N > 0; --seg) {
+        const int len = std::min(k, s->ck_steps - seg * k);
+        CK(cudaMemcpyAsync(s->tape_q.p, s->ck_q.as<float4>() + 6 * Nz * seg, sizeof(float4) * 6 * Nz,
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->tape_keys.p, s->ck_keys.as<uint32_t>() + Nz * seg, sizeof(uint32_t) * Nz,
+                           cudaMemcpyDeviceToDevice, st));
+        for (int j = 0; j < len; ++j) {
+            rc = record_step(s, tape_bufs(s, j), st, false);
+            if (rc) return rc;
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            StepBufs b = tape_bufs(s, j);
+            View V = s->view_for(b);
+            V.grid_mp = A.grid_gv;  // scatter target of the G2P reverse
+            A.q_next = b.q_out;
+            CK(cudaMemsetAsync(b.counters + CNT_P2G_CURSOR, 0, sizeof(uint32_t), st));
+            CK(launch_adj_scatter(V, A, s->pf, s->tune, s->num_sms, st));
+            CK(launch_adj_grid(V, A, s->tune, s->num_sms, st));
+            CK(launch_adj_gather(V, A, s->pf, s->tune, st));
+        }
+    }
+    // physical planes -> caller's arrays (upload order)
+    if (ptr_kind == PGMPM_PTR_DEVICE) {
+        CK(launch_planes_to_state(A.g, s->user_of_phys.as<uint32_t>(), gx_in, gv_in, gC_in, gF_in, N, st));
+        if (gE) CK(cudaMemcpyAsync(gE, A.gE, sizeof(float) * M, cudaMemcpyDeviceToDevice, st));
+        return PGMPM_OK;
+    }
+    CK(s->adj_stage.ensure(sizeof(float) * 24 * Nz));
+    float* b = s->adj_stage.as<float>();
+    float *sx = b, *sv = b + 3 * N, *sC = b + 6 * N, *sF = b + 15 * N;
+    CK(launch_planes_to_state(A.g, s->user_of_phys.as<uint32_t>(), gx_in ? sx : nullptr, gv_in ? sv : nullptr,
+                              gC_in ? sC : nullptr, gF_in ? sF : nullptr, N, st));
+    if (gx_in && N) CK(cudaMemcpyAsync(gx_in, sx, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
+    if (gv_in && N) CK(cudaMemcpyAsync(gv_in, sv, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
+    if (gC_in && N) CK(cudaMemcpyAsync(gC_in, sC, sizeof(float) * 9 * N, cudaMemcpyDeviceToHost, st));
+    if (gF_in && N) CK(cudaMemcpyAsync(gF_in, sF, sizeof(float) * 9 * N, cudaMemcpyDeviceToHost, st));
+    if (gE) CK(cudaMemcpyAsync(gE, A.gE, sizeof(float) * M, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PGMPM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------
+// launch_mpm_timestep_forward: src/pytorch_autograd.cu:371-382 shape.
+// One REF_COMPAT step on the unit cube with a grid_resolution^3 grid.  A
+// solver per (device, particle count, resolution) is kept for the process so
+// repeated calls reuse their device buffers.
+namespace {
+std::mutex g_launch_mu;
+std::map<std::tuple<int, int, int>, pgmpm_solver> g_launch_solvers;
+}  // namespace
+
+extern "C" void launch_mpm_timestep_forward(float* positions, float* velocities, const float* masses,
+                                            int num_particles, int grid_resolution, float dt, const float* gravity,
+                                            void* stream) {
+    if (num_particles < 0 || grid_resolution < 4 || !(dt > 0.f) || (num_particles > 0 && (!positions || !velocities || !masses))) {
+        fail(PGMPM_ERR_ARG, "launch_mpm_timestep_forward: invalid arguments");
+        return;
+    }
+    if (num_particles == 0) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaStream_t st = ST(stream);
+    pgmpm_solver s = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_launch_mu);
+        auto key = std::make_tuple(dev, num_particles, grid_resolution);
+        auto it = g_launch_solvers.find(key);
+        if (it == g_launch_solvers.end()) {
+            pgmpm_scene_desc d{};
+            d.n[0] = d.n[1] = d.n[2] = grid_resolution;
+            d.physics = PGMPM_PHYSICS_REF_COMPAT;
+            d.boundary = PGMPM_BC_NONE;
+            d.dx = 1.0f / (float)grid_resolution;
+            d.dt = dt;
+            const int64_t cnt = num_particles;
+            pgmpm_material mat{PGMPM_MAT_ELASTIC, PGMPM_MODEL_FIXED_COROTATED, 1e6f, 0.3f, 1000.f};
+            if (pgmpm_create(&d, 1, &cnt, &mat, 1, dev, &s) != PGMPM_OK) return;
+            g_launch_solvers[key] = s;
+        } else {
+            s = it->second;
+        }
+    }
+    // per-call dt and gravity (device pointer) into the scene table
+    if (s->scenes[0].dt != dt) {
+        s->scenes[0].dt = dt;
+        if (cudaMemcpyAsync(&s->d_scenes.as<SceneDev>()[0].dt, &s->scenes[0].dt, sizeof(float),
+                            cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            fail(PGMPM_ERR_CUDA, "launch_mpm_timestep_forward: dt update failed");
+            return;
+        }
+        cudaStreamSynchronize(st);
+    }
+    if (gravity) {
+        if (cudaMemcpyAsync(&s->d_scenes.as<SceneDev>()[0].gravity[0], gravity, 3 * sizeof(float),
+                            cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+            fail(PGMPM_ERR_CUDA, "launch_mpm_timestep_forward: gravity copy failed");
+            return;
+        }
+    }
+    std::vector<float> ones;  // volumes are not used by the REF_COMPAT physics
+    if (pgmpm_upload(s, positions, velocities, nullptr, nullptr, masses, nullptr, nullptr, PGMPM_PTR_DEVICE, stream))
+        return;
+    if (pgmpm_step(s, 1, stream)) return;
+    pgmpm_download(s, positions, velocities, nullptr, nullptr, PGMPM_PTR_DEVICE, stream);
 }

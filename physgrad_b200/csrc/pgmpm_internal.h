@@ -29,7 +29,8 @@ struct View {
     int S, M;
     const SceneDev* scenes;
     const MatDev* mats;
-    float4* q;                 // 6 planes of N float4
+    float4* q;                 // 6 planes of N float4 (state at the start of the step)
+    float4* q_out;             // where G2P writes the new state (== q in place; MLS only otherwise)
     const float2* mV;          // (mass, V0)
     const int32_t* mat;        // material id (null when M == 1)
     uint32_t* keys;            // cell key per particle (physical order), input of the next sort
@@ -92,17 +93,20 @@ cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x,
 cudaError_t launch_grid_download(const View& V, int scene, const SceneDev& sc, float* mass, float* vel,
                                  cudaStream_t st);
 
-// pgmpm_adjoint.cu
+// Reverse pass of one MLS step (pgmpm_adjoint.cu, and the scatter in
+// pgmpm_kernels.cu).  V describes the step as it ran (V.q = state before the
+// step, order / tiles / grid_v / grid_vpre of the step); V.grid_mp is the
+// scatter target for dL/dv_i.
 struct AdjView {
     // adjoint of the particle state after the step, overwritten with the
     // adjoint of the state before it (physical order, same plane packing)
     float4* g;                 // 6 planes
-    const float4* q_next;      // state after the step (for C' and F'raw)
-    float4* grid_gv;           // (dL/dv_i, -) scatter target, zeroed by the grid adjoint
+    const float4* q_next;      // state after the step (C' for the F update and the fluid reset)
+    float4* grid_gv;           // (0, dL/dv_i) scatter target, zeroed by the grid adjoint
     float4* grid_gpm;          // (dL/dp_i, dL/dm_i) per node
     float* gE;                 // [M] dL/dE accumulators
 };
-cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t,
+cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t, int num_sms,
                                cudaStream_t st);
 cudaError_t launch_adj_grid(const View& V, const AdjView& A, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_adj_gather(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t,

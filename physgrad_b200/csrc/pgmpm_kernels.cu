@@ -260,8 +260,14 @@ constexpr int PAY_B = 10;   // MLS: m v - (A dx) f ;  REF: v
 constexpr int PAY_A = 13;   // MLS: A dx (row-major)
 constexpr int PAY_MLS = 22;
 
-template <int PHYS, bool MULTI>
-__global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V) {
+// MODE: forward MLS, forward REF_COMPAT, or the reverse of G2P (dL/dv_i
+// scatter, same accumulation skeleton with an adjoint payload and no mass
+// channel).
+enum { MODE_MLS = 0, MODE_REF = 1, MODE_ADJ = 2 };
+
+template <int MODE, bool MULTI, bool FLUID>
+__global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V, AdjView AV) {
+    constexpr int PHYS = MODE == MODE_REF ? PHYS_REF : PHYS_MLS;
     __shared__ float sm[27 * 4 * 64];  // payload [22][P2G_SC], then transpose [27][4][64]
     __shared__ uint32_t cb[64], ce[64];
     __shared__ uint32_t s_work;
@@ -321,7 +327,43 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V) {
                 for (int a = 0; a < 3; ++a)
 #pragma unroll
                     for (int k = 0; k < 3; ++k) sm[(PAY_W + 3 * a + k) * P2G_SC + j] = st.w[a][k];
-                if (PHYS == PHYS_MLS) {
+                if (MODE == MODE_ADJ) {
+                    // reverse of G2P: dL/dv_i += w_i (gv + D gC d_i), with
+                    // gv = dL/dv' + dt dL/dx' and gC = dL/dC' + dt dL/dF'raw F^T
+                    const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+                    float xx[3], F[9];
+                    unpack_xF(q0, q1, q2, xx, F);
+                    float gx[3], gF[9], gv[3], gC[9];
+                    unpack_xF(AV.g[p], AV.g[N + p], AV.g[2 * N + p], gx, gF);
+                    unpack_vC(AV.g[3 * N + p], AV.g[4 * N + p], AV.g[5 * N + p], gv, gC);
+                    if (FLUID && V.mats[MULTI ? V.mat[p] : 0].model == MODEL_EOS) {
+                        // F' = cbrt(det Fraw) I, Fraw = (I + dt C') F
+                        float Cn[9], vdum[3], M[9], Fr[9], cof[9];
+                        unpack_vC(AV.q_next[3 * N + p], AV.q_next[4 * N + p], AV.q_next[5 * N + p], vdum, Cn);
+#pragma unroll
+                        for (int a = 0; a < 9; ++a) M[a] = sc.dt * Cn[a] + ((a % 4 == 0) ? 1.f : 0.f);
+                        m3_mul(M, F, Fr);
+                        m3_cof(Fr, cof);
+                        const float J = Fr[0] * cof[0] + Fr[1] * cof[1] + Fr[2] * cof[2];
+                        const float c = cbrtf(J) / (3.f * J) * (gF[0] + gF[4] + gF[8]);
+#pragma unroll
+                        for (int a = 0; a < 9; ++a) gF[a] = c * cof[a];
+                    }
+                    float gFFt[9];
+                    m3_mulT(gF, F, gFFt);
+                    const float sD = sc.D * sc.dx;
+                    float Ad[9];
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) Ad[a] = sD * (gC[a] + sc.dt * gFFt[a]);
+                    sm[PAY_M * P2G_SC + j] = 0.f;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        sm[(PAY_B + a) * P2G_SC + j] = (gv[a] + sc.dt * gx[a]) -
+                                                       (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] +
+                                                        Ad[3 * a + 2] * st.f[2]);
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) sm[(PAY_A + a) * P2G_SC + j] = Ad[a];
+                } else if (PHYS == PHYS_MLS) {
                     const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
                     const float4 q3 = V.q[3 * N + p], q4 = V.q[4 * N + p], q5 = V.q[5 * N + p];
                     float xx[3], F[9], v[3], C[9];
@@ -455,7 +497,8 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V) {
                         acc.w += sm[(o * 4 + 3) * 64 + c];
                     }
             const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
-            if (acc.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+            const bool any = MODE == MODE_ADJ ? (acc.y != 0.f || acc.z != 0.f || acc.w != 0.f) : acc.x != 0.f;
+            if (any && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
                 atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], acc);
         }
         __syncthreads();
@@ -568,12 +611,13 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
         float4 o0, o1, o2, o3, o4, o5;
         pack_xF(x, Fn, o0, o1, o2);
         pack_vC(nv, C, o3, o4, o5);
-        V.q[p] = o0;
-        V.q[N + p] = o1;
-        V.q[2 * N + p] = o2;
-        V.q[3 * N + p] = o3;
-        V.q[4 * N + p] = o4;
-        V.q[5 * N + p] = o5;
+        float4* qo = V.q_out;
+        qo[p] = o0;
+        qo[N + p] = o1;
+        qo[2 * N + p] = o2;
+        qo[3 * N + p] = o3;
+        qo[4 * N + p] = o4;
+        qo[5 * N + p] = o5;
     } else {
         // material_point_method.h:599-666 in the same order of operations
         float nv[3] = {0.f, 0.f, 0.f};
@@ -794,17 +838,37 @@ cudaError_t launch_mark(const View& V, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags& pf, const Tuning& t, int num_sms,
+                               cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
+    const int nb = num_sms * t.tile_blocks_per_sm;
+    if (pf.multi_mat) {
+        if (pf.has_fluid)
+            k_p2g_tiles<MODE_ADJ, true, true><<<nb, P2G_T, 0, st>>>(V, A);
+        else
+            k_p2g_tiles<MODE_ADJ, true, false><<<nb, P2G_T, 0, st>>>(V, A);
+    } else {
+        if (pf.has_fluid)
+            k_p2g_tiles<MODE_ADJ, false, true><<<nb, P2G_T, 0, st>>>(V, A);
+        else
+            k_p2g_tiles<MODE_ADJ, false, false><<<nb, P2G_T, 0, st>>>(V, A);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     if (t.p2g_variant == 0) {
         const int nb = num_sms * t.tile_blocks_per_sm;
+        const AdjView none{};
         if (pf.physics == PHYS_MLS) {
             if (pf.multi_mat)
-                k_p2g_tiles<PHYS_MLS, true><<<nb, P2G_T, 0, st>>>(V);
+                k_p2g_tiles<MODE_MLS, true, false><<<nb, P2G_T, 0, st>>>(V, none);
             else
-                k_p2g_tiles<PHYS_MLS, false><<<nb, P2G_T, 0, st>>>(V);
+                k_p2g_tiles<MODE_MLS, false, false><<<nb, P2G_T, 0, st>>>(V, none);
         } else {
-            k_p2g_tiles<PHYS_REF, false><<<nb, P2G_T, 0, st>>>(V);
+            k_p2g_tiles<MODE_REF, false, false><<<nb, P2G_T, 0, st>>>(V, none);
         }
         return cudaGetLastError();
     }

@@ -1,0 +1,211 @@
+// pgmpm_solver_impl.h -- the solver handle behind pgmpm_solver and the step
+// recorder, shared by the C-ABI translation units (pgmpm_capi.cu,
+// pgmpm_diff.cu).  Not installed.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pgmpm.h"
+#include "pgmpm_internal.h"
+
+namespace pgmpm {
+
+// Records an error message for pgmpm_last_error() and returns code.
+int fail(int code, const char* fmt, ...);
+
+#define CK(expr)                                                                                             \
+    do {                                                                                                     \
+        cudaError_t e_ = (expr);                                                                             \
+        if (e_ != cudaSuccess)                                                                               \
+            return ::pgmpm::fail(e_ == cudaErrorMemoryAllocation ? PGMPM_ERR_OOM : PGMPM_ERR_CUDA,           \
+                                 "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__);       \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t b) {
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    cudaError_t ensure(size_t b) { return bytes >= b ? cudaSuccess : alloc(b); }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+inline int bits_for(uint64_t v) {
+    int b = 0;
+    while ((1ull << b) < v) ++b;
+    return b < 1 ? 1 : b;
+}
+
+// Buffers one step reads and writes.  The live solver uses its own; the
+// reverse pass replays steps into per-step tape slots.
+struct StepBufs {
+    float4* q;             // state at the start of the step (read by P2G and G2P)
+    float4* q_out;         // state G2P writes (== q for the live solver)
+    uint32_t* keys_in;     // keys sorted by this step
+    uint32_t* keys_out;    // keys G2P writes for the next step (may equal keys_in)
+    uint32_t *ka, *va, *kb, *vb;  // sort ping-pong; result in (ka, va) if which == 0 else (kb, vb)
+    int which;
+    float4* grid_v;
+    float4* grid_vpre;     // may be null
+    uint32_t* tile_flags;
+    uint32_t* tile_list;
+    uint32_t* ctile_list;
+    uint2* ctile_range;
+    uint32_t* counters;
+};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+inline cudaStream_t ST(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int material_to_dev(const pgmpm_material& m, MatDev& d);
+
+}  // namespace pgmpm
+
+struct pgmpm_solver_s {
+    int device = 0;
+    int num_sms = 148;
+    int S = 0, M = 0;
+    int64_t N = 0;
+    std::vector<pgmpm_scene_desc> desc;
+    std::vector<pgmpm::SceneDev> scenes;
+    std::vector<pgmpm_material> mats_h;
+    std::vector<int64_t> counts;
+    pgmpm::PhysFlags pf{};
+    int total_ct = 0, total_nt = 0;
+    int key_bits = 1;
+    int sort_which = 0;
+    pgmpm::Tuning tune;
+    bool use_graph = true;
+    bool profiling = false;
+    bool uploaded = false;
+
+    // device buffers
+    pgmpm::DevBuf d_scenes, d_mats, q, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
+    pgmpm::DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
+    uint32_t* h_counters = nullptr;  // pinned
+
+    // graph
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    cudaGraph_t step_graph = nullptr;
+    cudaEvent_t ev[6] = {};
+
+    // metrics
+    pgmpm_metrics met{};
+
+    // differentiation (pgmpm_forward_checkpointed / pgmpm_backward)
+    int ck_steps = 0, ck_every = 0, ck_count = 0;
+    bool ck_valid = false;
+    pgmpm::DevBuf ck_q, ck_keys;         // checkpoints: states (6N float4) + keys (N u32)
+    int tape_slots = 0;                  // allocated tape depth (steps per segment)
+    pgmpm::DevBuf tape_q, tape_keys;     // (slots + 1) states and keys
+    pgmpm::DevBuf tape_sk, tape_ord;     // slots x N sorted keys / order
+    pgmpm::DevBuf tape_gv, tape_gvpre;   // slots x nodes float4
+    pgmpm::DevBuf tape_flags, tape_tiles, tape_ctiles, tape_crange, tape_counters;
+    pgmpm::DevBuf adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;
+
+    pgmpm::StepBufs live_bufs() const {
+        pgmpm::StepBufs b;
+        b.q = q.as<float4>();
+        b.q_out = q.as<float4>();
+        b.keys_in = keys.as<uint32_t>();
+        b.keys_out = keys.as<uint32_t>();
+        b.ka = ka.as<uint32_t>();
+        b.va = va.as<uint32_t>();
+        b.kb = kb.as<uint32_t>();
+        b.vb = vb.as<uint32_t>();
+        b.which = sort_which;
+        b.grid_v = grid_v.as<float4>();
+        b.grid_vpre = nullptr;
+        b.tile_flags = tile_flags.as<uint32_t>();
+        b.tile_list = tile_list.as<uint32_t>();
+        b.ctile_list = ctile_list.as<uint32_t>();
+        b.ctile_range = ctile_range.as<uint2>();
+        b.counters = counters.as<uint32_t>();
+        return b;
+    }
+
+    pgmpm::View view_for(const pgmpm::StepBufs& b) const {
+        pgmpm::View V;
+        V.N = N;
+        V.S = S;
+        V.M = M;
+        V.scenes = d_scenes.as<pgmpm::SceneDev>();
+        V.mats = d_mats.as<pgmpm::MatDev>();
+        V.q = b.q;
+        V.q_out = b.q_out;
+        V.mV = mV.as<float2>();
+        V.mat = pf.multi_mat ? mat.as<int32_t>() : nullptr;
+        V.keys = b.keys_out;
+        V.skeys = b.which ? b.kb : b.ka;
+        V.order = b.which ? b.vb : b.va;
+        V.grid_mp = grid_mp.as<float4>();
+        V.grid_v = b.grid_v;
+        V.grid_vpre = b.grid_vpre;
+        V.tile_flags = b.tile_flags;
+        V.tile_list = b.tile_list;
+        V.ctile_list = b.ctile_list;
+        V.ctile_range = b.ctile_range;
+        V.counters = b.counters;
+        V.total_ct = total_ct;
+        V.total_nt = total_nt;
+        return V;
+    }
+
+    pgmpm::View view() const { return view_for(live_bufs()); }
+
+    void drop_graph() {
+        if (step_exec) cudaGraphExecDestroy(step_exec);
+        if (step_graph) cudaGraphDestroy(step_graph);
+        step_exec = nullptr;
+        step_graph = nullptr;
+    }
+
+    ~pgmpm_solver_s() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        drop_graph();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (h_counters) cudaFreeHost(h_counters);
+        cudaSetDevice(prev);
+    }
+};
+
+namespace pgmpm {
+// Enqueue one step on `st` using buffers `b` (events ev[0..4] when timed).
+int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed);
+// Run n steps of the live state (graph, eager or profiled).
+int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st);
+}  // namespace pgmpm

@@ -1,0 +1,166 @@
+"""GPU adjoint (pgmpm_forward_checkpointed / pgmpm_backward) against the FP64
+oracle adjoint and against central finite differences of the GPU forward.
+
+Tolerances:
+  * vs the FP64 oracle adjoint: per field, max |gpu - oracle| <= 2e-3 *
+    max |oracle| (FP32 forward replay and atomics vs FP64);
+  * vs central FD of the GPU FP32 forward along structured directions (the
+    per-coordinate FD of a COM loss is below FP32 resolution, so the
+    directions sum many coordinates): relative error <= 1e-3 for v0 and E.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(rng, N, n, spread=0.03, lo=0.35, hi=0.6):
+    dx = 1.0 / n
+    V0 = np.full(N, (dx / 2) ** 3, np.float32)
+    return dict(x=rng.uniform(lo, hi, (N, 3)).astype(np.float32), v=rng.normal(0, 0.3, (N, 3)).astype(np.float32),
+                C=rng.normal(0, 0.5, (N, 9)).astype(np.float32),
+                F=(np.tile(np.eye(3).ravel(), (N, 1)) + rng.normal(0, spread, (N, 9))).astype(np.float32),
+                m=(1000 * V0).astype(np.float32), V0=V0, mat=(np.arange(N) % 3).astype(np.int32))
+
+
+@pytest.mark.parametrize("bc,k", [(1, 2), (2, 3), (3, 1), (1, 6)])
+def test_adjoint_matches_fp64_oracle(gpu, oracle, bc, k):
+    rng = np.random.default_rng(40 + bc + k)
+    N, n, steps, dt = 1500, 16, 6, 1e-3
+    st = _case(rng, N, n)
+    mats_o = [(oracle.FIXED_COROTATED, 1e4, 0.3), (oracle.NEO_HOOKEAN, 3e4, 0.25), (oracle.EOS_FLUID, 1e4, 0.0)]
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3), gpu.createElasticMaterial(1000, 3e4, 0.25, 1),
+            gpu.createFluidMaterial(1000, 1e4)]
+    scene = gpu.Scene((n, n, n), 1.0 / n, dt, (0, -9.8, 0), (0, 0, 0), 0, bc, 3)
+    sim = gpu.Simulator([scene], [N], mats)
+    sim.upload(st["x"], st["v"], st["C"], st["F"], st["m"], st["V0"], st["mat"])
+    sim.forward_checkpointed(steps, k)
+    out = sim.download()
+    tgt = np.array([0.5, 0.3, 0.5])
+    go = {"x": np.tile(2 * (out["x"].mean(0) - tgt) / N, (N, 1)).astype(np.float32),
+          "v": (0.2 * out["v"]).astype(np.float32), "F": (0.02 * out["F"].reshape(N, 9)).astype(np.float32),
+          "C": (0.01 * out["C"].reshape(N, 9)).astype(np.float32)}
+    g = sim.backward(go)
+    osc = oracle.make_scene((n, n, n), 1.0 / n, dt, physics=oracle.MLS, boundary=bc, bthick=3)
+    ost = {k_: st[k_].astype(np.float64) for k_ in ("x", "v", "C", "F", "m", "V0")}
+    ost["mat"] = st["mat"]
+    ref = oracle.adjoint(osc, oracle.make_materials(mats_o), ost, steps, {k_: v.astype(np.float64) for k_, v in go.items()})
+    for key in ("x", "v", "C", "F", "E"):
+        a = np.asarray(g[key]).reshape(-1)
+        b = np.asarray(ref[key]).reshape(-1)
+        err = np.abs(a - b).max() / np.abs(b).max()
+        print(f"bc{bc} k{k} d/d{key}: rel err {err:.2e} (max |ref| {np.abs(b).max():.3e})")
+        assert err <= 2e-3, (key, err)
+
+
+def test_checkpoint_interval_does_not_change_gradients(gpu):
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=8192, n=32, v_sigma=0.2, seed=21)
+    N = counts[0]
+    res = []
+    for k in (1, 4, 16):
+        sim = gpu.Simulator(scenes, counts, mats)
+        sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"])
+        sim.forward_checkpointed(16, k)
+        out = sim.download()
+        g = sim.backward({"x": np.tile(2 * (out["x"].mean(0) - np.array([0.5, 0.3, 0.5])) / N, (N, 1)).astype(np.float32)})
+        res.append(g)
+    for g in res[1:]:
+        for key in ("x", "v", "F", "E"):
+            a, b = np.asarray(g[key]).ravel(), np.asarray(res[0][key]).ravel()
+            assert np.abs(a - b).max() <= 1e-3 * np.abs(b).max() + 1e-12, key
+
+
+def _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k, E=None, v0=None, want_grad=True, loss_kind="com",
+                        F0=None):
+    """loss "com": ||COM(x_T) - (0.5, 0.3, 0.5)||^2 (the differentiable
+    configuration's loss); "spread": mean ||x_T - (0.5, 0.3, 0.5)||^2."""
+    import torch
+
+    from physgrad_b200.autograd import simulate
+
+    N = int(sum(counts))
+    sim = gpu.Simulator(scenes, counts, mats)
+    dev = torch.device("cuda")
+    x0 = torch.tensor(st["x"], device=dev)
+    v0t = torch.tensor(st["v"] if v0 is None else v0, device=dev, requires_grad=want_grad)
+    Et = torch.tensor([m.youngs_modulus for m in mats] if E is None else E, dtype=torch.float32, device=dev,
+                      requires_grad=want_grad)
+    m = torch.tensor(st["m"], device=dev)
+    V0 = torch.tensor(st["V0"], device=dev)
+    mat = torch.tensor(st["mat"], device=dev) if st.get("mat") is not None else None
+    F0t = None if F0 is None else torch.tensor(F0, device=dev)
+    x, v, C, F = simulate(sim, x0, v0t, Et, m, V0, steps, k, mat=mat, F0=F0t)
+    tgt = torch.tensor([0.5, 0.3, 0.5], device=dev, dtype=torch.float64)
+    if loss_kind == "com":
+        loss = ((x.double().mean(0) - tgt) ** 2).sum()
+    else:
+        loss = ((x.double() - tgt) ** 2).sum(1).mean()
+    if not want_grad:
+        return float(loss)
+    loss.backward()
+    return float(loss.detach()), v0t.grad.cpu().numpy(), Et.grad.cpu().numpy()
+
+
+def test_autograd_function_vs_central_differences(gpu):
+    """Config-3 shapes at reduced size: COM loss, gradients w.r.t. v0 and E."""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=32768, n=64, v_sigma=0.1, seed=3)
+    steps, k = 64, 16
+    L, gv0, gE = _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k)
+    # direction 1: uniform shift of v0 in y (sum of all dL/dv0_y)
+    for d_dir in ("y", "rand"):
+        rng = np.random.default_rng(5)
+        d = np.zeros_like(st["v"])
+        if d_dir == "y":
+            d[:, 1] = 1.0
+        else:
+            d = rng.choice([-1.0, 1.0], size=st["v"].shape).astype(np.float32) * (rng.random(st["v"].shape) < 0.5)
+            d += np.array([0.3, 0.6, -0.2], np.float32)
+        eps = 1e-3
+        Lp = _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k, v0=st["v"] + eps * d, want_grad=False)
+        Lm = _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k, v0=st["v"] - eps * d, want_grad=False)
+        fd = (Lp - Lm) / (2 * eps)
+        ad = float((gv0 * d).sum())
+        print(f"v0 direction {d_dir}: FD {fd:.6e} adjoint {ad:.6e} rel {abs(fd - ad) / abs(fd):.2e}")
+        assert abs(fd - ad) <= 1e-3 * abs(fd), (fd, ad)
+    # The COM loss does not depend on E: the transfers conserve momentum, so
+    # internal stress cannot move the centre of mass (no wall contact here).
+    assert abs(gE[0]) <= 1e-12
+    # dL/dE on a loss that does depend on it: a pre-stretched cube, spread loss
+    N = counts[0]
+    F0 = np.tile(np.diag([1.04, 0.97, 1.0]).astype(np.float32), (N, 1, 1))
+    kw = dict(loss_kind="spread", F0=F0)
+    _, _, gE2 = _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k, **kw)
+    E0 = mats[0].youngs_modulus
+    hE = 1e-2 * E0
+    Lp = _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k, E=[E0 + hE], want_grad=False, **kw)
+    Lm = _com_loss_and_grads(gpu, scenes, counts, mats, st, steps, k, E=[E0 - hE], want_grad=False, **kw)
+    fd = (Lp - Lm) / (2 * hE)
+    print(f"E (spread loss, stretched cube): FD {fd:.6e} adjoint {gE2[0]:.6e} rel {abs(fd - gE2[0]) / abs(fd):.2e}")
+    assert abs(fd - gE2[0]) <= 1e-2 * abs(fd), (fd, gE2[0])
+
+
+def test_batched_adjoint_equals_single_scenes(gpu):
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.batched_scenes(n_scenes=3, lo=2000, hi=8000, seed=8, v_sigma=0.2)
+    N = int(sum(counts))
+    sim = gpu.Simulator(scenes, counts, mats)
+    sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st["mat"])
+    sim.forward_checkpointed(8, 4)
+    out = sim.download()
+    go = {"x": (out["x"] - 0.5).astype(np.float32) / N}
+    gb = sim.backward(go)
+    off = 0
+    for s, c in enumerate(counts):
+        sl = slice(off, off + c)
+        one = gpu.Simulator([scenes[s]], [c], [mats[s]])
+        one.upload(st["x"][sl], st["v"][sl], None, None, st["m"][sl], st["V0"][sl])
+        one.forward_checkpointed(8, 4)
+        g1 = one.backward({"x": go["x"][sl]})
+        assert np.abs(gb["v"][sl] - g1["v"]).max() <= 1e-3 * np.abs(g1["v"]).max()
+        assert abs(gb["E"][s] - g1["E"][0]) <= 1e-3 * abs(g1["E"][0]) + 1e-12
+        off += c

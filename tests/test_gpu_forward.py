@@ -352,6 +352,35 @@ def test_invalid_material_rejected(gpu):
     assert ei.value.code == C.PGMPM_ERR_UNSUPPORTED
 
 
+def test_launch_mpm_timestep_forward_matches_ref_compat_solver(gpu, oracle):
+    """The extern-C launcher with the reference's signature
+    (src/pytorch_autograd.cu:371-382) advances device arrays in place by one
+    REF_COMPAT step; compare with the float oracle of the reference path."""
+    import ctypes
+
+    import torch
+
+    rng = np.random.default_rng(31)
+    N, res, dt = 5000, 32, 1e-3
+    x = rng.uniform(0.3, 0.7, (N, 3)).astype(np.float32)
+    v = rng.normal(0, 0.2, (N, 3)).astype(np.float32)
+    m = np.full(N, 1e-3, np.float32)
+    xt, vt, mt = (torch.tensor(a, device="cuda") for a in (x, v, m))
+    g = torch.tensor([0.0, -9.8, 0.0], device="cuda")
+    L = gpu.lib()
+    for _ in range(3):
+        L.launch_mpm_timestep_forward(ctypes.c_void_p(xt.data_ptr()), ctypes.c_void_p(vt.data_ptr()),
+                                      ctypes.c_void_p(mt.data_ptr()), N, res, dt, ctypes.c_void_p(g.data_ptr()), None)
+    torch.cuda.synchronize()
+    sc = oracle.make_scene((res,) * 3, np.float32(1 / res), np.float32(dt), gravity=(0, np.float32(-9.8), 0),
+                           physics=oracle.REF_COMPAT, boundary=oracle.BC_NONE)
+    ref = oracle.run(sc, oracle.make_materials([(0, 1e6, 0.3)]),
+                     dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)),
+                          F=np.tile(np.eye(3).ravel(), (N, 1)), m=m.astype(np.float64), V0=np.zeros(N)), 3, prec=32)
+    assert np.abs(xt.cpu().numpy() - ref["x"]).max() <= 1e-6
+    assert np.abs(vt.cpu().numpy() - ref["v"]).max() <= 1e-4 * np.abs(ref["v"]).max()
+
+
 def test_reference_shaped_solver_api(gpu):
     cfg = gpu.MPMSolverConfig(grid_dimensions=(32, 32, 32), grid_spacing=(1 / 32,) * 3, time_step=1e-4,
                               gravity=(0, -9.8, 0), max_particles=1000)
