@@ -283,8 +283,11 @@ template <class T> struct State {
 
 // Stencil origin of one coordinate in float (matches the CUDA key kernel and
 // the float REF_COMPAT oracle).
+// MLS: u = (x - o) * inv_dx with inv_dx = 1/dx rounded to float;
+// REF_COMPAT: u = (x - o) / dx as src/material_point_method.h:522-529.
 inline int stencil_origin_f(float xa, float oa, float dx, int n, int physics) {
-    float u = (xa - oa) / dx;
+    const float inv_dx = 1.0f / dx;
+    float u = physics == ORACLE_MLS ? (xa - oa) * inv_dx : (xa - oa) / dx;
     float s;
     if (physics == ORACLE_MLS)
         s = std::floor(u - 0.5f);
@@ -412,8 +415,9 @@ template <class T> struct Stencil {
 };
 
 template <class T> inline void mls_stencil(const oracle_scene& sc, const Grid& g, const T* x, Stencil<T>& s) {
+    const T inv_dx = T(1) / T(sc.dx);
     for (int a = 0; a < 3; ++a) {
-        T u = (x[a] - T(sc.origin[a])) / T(sc.dx);
+        T u = (x[a] - T(sc.origin[a])) * inv_dx;
         T b = std::floor(u - T(0.5));
         if (!(b == b)) b = 0;
         if (b < 0) b = 0;

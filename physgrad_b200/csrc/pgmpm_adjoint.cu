@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
         for (int a = 0; a < 3; ++a) {
             mls_dweights(st.f[a], dw[a]);
             // a clamped (escaped) coordinate has zero weight derivative
-            const float raw = __fsub_rn(__fdiv_rn(__fsub_rn(x[a], sc.origin[a]), sc.dx), (float)st.s[a]);
+            const float raw = __fsub_rn(__fmul_rn(__fsub_rn(x[a], sc.origin[a]), sc.inv_dx), (float)st.s[a]);
             if (raw < 0.5f || raw > 1.5f) dw[a][0] = dw[a][1] = dw[a][2] = 0.f;
         }
         // adjoint through the fluid reset and the F update

@@ -223,9 +223,10 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
         sd.p_end = (int)std::min<int64_t>(N, 0x7FFFFFFF);
         sd.dx = d.dx;
         sd.D = 4.f / (d.dx * d.dx);
+        sd.inv_dx = 1.0f / d.dx;
         sd.dt = d.dt;
         s->scenes.push_back(sd);
-        if (ct_base * 64 > 0xFFFFFFFFll || nt_base * 64 > (1ll << 40)) {
+        if (ct_base * 64 > 0xFFFFFFFFll || nt_base * 64 >= 0x7FFFFFFFll) {
             delete s;
             return fail(PGMPM_ERR_ARG, "grids too large for 32-bit cell keys");
         }
@@ -493,11 +494,16 @@ int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p
 int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant, int32_t p2g_tiles_per_sm,
                               int32_t g2p_tiles_per_sm) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
-    if (p2g_variant > 1 || g2p_variant > 1 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
-        return fail(PGMPM_ERR_ARG, "variants are 0 or 1; tiles per SM at most 16");
+    if (p2g_variant > 2 || g2p_variant > 2 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
+        return fail(PGMPM_ERR_ARG, "p2g_variant and g2p_variant 0..2; blocks per SM at most 16");
     if (p2g_variant >= 0) s->tune.p2g_variant = p2g_variant;
     if (g2p_variant >= 0) s->tune.g2p_variant = g2p_variant;
-    if (p2g_tiles_per_sm > 0) s->tune.tile_blocks_per_sm = p2g_tiles_per_sm;
+    if (p2g_tiles_per_sm > 0) {
+        if (s->tune.p2g_variant == 2)
+            s->tune.cell_blocks_per_sm = p2g_tiles_per_sm;
+        else
+            s->tune.tile_blocks_per_sm = p2g_tiles_per_sm;
+    }
     if (g2p_tiles_per_sm > 0) s->tune.g2p_tiles_per_sm = g2p_tiles_per_sm;
     s->drop_graph();
     return PGMPM_OK;
@@ -517,7 +523,7 @@ int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out) {
     s->met.graph_enabled = s->use_graph ? 1 : 0;
     s->met.p2g_variant = s->tune.p2g_variant;
     s->met.g2p_variant = s->tune.g2p_variant;
-    s->met.p2g_tiles_per_sm = s->tune.tile_blocks_per_sm;
+    s->met.p2g_tiles_per_sm = s->tune.p2g_variant == 2 ? s->tune.cell_blocks_per_sm : s->tune.tile_blocks_per_sm;
     s->met.g2p_tiles_per_sm = s->tune.g2p_tiles_per_sm;
     *out = s->met;
     return PGMPM_OK;
@@ -545,10 +551,10 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
     struct Cand {
         int variant, block, ppt, tiles_per_sm;
     };
-    const Cand p2g_c[] = {{0, 192, 0, 2}, {0, 192, 0, 3}, {0, 192, 0, 4}, {0, 192, 0, 6},
-                          {1, 256, 512, 0}, {1, 256, 1024, 0}, {1, 512, 2048, 0}};
-    const Cand g2p_c[] = {{0, 256, 0, 1}, {0, 256, 0, 2}, {0, 256, 0, 3},
-                          {1, 128, 0, 0}, {1, 256, 0, 0}, {1, 512, 0, 0}};
+    const Cand p2g_c[] = {{2, 64, 0, 4}, {2, 64, 0, 6}, {2, 64, 0, 8}, {0, 192, 0, 2}, {0, 192, 0, 3},
+                          {1, 256, 512, 0}, {1, 256, 1024, 0}};
+    const Cand g2p_c[] = {{2, 128, 0, 0}, {2, 256, 0, 0}, {2, 512, 0, 0}, {0, 256, 0, 2},
+                          {1, 128, 0, 0}, {1, 256, 0, 0}};
     Tuning best = keep;
     float best_p2g = 1e30f, best_g2p = 1e30f;
     View V = s->view();
@@ -571,6 +577,8 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
         t.p2g_variant = c.variant;
         if (c.variant == 0) {
             t.tile_blocks_per_sm = c.tiles_per_sm;
+        } else if (c.variant == 2) {
+            t.cell_blocks_per_sm = c.tiles_per_sm;
         } else {
             t.p2g_block = c.block;
             t.ppt = c.ppt;
@@ -582,6 +590,7 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
             best_p2g = ms;
             best.p2g_variant = t.p2g_variant;
             best.tile_blocks_per_sm = t.tile_blocks_per_sm;
+            best.cell_blocks_per_sm = t.cell_blocks_per_sm;
             best.p2g_block = t.p2g_block;
             best.ppt = t.ppt;
         }

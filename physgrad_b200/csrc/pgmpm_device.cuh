@@ -38,7 +38,7 @@ struct SceneDev {
     float origin[3];
     float dt;
     float gravity[3];
-    int pad;
+    float inv_dx;   // 1/dx rounded to float (MLS stencil coordinate)
 };
 
 struct MatDev {
@@ -107,12 +107,13 @@ __device__ __forceinline__ void pack_vC(const float v[3], const float C[9], floa
 }
 
 // --------------------------------------------------------------- stencils
-// Stencil origin of one coordinate.  u = (x - o) / dx is formed with a
-// correctly rounded division and subtraction (no contraction), so the cell
-// keys are bit-identical to the CPU definition.
-__device__ __forceinline__ int stencil_origin(float xa, float oa, float dx, int n, int physics, float& u,
-                                              uint32_t& flags) {
-    u = __fdiv_rn(__fsub_rn(xa, oa), dx);
+// Stencil origin of one coordinate.  The grid coordinate u is formed with
+// correctly rounded operations (no contraction) so the cell keys are
+// bit-identical to the CPU definition: MLS u = (x - o) * inv_dx (inv_dx =
+// 1/dx rounded to float); REF_COMPAT u = (x - o) / dx as the reference.
+__device__ __forceinline__ int stencil_origin(float xa, float oa, float dx, float inv_dx, int n, int physics,
+                                              float& u, uint32_t& flags) {
+    u = physics == PHYS_MLS ? __fmul_rn(__fsub_rn(xa, oa), inv_dx) : __fdiv_rn(__fsub_rn(xa, oa), dx);
     float s = physics == PHYS_MLS ? floorf(__fsub_rn(u, 0.5f)) : __fsub_rn(floorf(u), 1.0f);
     if (!(s == s)) {
         flags |= FLAG_NONFINITE;
@@ -160,7 +161,7 @@ __device__ __forceinline__ void make_stencil(const SceneDev& sc, const float x[3
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         float u;
-        st.s[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+        st.s[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS, u, flags);
         if (PHYS == PHYS_MLS) {
             // f is clamped to the stencil's support so that a particle that
             // left the grid (flagged ESCAPE) transfers as if at the wall

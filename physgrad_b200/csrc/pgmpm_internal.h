@@ -47,18 +47,21 @@ struct View {
     int total_ct, total_nt;
 };
 
-// P2G variants: 0 = per-cell register accumulation over occupied cell tiles
-// (default), 1 = per-particle shared-memory atomics over fixed chunks.
+// P2G variants: 0 = (cell, z-slice) register accumulation with a staged
+// payload, 1 = per-particle shared-memory atomics over fixed chunks,
+// 2 = one thread per cell, 108 register accumulators, no staging (default).
+// G2P variant 2 = direct gather in physical particle order (default).
 // G2P variants: 0 = node tile staged in shared memory, 1 = direct gather.
 struct Tuning {
     int p2g_block = 192;   // variant 0 uses exactly 192 threads (64 cells x 3 z-slices)
     int ppt = 1024;        // variant 1: particles per chunk; variant 0: sub-chunk staged at once is fixed
     int g2p_block = 256;
     int grid_block = 256;
-    int p2g_variant = 0;
-    int g2p_variant = 1;
+    int p2g_variant = 2;
+    int g2p_variant = 2;
     int tile_blocks_per_sm = 3;  // persistent P2G tile kernel: blocks per SM
     int g2p_tiles_per_sm = 2;    // persistent G2P tile kernel: blocks per SM (256 threads)
+    int cell_blocks_per_sm = 6;  // persistent P2G thread-per-cell kernel (variant 2): blocks per SM
 };
 
 // pgmpm_sort.cu

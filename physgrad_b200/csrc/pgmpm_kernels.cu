@@ -41,7 +41,7 @@ __global__ void k_keys(View V) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             float u;
-            so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+            so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS, u, flags);
         }
         V.keys[p] = cell_key(sc, so);
     }
@@ -53,21 +53,20 @@ __global__ void k_mark(View V) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < V.N; i += stride) {
         const uint32_t ct = V.skeys[i] >> 6;
-        if (i > 0 && (V.skeys[i - 1] >> 6) == ct) continue;
+        const bool first = i == 0 || (V.skeys[i - 1] >> 6) != ct;
+        const bool last = i + 1 == V.N || (V.skeys[i + 1] >> 6) != ct;
+        if (!first && !last) continue;
         if (ct >= (uint32_t)V.total_ct) {
             atomicOr(&V.counters[CNT_FLAGS], FLAG_TILE_RANGE);
             continue;
         }
-        // this thread found the first particle of cell tile ct: record the
-        // tile's sorted range and list it as occupied
+        // first / last particle of cell tile ct: record the tile's sorted
+        // range; the first one also lists the tile and marks its node tiles
+        uint32_t* rng = reinterpret_cast<uint32_t*>(&V.ctile_range[ct]);
+        if (last) rng[1] = (uint32_t)(i + 1);
+        if (!first) continue;
+        rng[0] = (uint32_t)i;
         {
-            int64_t lo = i + 1, hi = V.N;
-            const uint32_t target = (ct + 1u) << 6;
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (V.skeys[mid] < target) lo = mid + 1; else hi = mid;
-            }
-            V.ctile_range[ct] = make_uint2((uint32_t)i, (uint32_t)lo);
             const uint32_t slot = atomicAdd(&V.counters[CNT_CTILES], 1u);
             V.ctile_list[slot] = ct;
         }
@@ -506,6 +505,213 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V, AdjView AV) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// ------------------------------------------------ P2G, one thread per cell
+// Variant 2: one 64-thread block per occupied cell tile, thread c owns cell
+// c and all 27 nodes of its stencil (108 register accumulators).  The
+// thread walks its cell's particles (sorted, contiguous), computes each
+// particle's stress / affine payload itself and accumulates: no shared
+// payload staging and no barriers until the flush.  The flush is the same
+// shared-memory transpose + one vector atomic per tile node.
+constexpr int P2GC_T = 64;
+
+template <int MODE, bool MULTI, bool FLUID>
+__global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
+    constexpr int PHYS = MODE == MODE_REF ? PHYS_REF : PHYS_MLS;
+    __shared__ float T[27 * 4 * 64];
+    __shared__ uint32_t s_work;
+    const int c = threadIdx.x;
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    for (;;) {
+        if (c == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= ntiles) break;
+        const uint32_t ct = V.ctile_list[w];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        // this cell's sorted range: keys in the tile are ordered by local cell
+        const uint32_t kc = (ct << 6) | (uint32_t)c;
+        uint32_t lo = rg.x, hi = rg.y;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (V.skeys[mid] < kc) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t cb = lo;
+        hi = rg.y;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (V.skeys[mid] <= kc) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t ce = lo;
+        float acc[27][4];
+#pragma unroll
+        for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = acc[o][3] = 0.f;
+        for (uint32_t i = cb; i < ce; ++i) {
+            const uint32_t p = V.order[i];
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            const float4 q0 = V.q[p];
+            const float x[3] = {q0.x, q0.y, q0.z};
+            Stencil st;
+            make_stencil<PHYS>(sc, x, st, flags);
+            float m, b[3], Ad[9];
+            if (MODE == MODE_ADJ) {
+                const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+                float xx[3], F[9];
+                unpack_xF(q0, q1, q2, xx, F);
+                float gx[3], gF[9], gv[3], gC[9];
+                unpack_xF(AV.g[p], AV.g[N + p], AV.g[2 * N + p], gx, gF);
+                unpack_vC(AV.g[3 * N + p], AV.g[4 * N + p], AV.g[5 * N + p], gv, gC);
+                if (FLUID && V.mats[MULTI ? V.mat[p] : 0].model == MODEL_EOS) {
+                    float Cn[9], vdum[3], M[9], Fr[9], cof[9];
+                    unpack_vC(AV.q_next[3 * N + p], AV.q_next[4 * N + p], AV.q_next[5 * N + p], vdum, Cn);
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) M[a] = sc.dt * Cn[a] + ((a % 4 == 0) ? 1.f : 0.f);
+                    m3_mul(M, F, Fr);
+                    m3_cof(Fr, cof);
+                    const float J = Fr[0] * cof[0] + Fr[1] * cof[1] + Fr[2] * cof[2];
+                    const float cc = cbrtf(J) / (3.f * J) * (gF[0] + gF[4] + gF[8]);
+#pragma unroll
+                    for (int a = 0; a < 9; ++a) gF[a] = cc * cof[a];
+                }
+                float gFFt[9];
+                m3_mulT(gF, F, gFFt);
+                const float sD = sc.D * sc.dx;
+#pragma unroll
+                for (int a = 0; a < 9; ++a) Ad[a] = sD * (gC[a] + sc.dt * gFFt[a]);
+                m = 0.f;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    b[a] = (gv[a] + sc.dt * gx[a]) - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
+            } else if (PHYS == PHYS_MLS) {
+                const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+                const float4 q3 = V.q[3 * N + p], q4 = V.q[4 * N + p], q5 = V.q[5 * N + p];
+                const float2 mv = V.mV[p];
+                float xx[3], F[9], v[3], C[9];
+                unpack_xF(q0, q1, q2, xx, F);
+                unpack_vC(q3, q4, q5, v, C);
+                const MatDev mt = V.mats[MULTI ? V.mat[p] : 0];
+                float tau[9];
+                kirchhoff(F, mt, tau);
+                const float kk = -sc.dt * mv.y * sc.D;
+#pragma unroll
+                for (int a = 0; a < 9; ++a) Ad[a] = (kk * tau[a] + mv.x * C[a]) * sc.dx;
+                m = mv.x;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    b[a] = m * v[a] - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
+            } else {
+                const float4 q3 = V.q[3 * N + p];
+                const float2 mv = V.mV[p];
+                const bool regular = st.b[0] == st.s[0] && st.b[1] == st.s[1] && st.b[2] == st.s[2];
+                if (!regular) {
+                    // stencil partly outside the grid: scatter directly with
+                    // the reference's per-node bounds checks
+                    const float vel[3] = {q3.x, q3.y, q3.z};
+                    for (int ii = 0; ii < 3; ++ii) {
+                        const int gi = st.b[0] + ii;
+                        if (gi < 0 || gi >= sc.n[0]) continue;
+                        for (int jj = 0; jj < 3; ++jj) {
+                            const int gj = st.b[1] + jj;
+                            if (gj < 0 || gj >= sc.n[1]) continue;
+                            for (int kq = 0; kq < 3; ++kq) {
+                                const int gk = st.b[2] + kq;
+                                if (gk < 0 || gk >= sc.n[2]) continue;
+                                const float wgt = __fmul_rn(__fmul_rn(st.w[0][ii], st.w[1][jj]), st.w[2][kq]);
+                                if (!(wgt > 1e-10f)) continue;
+                                const float wm = __fmul_rn(wgt, mv.x);
+                                float* g = reinterpret_cast<float*>(&V.grid_mp[node_index(sc, gi, gj, gk)]);
+                                atomicAdd(g, wm);
+                                atomicAdd(g + 1, __fmul_rn(wm, vel[0]));
+                                atomicAdd(g + 2, __fmul_rn(wm, vel[1]));
+                                atomicAdd(g + 3, __fmul_rn(wm, vel[2]));
+                            }
+                        }
+                    }
+                    continue;
+                }
+#pragma unroll
+                for (int zz = 0; zz < 3; ++zz)
+#pragma unroll
+                    for (int yy = 0; yy < 3; ++yy)
+#pragma unroll
+                        for (int xx = 0; xx < 3; ++xx) {
+                            const float wgt = __fmul_rn(__fmul_rn(st.w[0][xx], st.w[1][yy]), st.w[2][zz]);
+                            if (wgt > 1e-10f) {
+                                const int o = xx + 3 * yy + 9 * zz;
+                                const float wm = __fmul_rn(wgt, mv.x);
+                                acc[o][0] += wm;
+                                acc[o][1] += __fmul_rn(wm, q3.x);
+                                acc[o][2] += __fmul_rn(wm, q3.y);
+                                acc[o][3] += __fmul_rn(wm, q3.z);
+                            }
+                        }
+                continue;
+            }
+            // MLS / adjoint: node o gets w_o (m, b + Ad o)
+#pragma unroll
+            for (int zz = 0; zz < 3; ++zz) {
+                const float bz0 = b[0] + Ad[2] * (float)zz, bz1 = b[1] + Ad[5] * (float)zz,
+                            bz2 = b[2] + Ad[8] * (float)zz;
+#pragma unroll
+                for (int yy = 0; yy < 3; ++yy) {
+                    const float wyz = st.w[1][yy] * st.w[2][zz];
+                    float v0 = bz0 + Ad[1] * (float)yy, v1 = bz1 + Ad[4] * (float)yy, v2 = bz2 + Ad[7] * (float)yy;
+#pragma unroll
+                    for (int xx = 0; xx < 3; ++xx) {
+                        const int o = xx + 3 * yy + 9 * zz;
+                        const float wgt = st.w[0][xx] * wyz;
+                        if (MODE != MODE_ADJ) acc[o][0] += wgt * m;
+                        acc[o][1] += wgt * v0;
+                        acc[o][2] += wgt * v1;
+                        acc[o][3] += wgt * v2;
+                        v0 += Ad[0];
+                        v1 += Ad[3];
+                        v2 += Ad[6];
+                    }
+                }
+            }
+        }
+        // flush: transpose through shared memory, one vector atomic per node
+#pragma unroll
+        for (int o = 0; o < 27; ++o) {
+            T[(o * 4 + 0) * 64 + c] = acc[o][0];
+            T[(o * 4 + 1) * 64 + c] = acc[o][1];
+            T[(o * 4 + 2) * 64 + c] = acc[o][2];
+            T[(o * 4 + 3) * 64 + c] = acc[o][3];
+        }
+        __syncthreads();
+        for (int n = c; n < TILE_NODES; n += P2GC_T) {
+            const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int zz = max(0, nz - 3); zz <= min(2, nz); ++zz)
+                for (int yy = max(0, ny - 3); yy <= min(2, ny); ++yy)
+                    for (int xx = max(0, nx - 3); xx <= min(2, nx); ++xx) {
+                        const int cc = (nx - xx) + 4 * (ny - yy) + 16 * (nz - zz);
+                        const int o = xx + 3 * yy + 9 * zz;
+                        a4.x += T[(o * 4 + 0) * 64 + cc];
+                        a4.y += T[(o * 4 + 1) * 64 + cc];
+                        a4.z += T[(o * 4 + 2) * 64 + cc];
+                        a4.w += T[(o * 4 + 3) * 64 + cc];
+                    }
+            const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
+            const bool any = MODE == MODE_ADJ ? (a4.y != 0.f || a4.z != 0.f || a4.w != 0.f) : a4.x != 0.f;
+            if (any && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+        }
+        __syncthreads();
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
 // ------------------------------------------------------------ grid update
 template <int PHYS>
 __global__ void k_grid(View V) {
@@ -568,35 +774,53 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
         const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
         float xx[3], F[9];
         unpack_xF(q0, q1, q2, xx, F);
-        const float dx = sc.dx;
+        // separable tiled node index: idx = X[i] + Y[j] + Z[k]
+        int X[3], Y[3], Z[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int gi = st.s[0] + a, gj = st.s[1] + a, gk = st.s[2] + a;
+            X[a] = ((gi >> 2) << 6) + (gi & 3);
+            Y[a] = (gj >> 2) * (sc.nt[0] << 6) + ((gj & 3) << 2);
+            Z[a] = (gk >> 2) * ((sc.nt[0] * sc.nt[1]) << 6) + ((gk & 3) << 4) + (sc.nt_base << 6);
+        }
+        // S = sum w v o^T (o = integer stencil offset), nv = sum w v;
+        // B = sum w v d^T = dx (S - nv f^T)
         float nv[3] = {0.f, 0.f, 0.f};
-        float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float S[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float dk = ((float)k - st.f[2]) * dx;
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                const float dj = ((float)j - st.f[1]) * dx;
                 const float wjk = st.w[1][j] * st.w[2][k];
-#pragma unroll
-                for (int ii = 0; ii < 3; ++ii) {
-                    const float di = ((float)ii - st.f[0]) * dx;
-                    const float4 g = fetch(st.s[0] + ii, st.s[1] + j, st.s[2] + k);
-                    const float w = st.w[0][ii] * wjk;
-                    const float wx = w * g.x, wy = w * g.y, wz = w * g.z;
-                    nv[0] += wx; nv[1] += wy; nv[2] += wz;
-                    B[0] += wx * di; B[1] += wx * dj; B[2] += wx * dk;
-                    B[3] += wy * di; B[4] += wy * dj; B[5] += wy * dk;
-                    B[6] += wz * di; B[7] += wz * dj; B[8] += wz * dk;
+                const int row = Y[j] + Z[k];
+                const float4 g0 = fetch(st.s[0], st.s[1] + j, st.s[2] + k, row + X[0]);
+                const float4 g1 = fetch(st.s[0] + 1, st.s[1] + j, st.s[2] + k, row + X[1]);
+                const float4 g2 = fetch(st.s[0] + 2, st.s[1] + j, st.s[2] + k, row + X[2]);
+                const float w0 = st.w[0][0] * wjk, w1 = st.w[0][1] * wjk, w2 = st.w[0][2] * wjk;
+                const float r1x = w1 * g1.x, r1y = w1 * g1.y, r1z = w1 * g1.z;
+                const float r2x = w2 * g2.x, r2y = w2 * g2.y, r2z = w2 * g2.z;
+                const float sx = w0 * g0.x + r1x + r2x, sy = w0 * g0.y + r1y + r2y, sz = w0 * g0.z + r1z + r2z;
+                nv[0] += sx; nv[1] += sy; nv[2] += sz;
+                S[0] += r1x + 2.f * r2x; S[3] += r1y + 2.f * r2y; S[6] += r1z + 2.f * r2z;
+                if (j) {
+                    const float fj = (float)j;
+                    S[1] += fj * sx; S[4] += fj * sy; S[7] += fj * sz;
+                }
+                if (k) {
+                    const float fk = (float)k;
+                    S[2] += fk * sx; S[5] += fk * sy; S[8] += fk * sz;
                 }
             }
         }
+        const float dx = sc.dx;
         float C[9], Fn[9], M[9];
 #pragma unroll
-        for (int a = 0; a < 9; ++a) {
-            C[a] = sc.D * B[a];
-            M[a] = sc.dt * C[a] + ((a % 4 == 0) ? 1.f : 0.f);
-        }
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                C[3 * a + b] = sc.D * dx * (S[3 * a + b] - nv[a] * st.f[b]);
+                M[3 * a + b] = sc.dt * C[3 * a + b] + (a == b ? 1.f : 0.f);
+            }
         m3_mul(M, F, Fn);
         if (FLUID) {
             const int mid = MULTI ? V.mat[p] : 0;
@@ -635,7 +859,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
                     if (gk < 0 || gk >= sc.n[2]) continue;
                     const float weight = __fmul_rn(__fmul_rn(st.w[0][ii], st.w[1][j]), st.w[2][k]);
                     if (!(weight > 1e-10f)) continue;
-                    const float4 g = fetch(gi, gj, gk);
+                    const float4 g = fetch(gi, gj, gk, (int)node_index(sc, gi, gj, gk));
                     nv[0] = __fadd_rn(nv[0], __fmul_rn(weight, g.x));
                     nv[1] = __fadd_rn(nv[1], __fmul_rn(weight, g.y));
                     nv[2] = __fadd_rn(nv[2], __fmul_rn(weight, g.z));
@@ -653,19 +877,24 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         float u;
-        so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.n[a], PHYS, u, flags);
+        so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS, u, flags);
     }
     V.keys[p] = cell_key(sc, so);
 }
 
-// G2P variant 1: one thread per sorted particle, 27 gathers through L1.
-template <int PHYS, bool MULTI, bool FLUID>
-__global__ void k_g2p(View V) {
+// G2P variants 1 and 2: one thread per particle, 27 gathers through L1.
+// Variant 1 visits particles in the step's sorted order; variant 2 in
+// physical order (p = i): a gather needs no grouping, the physical order was
+// sorted at upload and particles drift less than a cell per step, so
+// neighbouring threads still share grid nodes, and the state loads are fully
+// coalesced with no dependent load of the order array.
+template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER>
+__device__ __forceinline__ void k_g2p_impl(const View& V) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     uint32_t flags = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-        const uint32_t p = V.order[i];
+        const uint32_t p = PHYS_ORDER ? (uint32_t)i : V.order[i];
         if (p >= (uint32_t)N) {
             flags |= FLAG_TILE_RANGE;
             continue;
@@ -673,10 +902,19 @@ __global__ void k_g2p(View V) {
         const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
         const SceneDev& sc = scene_ref(V, s);
         const float4* gv = V.grid_v;
-        auto fetch = [&](int gi, int gj, int gk) { return __ldg(&gv[node_index(sc, gi, gj, gk)]); };
+        auto fetch = [&](int, int, int, int idx) { return __ldg(&gv[idx]); };
         g2p_particle<PHYS, MULTI, FLUID>(V, sc, p, fetch, flags);
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+template <int PHYS, bool MULTI, bool FLUID>
+__global__ void k_g2p(View V) {
+    k_g2p_impl<PHYS, MULTI, FLUID, false>(V);
+}
+template <int PHYS, bool MULTI, bool FLUID>
+__global__ void k_g2p_phys(View V) {
+    k_g2p_impl<PHYS, MULTI, FLUID, true>(V);
 }
 
 // G2P variant 0: one block per occupied cell tile; the tile's 6^3 node
@@ -708,10 +946,10 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(View V) {
         }
         __syncthreads();
         const float4* gv = V.grid_v;
-        auto fetch = [&](int gi, int gj, int gk) {
+        auto fetch = [&](int gi, int gj, int gk, int idx) {
             const unsigned lx = (unsigned)(gi - ox), ly = (unsigned)(gj - oy), lz = (unsigned)(gk - oz);
             if (lx < (unsigned)TN && ly < (unsigned)TN && lz < (unsigned)TN) return gsm[lx + TN * (ly + TN * lz)];
-            return __ldg(&gv[node_index(sc, gi, gj, gk)]);
+            return __ldg(&gv[idx]);
         };
         for (uint32_t i = rg.x + threadIdx.x; i < rg.y; i += blockDim.x) {
             const uint32_t p = V.order[i];
@@ -842,6 +1080,21 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
                                cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
+    if (t.p2g_variant == 2) {
+        const int nb = num_sms * t.cell_blocks_per_sm;
+        if (pf.multi_mat) {
+            if (pf.has_fluid)
+                k_p2g_cells<MODE_ADJ, true, true><<<nb, P2GC_T, 0, st>>>(V, A);
+            else
+                k_p2g_cells<MODE_ADJ, true, false><<<nb, P2GC_T, 0, st>>>(V, A);
+        } else {
+            if (pf.has_fluid)
+                k_p2g_cells<MODE_ADJ, false, true><<<nb, P2GC_T, 0, st>>>(V, A);
+            else
+                k_p2g_cells<MODE_ADJ, false, false><<<nb, P2GC_T, 0, st>>>(V, A);
+        }
+        return cudaGetLastError();
+    }
     const int nb = num_sms * t.tile_blocks_per_sm;
     if (pf.multi_mat) {
         if (pf.has_fluid)
@@ -859,6 +1112,19 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
 
 cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
+    if (t.p2g_variant == 2) {
+        const int nb = num_sms * t.cell_blocks_per_sm;
+        const AdjView none{};
+        if (pf.physics == PHYS_MLS) {
+            if (pf.multi_mat)
+                k_p2g_cells<MODE_MLS, true, false><<<nb, P2GC_T, 0, st>>>(V, none);
+            else
+                k_p2g_cells<MODE_MLS, false, false><<<nb, P2GC_T, 0, st>>>(V, none);
+        } else {
+            k_p2g_cells<MODE_REF, false, false><<<nb, P2GC_T, 0, st>>>(V, none);
+        }
+        return cudaGetLastError();
+    }
     if (t.p2g_variant == 0) {
         const int nb = num_sms * t.tile_blocks_per_sm;
         const AdjView none{};
@@ -923,9 +1189,12 @@ cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int 
     if (t.g2p_variant == 0) {
         const int nb = num_sms * t.g2p_tiles_per_sm;
         PGMPM_G2P_DISPATCH(k_g2p_tiles, nb, 256);
-    } else {
+    } else if (t.g2p_variant == 1) {
         const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
         PGMPM_G2P_DISPATCH(k_g2p, nb, t.g2p_block);
+    } else {
+        const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
+        PGMPM_G2P_DISPATCH(k_g2p_phys, nb, t.g2p_block);
     }
     return cudaGetLastError();
 }

@@ -28,22 +28,45 @@ static_assert(RS_TILE == RADIX_TILE && RS_MAXD == RADIX_MAX_DIGITS, "scratch siz
 
 __global__ void __launch_bounds__(RS_THREADS) rs_hist(const uint32_t* __restrict__ keys, int64_t n, int shift,
                                                       int bits, uint32_t* __restrict__ hist, int nblocks) {
-    __shared__ uint32_t cnt[RS_MAXD];
+    // warp-private histograms with native integer shared atomics, summed at the end
+    __shared__ uint32_t cnt[RS_WARPS][RS_MAXD];
     const int nd = 1 << bits;
     const uint32_t mask = (uint32_t)nd - 1u;
-    for (int d = threadIdx.x; d < nd; d += RS_THREADS) cnt[d] = 0;
+    for (int d = threadIdx.x; d < RS_WARPS * RS_MAXD; d += RS_THREADS) (&cnt[0][0])[d] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t base = (int64_t)blockIdx.x * RS_TILE + warp * (32 * RS_ITEMS);
+    uint32_t k[RS_ITEMS];
 #pragma unroll
     for (int r = 0; r < RS_ITEMS; ++r) {
         const int64_t i = base + r * 32 + lane;
-        const uint32_t d = i < n ? ((__ldg(keys + i) >> shift) & mask) : 0xFFFFFFFFu;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        if (d != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&cnt[d], (uint32_t)__popc(peers));
+        k[r] = i < n ? __ldg(keys + i) : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; ++r) {
+        const int64_t i = base + r * 32 + lane;
+        if (i < n) atomicAdd(&cnt[warp][(k[r] >> shift) & mask], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < nd; d += RS_THREADS) hist[(int64_t)d * nblocks + blockIdx.x] = cnt[d];
+    for (int d = threadIdx.x; d < nd; d += RS_THREADS) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; ++w) s += cnt[w][d];
+        hist[(int64_t)d * nblocks + blockIdx.x] = s;
+    }
+}
+
+// Lanes of the warp holding the same digit as this lane (bits <= 8), built
+// from one ballot per digit bit; only lanes with `ok` participate.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, int bits, bool ok) {
+    uint32_t peers = __ballot_sync(0xFFFFFFFFu, ok);
+    if (!ok) peers = ~peers;
+    for (int b = 0; b < bits; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+        peers &= bit ? bal : ~bal;
+    }
+    return peers;
 }
 
 // Block-wide exclusive scan of one value per thread (blockDim.x <= 1024).
@@ -123,8 +146,8 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
         const bool ok = i < n;
         k[r] = ok ? kin[i] : 0xFFFFFFFFu;
         v[r] = ok ? (vin ? vin[i] : (uint32_t)i) : 0u;
-        const uint32_t d = ok ? ((k[r] >> shift) & mask) : 0xFFFFFFFFu;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t d = ok ? ((k[r] >> shift) & mask) : 0u;
+        const uint32_t peers = digit_peers(d, bits, ok);
         uint32_t c = 0u;
         if (ok) c = wcnt[warp][d];
         rk[r] = c + (uint32_t)__popc(peers & lt);
