@@ -214,8 +214,21 @@ def run_ours(args, rank, world, device):
     import physgrad_b200 as pg
     from physgrad_b200 import _capi as C
 
+    from physgrad_b200.distributed import max_over_ranks, shard_scenes, sum_over_ranks
+
     torch.cuda.set_device(device)
     scenes, counts, mats, st, meta = make_workload(args.workload)
+    scaling = "weak"
+    if world > 1 and len(scenes) > 1:
+        # batched scenes: disjoint shards, no exchange (strong scaling)
+        mine = shard_scenes(counts, world, rank)
+        off = np.concatenate([[0], np.cumsum(counts)])
+        idx = np.concatenate([np.arange(off[s], off[s + 1]) for s in mine])
+        remap = {s: k for k, s in enumerate(mine)}
+        st = {k: (None if a is None else a[idx]) for k, a in st.items()}
+        st["mat"] = np.array([remap[int(m)] for m in st["mat"]], np.int32)
+        scenes, counts, mats = [scenes[s] for s in mine], [counts[s] for s in mine], [mats[s] for s in mine]
+        scaling = "strong"
     N = int(sum(counts))
     sim = pg.Simulator(scenes, counts, mats, device=device)
     Cm = st["C"].reshape(N, 9)
@@ -241,13 +254,11 @@ def run_ours(args, rank, world, device):
         ev1.record(stream)
         torch.cuda.synchronize()
         clk.mark_end()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, device=f"cuda:{device}")
+    n_total = int(sum_over_ranks(N, device=f"cuda:{device}"))
     if world > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     flags = sim.status()
     clocks = clk.summary()
@@ -284,7 +295,7 @@ def run_ours(args, rank, world, device):
         traffic = tj.get(args.workload, {}).get(dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": kernels[dom]["achieved_gbs"], "peak": hbm,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": kernels[dom]["frac"], "traffic": traffic}
-    value = world * N * args.steps / (ms * 1e-3)
+    value = n_total * args.steps / (ms * 1e-3)
     launches_per_step = kernel_launches_per_step(scenes)
 
     # e2e: host-buffer C-ABI call (pinned memory in/out), S steps per call
@@ -306,16 +317,10 @@ def run_ours(args, rank, world, device):
                                      hm.ctypes.data, hV.ctypes.data, hmat.ctypes.data if hmat is not None else None,
                                      S, ox.ctypes.data, ov.ctypes.data, oC.ctypes.data, oF.ctypes.data, sh))
         e2e_times.append(time.perf_counter() - t0)
-    e2e_t = statistics.median(e2e_times[1:])
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e2e_t], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(statistics.median(e2e_times[1:]), device=f"cuda:{device}")
     h2d = sum(a.nbytes for a in (hx, hv, hC, hF, hm, hV)) + (hmat.nbytes if hmat is not None else 0)
     d2h = sum(a.nbytes for a in (ox, ov, oC, oF))
-    e2e = {"value": world * N * S / e2e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / S,
+    e2e = {"value": n_total * S / e2e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / S,
            "d2h_bytes_per_step": d2h / S, "steps_per_call": S,
            "call": "pgmpm_advance_host: state in from pinned host, S steps, state out to pinned host"}
 
@@ -331,12 +336,12 @@ def run_ours(args, rank, world, device):
            "grid": [int(s.n[0]) for s in scenes][:8], "dt": float(scenes[0].dt), "physics": "MLS",
            "materials": meta.get("materials", "fixed-corotated"),
            "l2": f"inputs larger than L2: particle state {N * 104 / 1e6:.0f} MB + grid",
-           "parallelism": "replicas" if world > 1 else "single",
+           "parallelism": ("scene shards" if scaling == "strong" else "replicas") if world > 1 else "single",
            "tuning": {k: sim.metrics()[k] for k in ("p2g_block", "p2g_ppt", "g2p_block", "graph_enabled")},
            "active_nodes": A}
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": scaling, "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded uniform positions of the configuration's shapes)", "config": cfg,
             "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "device_flags": flags}
