@@ -61,10 +61,19 @@ def make_workload(name):
 
 
 def algorithmic_bytes(N, A, multi_mat):
-    """Algorithmic HBM bytes per launch (FP32): P2G 100 B/particle (+4 for a
-    material id) + 16 B/active node; G2P 144 B/particle + 12 B/node; grid
-    update 28 B/node."""
-    return {"p2g": (100 + (4 if multi_mat else 0)) * N + 16 * A, "g2p": 144 * N + 12 * A, "grid": 28 * A}
+    """Compulsory HBM bytes per launch (FP32) of each kernel as split here.
+
+    P2G reads the sorted order (4 B) and the precomputed payload (b, m, the
+    affine matrix, the stencil fraction: 64 B) per particle and adds 16 B
+    per active node.  G2P reads x and F (48 B), (m, V0) (8 B) and the
+    material id (4 B, several materials), writes x, v, C, F (96 B), the next
+    key (4 B) and the next payload (64 B) per particle, and reads 12 B per
+    active node.  The grid update moves 28 B per active node.  "step" is the
+    unfused accounting of the whole MLS step, 244 B per particle (+4 B for a
+    material id) + 56 B per active node, which leaves out the sort."""
+    mm = 4 if multi_mat else 0
+    return {"p2g": 68 * N + 16 * A, "g2p": (220 + mm) * N + 12 * A, "grid": 28 * A,
+            "step": (244 + mm) * N + 56 * A}
 
 
 def kernel_launches_per_step(scenes):
@@ -254,6 +263,7 @@ def run_ours(args, rank, world, device):
         ev1.record(stream)
         torch.cuda.synchronize()
         clk.mark_end()
+    ms = ev0.elapsed_time(ev1)
     ms = max_over_ranks(ms, device=f"cuda:{device}")
     n_total = int(sum_over_ranks(N, device=f"cuda:{device}"))
     if world > 1:
@@ -295,6 +305,10 @@ def run_ours(args, rank, world, device):
         traffic = tj.get(args.workload, {}).get(dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": kernels[dom]["achieved_gbs"], "peak": hbm,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": kernels[dom]["frac"], "traffic": traffic}
+    step_gbs = alg["step"] * n_total / N / (ms / args.steps * 1e-3) / 1e9
+    step_roofline = {"bytes_per_step": alg["step"] * n_total // N, "achieved": round(step_gbs, 1), "peak": hbm,
+                     "unit": "GB/s", "frac": round(step_gbs / hbm, 4),
+                     "note": "whole step incl. the sort, unfused algorithmic bytes 244 B/particle + 56 B/node"}
     value = n_total * args.steps / (ms * 1e-3)
     launches_per_step = kernel_launches_per_step(scenes)
 
@@ -343,7 +357,7 @@ def run_ours(args, rank, world, device):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": scaling, "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded uniform positions of the configuration's shapes)", "config": cfg,
-            "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "device_flags": flags}
     sim.close()
     return line

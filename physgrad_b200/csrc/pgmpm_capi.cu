@@ -70,6 +70,12 @@ int material_to_dev(const pgmpm_material& m, MatDev& d) {
     return PGMPM_OK;
 }
 
+int refresh_payload(pgmpm_solver s, cudaStream_t st) {
+    if (s->N == 0 || s->pf.physics != PHYS_MLS) return PGMPM_OK;
+    CK(launch_payload(s->view(), s->pf, st));
+    return PGMPM_OK;
+}
+
 int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) {
     if (s->N == 0) {  // nothing to move; keep the timing events consistent
         if (timed)
@@ -264,6 +270,7 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->d_scenes, sizeof(SceneDev) * n_scenes);
     AL(s->d_mats, sizeof(MatDev) * n_materials);
     AL(s->q, sizeof(float4) * 6 * (size_t)std::max<int64_t>(N, 1));
+    if (s->pf.physics == PHYS_MLS) AL(s->pay, sizeof(float4) * 4 * (size_t)std::max<int64_t>(N, 1));
     AL(s->mV, sizeof(float2) * (size_t)std::max<int64_t>(N, 1));
     if (s->pf.multi_mat) AL(s->mat, n4);
     AL(s->user_of_phys, n4);
@@ -327,6 +334,13 @@ int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t
     // ordered with prior work on the legacy stream; graphs read the table at run time
     CK(cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice));
     s->mats_h.assign(materials, materials + n_materials);
+    if (s->uploaded) {
+        // the payload holds the stress of the old material table
+        CK(cudaDeviceSynchronize());
+        int rc = refresh_payload(s, s->cap_stream);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(s->cap_stream));
+    }
     return PGMPM_OK;
 }
 
@@ -392,6 +406,8 @@ int pgmpm_upload(pgmpm_solver s, const float* x, const float* v, const float* C,
         CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, ord, s->user_of_phys.as<uint32_t>(), s->mV.as<float2>(),
                        s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr, st));
         CK(cudaMemcpyAsync(s->keys.p, sk, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
+        int rc = refresh_payload(s, st);
+        if (rc) return rc;
     }
     s->uploaded = true;
     return PGMPM_OK;
@@ -614,6 +630,8 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
     CK(cudaMemcpyAsync(s->q.p, save.p, qb, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->keys.p, save.as<char>() + qb, sizeof(uint32_t) * s->N, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemsetAsync(s->grid_mp.p, 0, s->grid_mp.bytes, st));
+    rc = refresh_payload(s, st);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(st));
     s->tune = best;
     s->use_graph = keep_graph;

@@ -352,6 +352,31 @@ __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const MatDe
     }
 }
 
+// --------------------------------------------------------- P2G payload
+// What P2G needs of one MLS particle, computed where the state is already in
+// registers (G2P of the previous step, or k_payload after an upload):
+//   node o of the stencil receives w_o(f) * (m, b + Ad o) with
+//   Ad = dx * A, A = -dt V0 D tau(F) + m C, b = m v - Ad f.
+// Packed as 4 float4 planes: p0 = (b, m), p1 = Ad[0..3], p2 = Ad[4..7],
+// p3 = (Ad[8], f).
+__device__ __forceinline__ void mls_payload(const SceneDev& sc, const MatDev& mt, const float f[3], const float F[9],
+                                            const float v[3], const float C[9], float m, float V0, float4& p0,
+                                            float4& p1, float4& p2, float4& p3) {
+    float tau[9];
+    kirchhoff(F, mt, tau);
+    const float kk = -sc.dt * V0 * sc.D;
+    float Ad[9];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) Ad[a] = (kk * tau[a] + m * C[a]) * sc.dx;
+    float b[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) b[a] = m * v[a] - (Ad[3 * a] * f[0] + Ad[3 * a + 1] * f[1] + Ad[3 * a + 2] * f[2]);
+    p0 = make_float4(b[0], b[1], b[2], m);
+    p1 = make_float4(Ad[0], Ad[1], Ad[2], Ad[3]);
+    p2 = make_float4(Ad[4], Ad[5], Ad[6], Ad[7]);
+    p3 = make_float4(Ad[8], f[0], f[1], f[2]);
+}
+
 // ----------------------------------------------------------- grid update
 __device__ __forceinline__ bool in_wall(const SceneDev& sc, int a, int idx, int& side) {
     if (idx < sc.bthick) { side = -1; return true; }

@@ -32,6 +32,7 @@ int ensure_tape(pgmpm_solver s, int slots) {
     s->tape_slots = 0;
     CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1)));
     CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1)));
+    if (s->pf.physics == PHYS_MLS) CK(s->tape_pay.alloc(sizeof(float4) * 4 * N));
     CK(s->tape_sk.alloc(sizeof(uint32_t) * N * slots));
     CK(s->tape_ord.alloc(sizeof(uint32_t) * N * slots));
     CK(s->tape_gv.alloc(sizeof(float4) * nodes * slots));
@@ -52,6 +53,7 @@ StepBufs tape_bufs(pgmpm_solver s, int j) {
     StepBufs b;
     b.q = s->tape_q.as<float4>() + 6 * N * j;
     b.q_out = s->tape_q.as<float4>() + 6 * N * (j + 1);
+    b.pay = s->pf.physics == PHYS_MLS ? s->tape_pay.as<float4>() : nullptr;
     b.keys_in = s->tape_keys.as<uint32_t>() + N * j;
     b.keys_out = s->tape_keys.as<uint32_t>() + N * (j + 1);
     uint32_t* sk = s->tape_sk.as<uint32_t>() + N * j;
@@ -157,6 +159,7 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_keys.p, s->ck_keys.as<uint32_t>() + Nz * seg, sizeof(uint32_t) * Nz,
                            cudaMemcpyDeviceToDevice, st));
+        CK(launch_payload(s->view_for(tape_bufs(s, 0)), s->pf, st));
         for (int j = 0; j < len; ++j) {
             rc = record_step(s, tape_bufs(s, j), st, false);
             if (rc) return rc;

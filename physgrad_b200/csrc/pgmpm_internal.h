@@ -31,6 +31,8 @@ struct View {
     const MatDev* mats;
     float4* q;                 // 6 planes of N float4 (state at the start of the step)
     float4* q_out;             // where G2P writes the new state (== q in place; MLS only otherwise)
+    float4* pay;               // MLS P2G payload of the state in q (4 planes), read by P2G
+    float4* pay_out;           // payload of the state G2P writes (null: G2P does not write one)
     const float2* mV;          // (mass, V0)
     const int32_t* mat;        // material id (null when M == 1)
     uint32_t* keys;            // cell key per particle (physical order), input of the next sort
@@ -84,6 +86,7 @@ struct PhysFlags {
     bool has_fluid;  // some material uses the EOS model
 };
 cudaError_t launch_keys(const View& V, const PhysFlags& pf, cudaStream_t st);
+cudaError_t launch_payload(const View& V, const PhysFlags& pf, cudaStream_t st);
 cudaError_t launch_mark(const View& V, cudaStream_t st);
 cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);

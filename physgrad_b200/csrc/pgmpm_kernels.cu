@@ -48,6 +48,33 @@ __global__ void k_keys(View V) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// --------------------------------------------------------------- payload
+// P2G payload of the current MLS state (after an upload, a material change,
+// or at the start of a replayed segment); G2P keeps it current afterwards.
+template <bool MULTI>
+__global__ void k_payload(View V) {
+    const int64_t N = V.N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint32_t flags = 0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
+        const SceneDev& sc = scene_ref(V, s);
+        float x[3], F[9], v[3], C[9];
+        unpack_xF(V.q[p], V.q[N + p], V.q[2 * N + p], x, F);
+        unpack_vC(V.q[3 * N + p], V.q[4 * N + p], V.q[5 * N + p], v, C);
+        Stencil st;
+        make_stencil<PHYS_MLS>(sc, x, st, flags);
+        const float2 mv = V.mV[p];
+        float4 a0, a1, a2, a3;
+        mls_payload(sc, V.mats[MULTI ? V.mat[p] : 0], st.f, F, v, C, mv.x, mv.y, a0, a1, a2, a3);
+        V.pay[p] = a0;
+        V.pay[N + p] = a1;
+        V.pay[2 * N + p] = a2;
+        V.pay[3 * N + p] = a3;
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
 // ------------------------------------------------------------------ mark
 __global__ void k_mark(View V) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -363,23 +390,13 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V, AdjView AV) {
 #pragma unroll
                     for (int a = 0; a < 9; ++a) sm[(PAY_A + a) * P2G_SC + j] = Ad[a];
                 } else if (PHYS == PHYS_MLS) {
-                    const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
-                    const float4 q3 = V.q[3 * N + p], q4 = V.q[4 * N + p], q5 = V.q[5 * N + p];
-                    float xx[3], F[9], v[3], C[9];
-                    unpack_xF(q0, q1, q2, xx, F);
-                    unpack_vC(q3, q4, q5, v, C);
-                    const MatDev mt = V.mats[MULTI ? V.mat[p] : 0];
-                    float tau[9];
-                    kirchhoff(F, mt, tau);
-                    const float kk = -sc.dt * mv.y * sc.D;
-                    float Ad[9];
-#pragma unroll
-                    for (int a = 0; a < 9; ++a) Ad[a] = (kk * tau[a] + mv.x * C[a]) * sc.dx;
-                    sm[PAY_M * P2G_SC + j] = mv.x;
-#pragma unroll
-                    for (int a = 0; a < 3; ++a)
-                        sm[(PAY_B + a) * P2G_SC + j] =
-                            mv.x * v[a] - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
+                    // precomputed payload (G2P of the previous step / k_payload)
+                    const float4 a0 = V.pay[p], a1 = V.pay[N + p], a2 = V.pay[2 * N + p], a3 = V.pay[3 * N + p];
+                    sm[PAY_M * P2G_SC + j] = a0.w;
+                    sm[(PAY_B + 0) * P2G_SC + j] = a0.x;
+                    sm[(PAY_B + 1) * P2G_SC + j] = a0.y;
+                    sm[(PAY_B + 2) * P2G_SC + j] = a0.z;
+                    const float Ad[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
 #pragma unroll
                     for (int a = 0; a < 9; ++a) sm[(PAY_A + a) * P2G_SC + j] = Ad[a];
                 } else {
@@ -558,12 +575,27 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
                 flags |= FLAG_TILE_RANGE;
                 continue;
             }
-            const float4 q0 = V.q[p];
-            const float x[3] = {q0.x, q0.y, q0.z};
             Stencil st;
-            make_stencil<PHYS>(sc, x, st, flags);
             float m, b[3], Ad[9];
-            if (MODE == MODE_ADJ) {
+            if (MODE == MODE_MLS) {
+                // precomputed payload (G2P of the previous step / k_payload)
+                const float4 a0 = V.pay[p], a1 = V.pay[N + p], a2 = V.pay[2 * N + p], a3 = V.pay[3 * N + p];
+                m = a0.w;
+                b[0] = a0.x;
+                b[1] = a0.y;
+                b[2] = a0.z;
+                Ad[0] = a1.x; Ad[1] = a1.y; Ad[2] = a1.z; Ad[3] = a1.w;
+                Ad[4] = a2.x; Ad[5] = a2.y; Ad[6] = a2.z; Ad[7] = a2.w;
+                Ad[8] = a3.x;
+                st.f[0] = a3.y;
+                st.f[1] = a3.z;
+                st.f[2] = a3.w;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) mls_weights(st.f[a], st.w[a]);
+            } else if (MODE == MODE_ADJ) {
+                const float4 q0 = V.q[p];
+                const float x[3] = {q0.x, q0.y, q0.z};
+                make_stencil<PHYS>(sc, x, st, flags);
                 const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
                 float xx[3], F[9];
                 unpack_xF(q0, q1, q2, xx, F);
@@ -591,24 +623,10 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
                     b[a] = (gv[a] + sc.dt * gx[a]) - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
-            } else if (PHYS == PHYS_MLS) {
-                const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
-                const float4 q3 = V.q[3 * N + p], q4 = V.q[4 * N + p], q5 = V.q[5 * N + p];
-                const float2 mv = V.mV[p];
-                float xx[3], F[9], v[3], C[9];
-                unpack_xF(q0, q1, q2, xx, F);
-                unpack_vC(q3, q4, q5, v, C);
-                const MatDev mt = V.mats[MULTI ? V.mat[p] : 0];
-                float tau[9];
-                kirchhoff(F, mt, tau);
-                const float kk = -sc.dt * mv.y * sc.D;
-#pragma unroll
-                for (int a = 0; a < 9; ++a) Ad[a] = (kk * tau[a] + mv.x * C[a]) * sc.dx;
-                m = mv.x;
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-                    b[a] = m * v[a] - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
             } else {
+                const float4 q0 = V.q[p];
+                const float x[3] = {q0.x, q0.y, q0.z};
+                make_stencil<PHYS>(sc, x, st, flags);
                 const float4 q3 = V.q[3 * N + p];
                 const float2 mv = V.mV[p];
                 const bool regular = st.b[0] == st.s[0] && st.b[1] == st.s[1] && st.b[2] == st.s[2];
@@ -842,6 +860,26 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
         qo[3 * N + p] = o3;
         qo[4 * N + p] = o4;
         qo[5 * N + p] = o5;
+        // key and P2G payload of the new state for the next step
+        int so[3];
+        float fn[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float u;
+            so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS, u, flags);
+            fn[a] = fminf(fmaxf(__fsub_rn(u, (float)so[a]), 0.5f), 1.5f);
+        }
+        V.keys[p] = cell_key(sc, so);
+        if (V.pay_out) {
+            const float2 mv = V.mV[p];
+            float4 a0, a1, a2, a3;
+            mls_payload(sc, V.mats[MULTI ? V.mat[p] : 0], fn, Fn, nv, C, mv.x, mv.y, a0, a1, a2, a3);
+            V.pay_out[p] = a0;
+            V.pay_out[N + p] = a1;
+            V.pay_out[2 * N + p] = a2;
+            V.pay_out[3 * N + p] = a3;
+        }
+        return;
     } else {
         // material_point_method.h:599-666 in the same order of operations
         float nv[3] = {0.f, 0.f, 0.f};
@@ -1067,6 +1105,16 @@ cudaError_t launch_keys(const View& V, const PhysFlags& pf, cudaStream_t st) {
         k_keys<PHYS_MLS><<<grid_for(V.N, 256), 256, 0, st>>>(V);
     else
         k_keys<PHYS_REF><<<grid_for(V.N, 256), 256, 0, st>>>(V);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_payload(const View& V, const PhysFlags& pf, cudaStream_t st) {
+    if (V.N == 0 || pf.physics != PHYS_MLS) return cudaSuccess;
+    if (!V.pay) return cudaErrorInvalidValue;
+    if (pf.multi_mat)
+        k_payload<true><<<grid_for(V.N, 256), 256, 0, st>>>(V);
+    else
+        k_payload<false><<<grid_for(V.N, 256), 256, 0, st>>>(V);
     return cudaGetLastError();
 }
 

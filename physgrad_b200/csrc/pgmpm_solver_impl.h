@@ -58,6 +58,7 @@ inline int bits_for(uint64_t v) {
 struct StepBufs {
     float4* q;             // state at the start of the step (read by P2G and G2P)
     float4* q_out;         // state G2P writes (== q for the live solver)
+    float4* pay;           // MLS P2G payload of q, rewritten by G2P for q_out (null for REF physics)
     uint32_t* keys_in;     // keys sorted by this step
     uint32_t* keys_out;    // keys G2P writes for the next step (may equal keys_in)
     uint32_t *ka, *va, *kb, *vb;  // sort ping-pong; result in (ka, va) if which == 0 else (kb, vb)
@@ -109,7 +110,7 @@ struct pgmpm_solver_s {
     bool uploaded = false;
 
     // device buffers
-    pgmpm::DevBuf d_scenes, d_mats, q, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
+    pgmpm::DevBuf d_scenes, d_mats, q, pay, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
     pgmpm::DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
     uint32_t* h_counters = nullptr;  // pinned
 
@@ -128,6 +129,7 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf ck_q, ck_keys;         // checkpoints: states (6N float4) + keys (N u32)
     int tape_slots = 0;                  // allocated tape depth (steps per segment)
     pgmpm::DevBuf tape_q, tape_keys;     // (slots + 1) states and keys
+    pgmpm::DevBuf tape_pay;              // payload of the replayed state (one, reused by every slot)
     pgmpm::DevBuf tape_sk, tape_ord;     // slots x N sorted keys / order
     pgmpm::DevBuf tape_gv, tape_gvpre;   // slots x nodes float4
     pgmpm::DevBuf tape_flags, tape_tiles, tape_ctiles, tape_crange, tape_counters;
@@ -137,6 +139,7 @@ struct pgmpm_solver_s {
         pgmpm::StepBufs b;
         b.q = q.as<float4>();
         b.q_out = q.as<float4>();
+        b.pay = pf.physics == pgmpm::PHYS_MLS ? pay.as<float4>() : nullptr;
         b.keys_in = keys.as<uint32_t>();
         b.keys_out = keys.as<uint32_t>();
         b.ka = ka.as<uint32_t>();
@@ -163,6 +166,8 @@ struct pgmpm_solver_s {
         V.mats = d_mats.as<pgmpm::MatDev>();
         V.q = b.q;
         V.q_out = b.q_out;
+        V.pay = b.pay;
+        V.pay_out = b.pay;
         V.mV = mV.as<float2>();
         V.mat = pf.multi_mat ? mat.as<int32_t>() : nullptr;
         V.keys = b.keys_out;
@@ -204,6 +209,9 @@ struct pgmpm_solver_s {
 };
 
 namespace pgmpm {
+// Recompute the live MLS payload from the live state (after an upload, a
+// material change or a state restore).
+int refresh_payload(pgmpm_solver s, cudaStream_t st);
 // Enqueue one step on `st` using buffers `b` (events ev[0..4] when timed).
 int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed);
 // Run n steps of the live state (graph, eager or profiled).
