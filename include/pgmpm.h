@@ -181,13 +181,23 @@ PGMPM_API int pgmpm_check_status(pgmpm_solver s, uint32_t* flags, void* stream);
 /* p2g_block, g2p_block: threads per block; ppt: particles per P2G chunk.
  * 0 keeps the current value.  use_graph: capture each step as a CUDA graph. */
 PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p_block, int32_t use_graph);
-/* Kernel variants.  p2g_variant 0: per-cell register accumulation over
- * occupied 4^3 cell tiles (persistent, p2g_tiles_per_sm blocks per SM);
- * 1: per-particle shared-memory atomics over chunks of ppt particles.
+/* Kernel variants.  p2g_variant 0: (cell, z-slice) register accumulation
+ * over occupied 4^3 cell tiles (persistent, p2g_tiles_per_sm blocks per SM);
+ * 1: per-particle shared-memory atomics over chunks of ppt particles;
+ * 2: one thread per cell with 108 register accumulators (default).
  * g2p_variant 0: tile-staged gather (g2p_tiles_per_sm blocks per SM);
- * 1: direct gather, one thread per particle.  Negative keeps a value. */
+ * 1: direct gather in sorted order; 2: direct gather in physical order.
+ * Negative keeps a value. */
 PGMPM_API int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant,
                                         int32_t p2g_tiles_per_sm, int32_t g2p_tiles_per_sm);
+/* Per-step grouping of particles by cell.  PGMPM_SORT_BINS (default): two
+ * counting sorts (cell tile, then cell in tile), O(N + tiles); the keys come
+ * out sorted, particles that share a cell in atomic-arrival order.
+ * PGMPM_SORT_RADIX: the stable LSD radix sort (same order as a stable CPU
+ * sort of the keys). */
+#define PGMPM_SORT_BINS 0
+#define PGMPM_SORT_RADIX 1
+PGMPM_API int pgmpm_set_step_sort(pgmpm_solver s, int32_t kind);
 /* Time candidate (block, ppt) settings on the solver's own state (restored
  * afterwards) and keep the fastest. */
 PGMPM_API int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream);

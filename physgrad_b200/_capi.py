@@ -47,6 +47,9 @@ ARRAY_KEYS = 1
 ARRAY_SORTED_KEYS = 2
 ARRAY_SORTED_ORDER = 3
 
+SORT_BINS = 0
+SORT_RADIX = 1
+
 PTR_HOST = 0
 PTR_DEVICE = 1
 
@@ -119,6 +122,7 @@ SIGNATURES = {
     "pgmpm_set_tuning": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
     "pgmpm_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
     "pgmpm_set_kernel_variants": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
+    "pgmpm_set_step_sort": (ctypes.c_int, [_vp, _i32]),
     "pgmpm_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "pgmpm_get_metrics": (ctypes.c_int, [_vp, ctypes.POINTER(Metrics)]),
     "pgmpm_forward_checkpointed": (ctypes.c_int, [_vp, _i32, _i32, _vp]),

@@ -87,11 +87,26 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) 
     CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
     CK(cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * CNT_RESET, st));
     if (timed) CK(cudaEventRecord(s->ev[0], st));
-    int which = 0;
-    CK(radix_sort_pairs(b.keys_in, nullptr, b.ka, b.va, b.kb, b.vb, s->sort_scratch.as<uint32_t>(), s->N,
-                        s->key_bits, &which, st));
-    if (which != b.which) return fail(PGMPM_ERR_STATE, "internal: sort buffer parity changed");
-    CK(launch_mark(V, st));
+    if (s->tune.step_sort == 0) {
+        BinSortBufs B;
+        B.keys_in = b.keys_in;
+        B.tcount = s->bs_tcount.as<uint32_t>();
+        B.toff = s->bs_toff.as<uint32_t>();
+        B.bsum = s->bs_bsum.as<uint32_t>();
+        B.slot = s->bs_slot.as<uint32_t>();
+        B.out_k = b.which ? b.kb : b.ka;  // where the step's readers look (View::skeys / order)
+        B.out_v = b.which ? b.vb : b.va;
+        B.tmp_k = b.which ? b.ka : b.kb;
+        B.tmp_v = b.which ? b.va : b.vb;
+        B.cell_range = b.cell_range;
+        CK(bin_sort_step(V, B, s->num_sms, st));
+    } else {
+        int which = 0;
+        CK(radix_sort_pairs(b.keys_in, nullptr, b.ka, b.va, b.kb, b.vb, s->sort_scratch.as<uint32_t>(), s->N,
+                            s->key_bits, &which, st));
+        if (which != b.which) return fail(PGMPM_ERR_STATE, "internal: sort buffer parity changed");
+        CK(launch_mark(V, st));
+    }
     if (timed) CK(cudaEventRecord(s->ev[1], st));
     CK(launch_p2g(V, s->pf, s->tune, s->num_sms, st));
     if (timed) CK(cudaEventRecord(s->ev[2], st));
@@ -287,6 +302,11 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->ctile_list, sizeof(uint32_t) * (size_t)ct_base);
     AL(s->ctile_range, sizeof(uint2) * (size_t)ct_base);
     AL(s->counters, sizeof(uint32_t) * CNT_WORDS);
+    AL(s->bs_tcount, sizeof(uint32_t) * ((size_t)ct_base + 1));
+    AL(s->bs_toff, sizeof(uint32_t) * ((size_t)ct_base + 1));
+    AL(s->bs_bsum, sizeof(uint32_t) * (size_t)bin_sort_scan_blocks((int)ct_base));
+    AL(s->bs_slot, n4);
+    AL(s->cell_range, sizeof(uint2) * 64 * (size_t)ct_base);
 #undef AL
     if (e == cudaSuccess) e = cudaMemcpy(s->d_scenes.p, s->scenes.data(), sizeof(SceneDev) * n_scenes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice);
@@ -521,6 +541,15 @@ int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_v
             s->tune.tile_blocks_per_sm = p2g_tiles_per_sm;
     }
     if (g2p_tiles_per_sm > 0) s->tune.g2p_tiles_per_sm = g2p_tiles_per_sm;
+    s->drop_graph();
+    return PGMPM_OK;
+}
+
+int pgmpm_set_step_sort(pgmpm_solver s, int32_t kind) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (kind != PGMPM_SORT_BINS && kind != PGMPM_SORT_RADIX)
+        return fail(PGMPM_ERR_ARG, "kind must be PGMPM_SORT_BINS or PGMPM_SORT_RADIX");
+    s->tune.step_sort = kind;
     s->drop_graph();
     return PGMPM_OK;
 }

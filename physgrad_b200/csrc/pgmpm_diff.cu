@@ -77,6 +77,7 @@ StepBufs tape_bufs(pgmpm_solver s, int j) {
     b.tile_list = s->tape_tiles.as<uint32_t>() + (size_t)s->total_nt * j;
     b.ctile_list = s->tape_ctiles.as<uint32_t>() + (size_t)s->total_ct * j;
     b.ctile_range = s->tape_crange.as<uint2>() + (size_t)s->total_ct * j;
+    b.cell_range = nullptr;  // replayed steps keep no cell table: P2G searches the sorted keys
     b.counters = s->tape_counters.as<uint32_t>() + CNT_WORDS * j;
     return b;
 }

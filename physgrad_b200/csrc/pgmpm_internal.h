@@ -45,6 +45,7 @@ struct View {
     uint32_t* tile_list;       // active node tiles
     uint32_t* ctile_list;      // occupied cell tiles (global cell tile ids)
     uint2* ctile_range;        // per global cell tile: [begin, end) in sorted order
+    const uint2* cell_range;   // per global cell: [begin, end) in sorted order (null: search skeys)
     uint32_t* counters;        // see CNT_*
     int total_ct, total_nt;
 };
@@ -64,6 +65,7 @@ struct Tuning {
     int tile_blocks_per_sm = 3;  // persistent P2G tile kernel: blocks per SM
     int g2p_tiles_per_sm = 2;    // persistent G2P tile kernel: blocks per SM (256 threads)
     int cell_blocks_per_sm = 6;  // persistent P2G thread-per-cell kernel (variant 2): blocks per SM
+    int step_sort = 0;           // per-step sort: 0 = bin sort (counting sorts by tile, then cell), 1 = radix sort
 };
 
 // pgmpm_sort.cu
@@ -78,6 +80,23 @@ int radix_passes(int key_bits);
 cudaError_t radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uint32_t* va, uint32_t* kb,
                              uint32_t* vb, uint32_t* scratch, int64_t n, int key_bits, int* which,
                              cudaStream_t st);
+
+// Per-step bin sort (pgmpm_sort.cu): keys_in (physical order) -> out_k /
+// out_v sorted by key, plus the occupied cell tiles, their ranges, the
+// active node tiles (View fields) and, when cell_range is set, every cell's
+// [begin, end) in the sorted order.
+struct BinSortBufs {
+    const uint32_t* keys_in;
+    uint32_t* tcount;      // total_ct + 1 words
+    uint32_t* toff;        // total_ct + 1 words
+    uint32_t* bsum;        // bin_sort_scan_blocks(total_ct) words
+    uint32_t* slot;        // N words
+    uint32_t *tmp_k, *tmp_v;  // N words each (tile-grouped)
+    uint32_t *out_k, *out_v;  // N words each
+    uint2* cell_range;     // total_ct * 64, or null
+};
+int64_t bin_sort_scan_blocks(int total_ct);
+cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cudaStream_t st);
 
 // pgmpm_kernels.cu
 struct PhysFlags {

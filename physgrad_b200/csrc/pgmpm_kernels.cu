@@ -1,21 +1,25 @@
 // pgmpm_kernels.cu -- the forward MLS-MPM step on sm_100a.
 //
-// Per step (all on one stream, capturable as a CUDA graph):
-//   [sort]   radix sort of the cell keys written by the previous G2P
-//   k_mark   node tiles touched by each occupied cell tile -> active list
-//   k_p2g    one block per chunk of `ppt` sorted particles; for each run of
-//            the chunk that lies in one 4^3 cell tile the block accumulates
-//            into a 6^3-node shared-memory tile (4 channels: m, p) and then
-//            flushes every touched node with ONE vector atomic
-//            (red.global.add.v4.f32) into grid_mp.  Lanes are spread over
-//            the run (lane l of a warp takes particle l*R + r) so that the 32
-//            shared atomics of one instruction fall in different cells.
+// Per step (all on one stream, captured as one CUDA graph):
+//   [sort]   bin sort of the cell keys written by the previous G2P
+//            (pgmpm_sort.cu): occupied cell tiles, their sorted ranges, each
+//            cell's range, and the active node tiles
+//   P2G      default k_p2g_cells: one 64-thread block per occupied 4^3 cell
+//            tile, thread c owns cell c and the 27 nodes of its stencil (108
+//            register accumulators), walks its cell's particles and adds the
+//            payload (m, b, affine matrix, stencil fraction) precomputed by
+//            the previous G2P; the block then sums the 6^3 nodes the tile
+//            touches in shared memory and flushes each with one vector atomic
+//            (red.global.add.v4.f32) into grid_mp.  k_p2g_tiles (cell x
+//            z-slice) and k_p2g (chunks, shared atomics) are the other
+//            variants.
 //   k_grid   active node tiles only: v = p/m + dt g, walls, (v, m) -> grid_v,
 //            grid_mp cleared for the next step.
-//   k_g2p    one thread per sorted particle: 27-node gather of v, APIC C,
-//            F <- (I + dt C) F, x <- x + dt v, and the particle's next key.
-// HBM-bound: no tensor-core work exists on this path (scatter/gather
-// stencil, not a dense contraction).
+//   G2P      default k_g2p_phys: one thread per particle in physical order:
+//            27-node gather of v, APIC C, F <- (I + dt C) F, x <- x + dt v,
+//            the particle's next key and next P2G payload.
+// HBM- and latency-bound: no tensor-core work exists on this path (a
+// scatter/gather stencil, not a dense contraction).
 #include "pgmpm_internal.h"
 
 namespace pgmpm {
@@ -522,6 +526,44 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V, AdjView AV) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// Reverse of G2P for one particle (MLS): the scatter payload of dL/dv_i
+// and dL/dm_i contributions, node o gets w_o (b + Ad o).  Also fills the
+// stencil (f, w) of the particle's position.
+template <bool MULTI, bool FLUID>
+__device__ __forceinline__ void adj_payload(const View& V, const AdjView& AV, const SceneDev& sc, int64_t p,
+                                            Stencil& st, uint32_t& flags, float b[3], float Ad[9]) {
+    const int64_t N = V.N;
+    const float4 q0 = V.q[p];
+    const float x[3] = {q0.x, q0.y, q0.z};
+    make_stencil<PHYS_MLS>(sc, x, st, flags);
+    const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
+    float xx[3], F[9];
+    unpack_xF(q0, q1, q2, xx, F);
+    float gx[3], gF[9], gv[3], gC[9];
+    unpack_xF(AV.g[p], AV.g[N + p], AV.g[2 * N + p], gx, gF);
+    unpack_vC(AV.g[3 * N + p], AV.g[4 * N + p], AV.g[5 * N + p], gv, gC);
+    if (FLUID && V.mats[MULTI ? V.mat[p] : 0].model == MODEL_EOS) {
+        float Cn[9], vdum[3], M[9], Fr[9], cof[9];
+        unpack_vC(AV.q_next[3 * N + p], AV.q_next[4 * N + p], AV.q_next[5 * N + p], vdum, Cn);
+#pragma unroll
+        for (int a = 0; a < 9; ++a) M[a] = sc.dt * Cn[a] + ((a % 4 == 0) ? 1.f : 0.f);
+        m3_mul(M, F, Fr);
+        m3_cof(Fr, cof);
+        const float J = Fr[0] * cof[0] + Fr[1] * cof[1] + Fr[2] * cof[2];
+        const float cc = cbrtf(J) / (3.f * J) * (gF[0] + gF[4] + gF[8]);
+#pragma unroll
+        for (int a = 0; a < 9; ++a) gF[a] = cc * cof[a];
+    }
+    float gFFt[9];
+    m3_mulT(gF, F, gFFt);
+    const float sD = sc.D * sc.dx;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) Ad[a] = sD * (gC[a] + sc.dt * gFFt[a]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        b[a] = (gv[a] + sc.dt * gx[a]) - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
+}
+
 // ------------------------------------------------ P2G, one thread per cell
 // Variant 2: one 64-thread block per occupied cell tile, thread c owns cell
 // c and all 27 nodes of its stencil (108 register accumulators).  The
@@ -552,20 +594,28 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
         const int lt = (int)ct - sc.ct_base;
         const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
                   oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
-        // this cell's sorted range: keys in the tile are ordered by local cell
-        const uint32_t kc = (ct << 6) | (uint32_t)c;
-        uint32_t lo = rg.x, hi = rg.y;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (V.skeys[mid] < kc) lo = mid + 1; else hi = mid;
+        // this cell's sorted range: from the sort's cell table, else a
+        // search of the tile's keys (ordered by local cell)
+        uint32_t cb, ce;
+        if (V.cell_range) {
+            const uint2 cr = V.cell_range[(size_t)ct * 64 + c];
+            cb = max(cr.x, rg.x);
+            ce = min(cr.y, rg.y);
+        } else {
+            const uint32_t kc = (ct << 6) | (uint32_t)c;
+            uint32_t lo = rg.x, hi = rg.y;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (V.skeys[mid] < kc) lo = mid + 1; else hi = mid;
+            }
+            cb = lo;
+            hi = rg.y;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (V.skeys[mid] <= kc) lo = mid + 1; else hi = mid;
+            }
+            ce = lo;
         }
-        const uint32_t cb = lo;
-        hi = rg.y;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (V.skeys[mid] <= kc) lo = mid + 1; else hi = mid;
-        }
-        const uint32_t ce = lo;
         float acc[27][4];
 #pragma unroll
         for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = acc[o][3] = 0.f;
@@ -593,36 +643,8 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
 #pragma unroll
                 for (int a = 0; a < 3; ++a) mls_weights(st.f[a], st.w[a]);
             } else if (MODE == MODE_ADJ) {
-                const float4 q0 = V.q[p];
-                const float x[3] = {q0.x, q0.y, q0.z};
-                make_stencil<PHYS>(sc, x, st, flags);
-                const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
-                float xx[3], F[9];
-                unpack_xF(q0, q1, q2, xx, F);
-                float gx[3], gF[9], gv[3], gC[9];
-                unpack_xF(AV.g[p], AV.g[N + p], AV.g[2 * N + p], gx, gF);
-                unpack_vC(AV.g[3 * N + p], AV.g[4 * N + p], AV.g[5 * N + p], gv, gC);
-                if (FLUID && V.mats[MULTI ? V.mat[p] : 0].model == MODEL_EOS) {
-                    float Cn[9], vdum[3], M[9], Fr[9], cof[9];
-                    unpack_vC(AV.q_next[3 * N + p], AV.q_next[4 * N + p], AV.q_next[5 * N + p], vdum, Cn);
-#pragma unroll
-                    for (int a = 0; a < 9; ++a) M[a] = sc.dt * Cn[a] + ((a % 4 == 0) ? 1.f : 0.f);
-                    m3_mul(M, F, Fr);
-                    m3_cof(Fr, cof);
-                    const float J = Fr[0] * cof[0] + Fr[1] * cof[1] + Fr[2] * cof[2];
-                    const float cc = cbrtf(J) / (3.f * J) * (gF[0] + gF[4] + gF[8]);
-#pragma unroll
-                    for (int a = 0; a < 9; ++a) gF[a] = cc * cof[a];
-                }
-                float gFFt[9];
-                m3_mulT(gF, F, gFFt);
-                const float sD = sc.D * sc.dx;
-#pragma unroll
-                for (int a = 0; a < 9; ++a) Ad[a] = sD * (gC[a] + sc.dt * gFFt[a]);
+                adj_payload<MULTI, FLUID>(V, AV, sc, p, st, flags, b, Ad);
                 m = 0.f;
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-                    b[a] = (gv[a] + sc.dt * gx[a]) - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
             } else {
                 const float4 q0 = V.q[p];
                 const float x[3] = {q0.x, q0.y, q0.z};

@@ -198,7 +198,197 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
         }
     }
 }
+
+// --------------------------------------------------- per-step bin sort
+// The MPM step groups particles by cell without a full radix sort: the key
+// is (cell tile << 6 | cell in tile), and both levels are counting sorts.
+//   bs_count     one pass over the keys: particles per cell tile (warp-
+//                aggregated atomics, match.any on the tile) and each
+//                particle's slot inside its tile.
+//   bs_reduce / bs_top / bs_down
+//                exclusive scan of the tile counts (reduce, scan of block
+//                sums, scan + offsets).  bs_down also emits every occupied
+//                tile: its sorted range, its entry in the occupied-tile list
+//                and the marks of the 8 node tiles it touches.
+//   bs_scatter   particle -> tile offset + slot (tile-grouped order).
+//   bs_cells     per occupied tile: 64-bin counting sort by cell into the
+//                final (key, particle) arrays, and every cell's range.
+// O(N + tiles) traffic.  Keys come out sorted; the order of particles that
+// share a cell depends on atomic arrival, which the step does not rely on.
+constexpr int BS_T = 256;
+constexpr int BS_SCAN = 1024;  // tile counts per scan block
+
+__global__ void __launch_bounds__(BS_T) bs_count(const uint32_t* __restrict__ keys, int64_t n, uint32_t total_ct,
+                                                 uint32_t* __restrict__ tcount, uint32_t* __restrict__ slot,
+                                                 uint32_t* __restrict__ counters) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const int64_t stride = (int64_t)gridDim.x * BS_T;
+    uint32_t bad = 0;
+    // whole warps iterate together (match.any needs every lane)
+    for (int64_t base = (int64_t)blockIdx.x * BS_T + (threadIdx.x & ~31); base < n; base += stride) {
+        const int64_t i = base + lane;
+        const bool ok = i < n;
+        uint32_t t = 0xFFFFFFFFu;
+        if (ok) {
+            t = keys[i] >> 6;
+            if (t >= total_ct) {  // out-of-range key: overflow bin after the last tile
+                bad = 1;
+                t = total_ct;
+            }
+        }
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, t);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (ok && lane == leader) b = atomicAdd(&tcount[t], (uint32_t)__popc(peers));
+        b = __shfl_sync(0xFFFFFFFFu, b, leader);
+        if (ok) slot[i] = b + (uint32_t)__popc(peers & lt);
+    }
+    if (bad) atomicOr(&counters[CNT_FLAGS], FLAG_TILE_RANGE);
+}
+
+__global__ void __launch_bounds__(BS_SCAN) bs_reduce(const uint32_t* __restrict__ tcount, int64_t n,
+                                                     uint32_t* __restrict__ bsum) {
+    __shared__ uint32_t sh[32];
+    const int64_t i = (int64_t)blockIdx.x * BS_SCAN + threadIdx.x;
+    uint32_t tot;
+    block_excl_scan(i < n ? tcount[i] : 0u, sh, tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(BS_SCAN) bs_top(uint32_t* __restrict__ bsum, int nb) {
+    __shared__ uint32_t sh[32];
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += BS_SCAN) {
+        const int b = b0 + threadIdx.x;
+        const uint32_t v = b < nb ? bsum[b] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(v, sh, tot);
+        if (b < nb) bsum[b] = carry + ex;
+        carry += tot;
+    }
+}
+
+__global__ void __launch_bounds__(BS_SCAN) bs_down(View V, const uint32_t* __restrict__ tcount, int64_t n,
+                                                   const uint32_t* __restrict__ bsum, uint32_t* __restrict__ toff) {
+    __shared__ uint32_t sh[32];
+    const int64_t t = (int64_t)blockIdx.x * BS_SCAN + threadIdx.x;
+    const uint32_t c = t < n ? tcount[t] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(c, sh, tot) + bsum[blockIdx.x];
+    if (t >= n) return;
+    toff[t] = ex;
+    if (c == 0 || t >= V.total_ct) return;  // empty, or the overflow bin
+    V.ctile_range[t] = make_uint2(ex, ex + c);
+    V.ctile_list[atomicAdd(&V.counters[CNT_CTILES], 1u)] = (uint32_t)t;
+    const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)t);
+    const SceneDev& sc = V.scenes[s];
+    const int lt = (int)t - sc.ct_base;
+    const int tx = lt % sc.ct[0], ty = (lt / sc.ct[0]) % sc.ct[1], tz = lt / (sc.ct[0] * sc.ct[1]);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int nx = tx + (k & 1), ny = ty + ((k >> 1) & 1), nz = tz + (k >> 2);
+        const uint32_t nt = (uint32_t)(sc.nt_base + (nz * sc.nt[1] + ny) * sc.nt[0] + nx);
+        if (atomicExch(&V.tile_flags[nt], 1u) == 0u) V.tile_list[atomicAdd(&V.counters[CNT_TILES], 1u)] = nt;
+    }
+}
+
+__global__ void __launch_bounds__(BS_T) bs_scatter(const uint32_t* __restrict__ keys, int64_t n, uint32_t total_ct,
+                                                   const uint32_t* __restrict__ slot,
+                                                   const uint32_t* __restrict__ toff, uint32_t* __restrict__ tk,
+                                                   uint32_t* __restrict__ tv) {
+    const int64_t stride = (int64_t)gridDim.x * BS_T;
+    for (int64_t i = (int64_t)blockIdx.x * BS_T + threadIdx.x; i < n; i += stride) {
+        const uint32_t key = keys[i];
+        const uint32_t t = min(key >> 6, total_ct);
+        const uint32_t pos = toff[t] + slot[i];
+        if ((int64_t)pos < n) {
+            tk[pos] = key;
+            tv[pos] = (uint32_t)i;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(BS_T) bs_cells(View V, const uint32_t* __restrict__ tk,
+                                                 const uint32_t* __restrict__ tv, uint32_t* __restrict__ ok_,
+                                                 uint32_t* __restrict__ ov, uint2* __restrict__ cell_range) {
+    __shared__ uint32_t s_cnt[64];
+    __shared__ uint32_t s_off[64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    for (uint32_t w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        const uint32_t ct = V.ctile_list[w];
+        const uint2 rg = V.ctile_range[ct];
+        if (threadIdx.x < 64) s_cnt[threadIdx.x] = 0u;
+        __syncthreads();
+        for (uint32_t b = rg.x + warp * 32; b < rg.y; b += BS_T) {
+            const uint32_t i = b + lane;
+            const bool ok = i < rg.y;
+            const uint32_t c = ok ? (tk[i] & 63u) : 64u + lane;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, c);
+            if (ok && lane == __ffs(peers) - 1) atomicAdd(&s_cnt[c], (uint32_t)__popc(peers));
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t a = s_cnt[2 * lane], b = s_cnt[2 * lane + 1];
+            uint32_t x = a + b;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= o) x += y;
+            }
+            const uint32_t e = x - a - b;  // exclusive prefix of cell 2*lane
+            s_off[2 * lane] = e;
+            s_off[2 * lane + 1] = e + a;
+            if (cell_range) {
+                cell_range[(size_t)ct * 64 + 2 * lane] = make_uint2(rg.x + e, rg.x + e + a);
+                cell_range[(size_t)ct * 64 + 2 * lane + 1] = make_uint2(rg.x + e + a, rg.x + e + a + b);
+            }
+        }
+        __syncthreads();
+        for (uint32_t b = rg.x + warp * 32; b < rg.y; b += BS_T) {
+            const uint32_t i = b + lane;
+            const bool ok = i < rg.y;
+            const uint32_t key = ok ? tk[i] : 0u;
+            const uint32_t c = ok ? (key & 63u) : 64u + lane;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, c);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (ok && lane == leader) base = atomicAdd(&s_off[c], (uint32_t)__popc(peers));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (ok) {
+                const uint32_t pos = rg.x + base + (uint32_t)__popc(peers & lt);
+                if (pos < rg.y) {
+                    ok_[pos] = key;
+                    ov[pos] = tv[i];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
 }  // namespace
+
+int64_t bin_sort_scan_blocks(int total_ct) { return ((int64_t)total_ct + 1 + BS_SCAN - 1) / BS_SCAN; }
+
+cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cudaStream_t st) {
+    const int64_t n = V.N;
+    if (n <= 0) return cudaSuccess;
+    const int64_t nbins = (int64_t)V.total_ct + 1;  // + overflow bin
+    const int nb = (int)bin_sort_scan_blocks(V.total_ct);
+    cudaError_t e = cudaMemsetAsync(B.tcount, 0, sizeof(uint32_t) * nbins, st);
+    if (e != cudaSuccess) return e;
+    const int64_t g64 = (n + BS_T - 1) / BS_T;
+    const int g = (int)(g64 < (int64_t)num_sms * 8 ? g64 : (int64_t)num_sms * 8);
+    bs_count<<<g, BS_T, 0, st>>>(B.keys_in, n, (uint32_t)V.total_ct, B.tcount, B.slot, V.counters);
+    bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, nbins, B.bsum);
+    bs_top<<<1, BS_SCAN, 0, st>>>(B.bsum, nb);
+    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, nbins, B.bsum, B.toff);
+    bs_scatter<<<g, BS_T, 0, st>>>(B.keys_in, n, (uint32_t)V.total_ct, B.slot, B.toff, B.tmp_k, B.tmp_v);
+    bs_cells<<<num_sms * 8, BS_T, 0, st>>>(V, B.tmp_k, B.tmp_v, B.out_k, B.out_v, B.cell_range);
+    return cudaGetLastError();
+}
 
 int64_t radix_sort_scratch_words(int64_t n) { return radix_scratch_words_for(n); }
 

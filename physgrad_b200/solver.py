@@ -251,6 +251,10 @@ class Simulator:
         check(lib().pgmpm_set_kernel_variants(self._h, int(p2g_variant), int(g2p_variant), int(p2g_tiles_per_sm),
                                               int(g2p_tiles_per_sm)))
 
+    def set_step_sort(self, kind: int):
+        """C.SORT_BINS (default) or C.SORT_RADIX (stable order within a cell)."""
+        check(lib().pgmpm_set_step_sort(self._h, int(kind)))
+
     def autotune(self, reps: int = 3, stream=None) -> dict:
         check(lib().pgmpm_autotune(self._h, int(reps), _stream_handle(stream)))
         m = self.metrics()
