@@ -190,11 +190,12 @@ PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, i
  * Negative keeps a value. */
 PGMPM_API int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant,
                                         int32_t p2g_tiles_per_sm, int32_t g2p_tiles_per_sm);
-/* Per-step grouping of particles by cell.  PGMPM_SORT_BINS (default): two
- * counting sorts (cell tile, then cell in tile), O(N + tiles); the keys come
- * out sorted, particles that share a cell in atomic-arrival order.
- * PGMPM_SORT_RADIX: the stable LSD radix sort (same order as a stable CPU
- * sort of the keys). */
+/* Per-step grouping of particles by cell.  PGMPM_SORT_BINS: a counting sort
+ * over the cells, O(N + occupied cells + tiles) per step with 8 bytes of
+ * scratch per cell; the keys come out sorted, particles that share a cell in
+ * atomic-arrival order.  PGMPM_SORT_RADIX: the stable LSD radix sort, O(N)
+ * per pass (the order of a stable CPU sort of the keys).  pgmpm_create picks
+ * BINS when the grids hold at most about 8 cells per particle, else RADIX. */
 #define PGMPM_SORT_BINS 0
 #define PGMPM_SORT_RADIX 1
 PGMPM_API int pgmpm_set_step_sort(pgmpm_solver s, int32_t kind);

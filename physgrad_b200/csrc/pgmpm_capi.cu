@@ -70,6 +70,22 @@ int material_to_dev(const pgmpm_material& m, MatDev& d) {
     return PGMPM_OK;
 }
 
+int alloc_bin_sort(pgmpm_solver s) {
+    if (s->bs_ccount.p) return PGMPM_OK;
+    const size_t ct = (size_t)s->total_ct;
+    CK(s->bs_ccount.alloc(sizeof(uint32_t) * (ct * 64 + 1)));
+    CK(s->bs_coff.alloc(sizeof(uint32_t) * ct * 64));
+    CK(s->bs_tcount.alloc(sizeof(uint32_t) * (ct + 1)));
+    CK(s->bs_toff.alloc(sizeof(uint32_t) * (ct + 1)));
+    CK(s->bs_bsum.alloc(sizeof(uint32_t) * (size_t)bin_sort_scan_blocks((int)ct)));
+    CK(s->bs_slot.alloc(sizeof(uint32_t) * (size_t)std::max<int64_t>(s->N, 1)));
+    CK(s->cell_range.alloc(sizeof(uint2) * 64 * std::max<size_t>(ct, 1)));
+    // the counters start at zero and every sort leaves them zero
+    CK(cudaMemset(s->bs_ccount.p, 0, s->bs_ccount.bytes));
+    CK(cudaMemset(s->bs_tcount.p, 0, s->bs_tcount.bytes));
+    return PGMPM_OK;
+}
+
 int refresh_payload(pgmpm_solver s, cudaStream_t st) {
     if (s->N == 0 || s->pf.physics != PHYS_MLS) return PGMPM_OK;
     CK(launch_payload(s->view(), s->pf, st));
@@ -83,21 +99,22 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) 
         return PGMPM_OK;
     }
     View V = s->view_for(b);
-    // per-step resets: active tile flags, tile counts, active node count, work cursors
-    CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
+    // per-step resets: tile counts, active node count, work cursors, and the
+    // active node tile flags (the bin sort writes every flag itself)
+    if (s->tune.step_sort != 0) CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
     CK(cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * CNT_RESET, st));
     if (timed) CK(cudaEventRecord(s->ev[0], st));
     if (s->tune.step_sort == 0) {
         BinSortBufs B;
         B.keys_in = b.keys_in;
+        B.ccount = s->bs_ccount.as<uint32_t>();
+        B.coff = s->bs_coff.as<uint32_t>();
         B.tcount = s->bs_tcount.as<uint32_t>();
         B.toff = s->bs_toff.as<uint32_t>();
         B.bsum = s->bs_bsum.as<uint32_t>();
         B.slot = s->bs_slot.as<uint32_t>();
         B.out_k = b.which ? b.kb : b.ka;  // where the step's readers look (View::skeys / order)
         B.out_v = b.which ? b.vb : b.va;
-        B.tmp_k = b.which ? b.ka : b.kb;
-        B.tmp_v = b.which ? b.va : b.vb;
         B.cell_range = b.cell_range;
         CK(bin_sort_step(V, B, s->num_sms, st));
     } else {
@@ -302,12 +319,11 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->ctile_list, sizeof(uint32_t) * (size_t)ct_base);
     AL(s->ctile_range, sizeof(uint2) * (size_t)ct_base);
     AL(s->counters, sizeof(uint32_t) * CNT_WORDS);
-    AL(s->bs_tcount, sizeof(uint32_t) * ((size_t)ct_base + 1));
-    AL(s->bs_toff, sizeof(uint32_t) * ((size_t)ct_base + 1));
-    AL(s->bs_bsum, sizeof(uint32_t) * (size_t)bin_sort_scan_blocks((int)ct_base));
-    AL(s->bs_slot, n4);
-    AL(s->cell_range, sizeof(uint2) * 64 * (size_t)ct_base);
 #undef AL
+    // the bin sort keeps 8 bytes per cell: default for grids with at most ~8
+    // cells per particle, the radix sort (O(N) per pass) for sparser ones
+    s->tune.step_sort = (int64_t)ct_base * 64 <= 8 * std::max<int64_t>(N, 1) + (1 << 20) ? 0 : 1;
+    if (e == cudaSuccess && s->tune.step_sort == 0 && alloc_bin_sort(s) != PGMPM_OK) e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = cudaMemcpy(s->d_scenes.p, s->scenes.data(), sizeof(SceneDev) * n_scenes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(s->grid_mp.p, 0, s->grid_mp.bytes);
@@ -549,6 +565,11 @@ int pgmpm_set_step_sort(pgmpm_solver s, int32_t kind) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
     if (kind != PGMPM_SORT_BINS && kind != PGMPM_SORT_RADIX)
         return fail(PGMPM_ERR_ARG, "kind must be PGMPM_SORT_BINS or PGMPM_SORT_RADIX");
+    if (kind == PGMPM_SORT_BINS) {
+        DeviceGuard dg(s->device);
+        int rc = alloc_bin_sort(s);
+        if (rc) return rc;
+    }
     s->tune.step_sort = kind;
     s->drop_graph();
     return PGMPM_OK;

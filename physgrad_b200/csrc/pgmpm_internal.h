@@ -83,15 +83,17 @@ cudaError_t radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t*
 
 // Per-step bin sort (pgmpm_sort.cu): keys_in (physical order) -> out_k /
 // out_v sorted by key, plus the occupied cell tiles, their ranges, the
-// active node tiles (View fields) and, when cell_range is set, every cell's
-// [begin, end) in the sorted order.
+// active node tiles and their flags (View fields) and, when cell_range is
+// set, every cell's [begin, end) in the sorted order of the occupied tiles.
+// ccount and tcount must be zero on entry and are left zero.
 struct BinSortBufs {
     const uint32_t* keys_in;
-    uint32_t* tcount;      // total_ct + 1 words
+    uint32_t* ccount;      // total_ct * 64 + 1 words (cells + overflow bin), zero between steps
+    uint32_t* coff;        // total_ct * 64 words
+    uint32_t* tcount;      // total_ct + 1 words, zero between steps
     uint32_t* toff;        // total_ct + 1 words
     uint32_t* bsum;        // bin_sort_scan_blocks(total_ct) words
     uint32_t* slot;        // N words
-    uint32_t *tmp_k, *tmp_v;  // N words each (tile-grouped)
     uint32_t *out_k, *out_v;  // N words each
     uint2* cell_range;     // total_ct * 64, or null
 };

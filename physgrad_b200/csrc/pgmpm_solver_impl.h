@@ -113,7 +113,7 @@ struct pgmpm_solver_s {
     // device buffers
     pgmpm::DevBuf d_scenes, d_mats, q, pay, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
     pgmpm::DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
-    pgmpm::DevBuf bs_tcount, bs_toff, bs_bsum, bs_slot, cell_range;  // per-step bin sort scratch
+    pgmpm::DevBuf bs_ccount, bs_coff, bs_tcount, bs_toff, bs_bsum, bs_slot, cell_range;  // per-step bin sort
     uint32_t* h_counters = nullptr;  // pinned
 
     // graph
@@ -216,6 +216,8 @@ namespace pgmpm {
 // Recompute the live MLS payload from the live state (after an upload, a
 // material change or a state restore).
 int refresh_payload(pgmpm_solver s, cudaStream_t st);
+// Allocate the bin sort's buffers (8 bytes per cell, counters cleared).
+int alloc_bin_sort(pgmpm_solver s);
 // Enqueue one step on `st` using buffers `b` (events ev[0..4] when timed).
 int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed);
 // Run n steps of the live state (graph, eager or profiled).

@@ -200,49 +200,77 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
 }
 
 // --------------------------------------------------- per-step bin sort
-// The MPM step groups particles by cell without a full radix sort: the key
-// is (cell tile << 6 | cell in tile), and both levels are counting sorts.
-//   bs_count     one pass over the keys: particles per cell tile (warp-
-//                aggregated atomics, match.any on the tile) and each
-//                particle's slot inside its tile.
+// The MPM step groups particles by cell with a counting sort over the cells
+// (key = cell tile << 6 | cell in tile) instead of a full radix sort:
+//   bs_count     particles per cell and per cell tile, and each particle's
+//                slot in its cell.  Lanes holding equal keys in a run (the
+//                physical order stays close to cell order) share one atomic:
+//                the run's first lane adds the run length.  8 keys per thread
+//                with their loads and atomics issued back to back.
 //   bs_reduce / bs_top / bs_down
-//                exclusive scan of the tile counts (reduce, scan of block
-//                sums, scan + offsets).  bs_down also emits every occupied
-//                tile: its sorted range, its entry in the occupied-tile list
-//                and the marks of the 8 node tiles it touches.
-//   bs_scatter   particle -> tile offset + slot (tile-grouped order).
-//   bs_cells     per occupied tile: 64-bin counting sort by cell into the
-//                final (key, particle) arrays, and every cell's range.
-// O(N + tiles) traffic.  Keys come out sorted; the order of particles that
-// share a cell depends on atomic arrival, which the step does not rely on.
+//                exclusive scan of the tile counts; bs_down also emits each
+//                occupied tile (sorted range, entry in the occupied-tile
+//                list) and clears the tile counters it read.
+//   bs_finish    (a) one warp per occupied tile: scan of its 64 cell counts
+//                -> every cell's first sorted position and range, clearing
+//                the cell counters it read; (b) one thread per node tile:
+//                active iff one of the 8 cell tiles around it is occupied.
+//   bs_scatter   particle -> cell offset + slot.
+// The counters are left zero for the next step by their readers, so a step
+// costs O(N + occupied cells + tiles) with no clearing pass.  Keys come out
+// sorted; particles that share a cell in atomic-arrival order, which the
+// step does not rely on.
 constexpr int BS_T = 256;
-constexpr int BS_SCAN = 1024;  // tile counts per scan block
+constexpr int BS_ITEMS = 8;                 // keys per thread in bs_count / bs_scatter
+constexpr int BS_TILE = BS_T * BS_ITEMS;    // keys per block
+constexpr int BS_SCAN = 1024;               // tile counts per scan block
 
-__global__ void __launch_bounds__(BS_T) bs_count(const uint32_t* __restrict__ keys, int64_t n, uint32_t total_ct,
-                                                 uint32_t* __restrict__ tcount, uint32_t* __restrict__ slot,
-                                                 uint32_t* __restrict__ counters) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t lt = (1u << lane) - 1u;
-    const int64_t stride = (int64_t)gridDim.x * BS_T;
-    uint32_t bad = 0;
-    // whole warps iterate together (match.any needs every lane)
-    for (int64_t base = (int64_t)blockIdx.x * BS_T + (threadIdx.x & ~31); base < n; base += stride) {
-        const int64_t i = base + lane;
-        const bool ok = i < n;
-        uint32_t t = 0xFFFFFFFFu;
-        if (ok) {
-            t = keys[i] >> 6;
-            if (t >= total_ct) {  // out-of-range key: overflow bin after the last tile
-                bad = 1;
-                t = total_ct;
-            }
+// Run structure of `bin` over a warp: first lane of this lane's run and one
+// past its last lane.  A run is a maximal stretch of consecutive lanes with
+// the same bin and the same ok.
+__device__ __forceinline__ void bs_run(uint32_t bin, bool ok, int lane, int& start, int& end) {
+    const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, bin, 1);
+    const uint32_t okp = __shfl_up_sync(0xFFFFFFFFu, (uint32_t)ok, 1);
+    const bool head = lane == 0 || bin != prev || (uint32_t)ok != okp;
+    const uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
+    const uint32_t upto = lane == 31 ? 0xFFFFFFFFu : ((2u << lane) - 1u);  // lanes <= this one
+    start = 31 - __clz(heads & upto);
+    const uint32_t after = heads & ~upto;
+    end = after ? __ffs(after) - 1 : 32;
+}
+
+__global__ void __launch_bounds__(BS_T) bs_count(const uint32_t* __restrict__ keys, int64_t n, uint32_t ncells,
+                                                 uint32_t* __restrict__ ccount, uint32_t* __restrict__ tcount,
+                                                 uint32_t* __restrict__ slot, uint32_t* __restrict__ counters) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * BS_TILE + warp * (32 * BS_ITEMS);
+    uint32_t k[BS_ITEMS], cb[BS_ITEMS];
+    int st[BS_ITEMS];
+    bool bad = false;
+#pragma unroll
+    for (int r = 0; r < BS_ITEMS; ++r) {
+        const int64_t i = base + r * 32 + lane;
+        k[r] = i < n ? keys[i] : 0u;
+        if (i < n && k[r] >= ncells) {  // out-of-range key: overflow bin after the last cell
+            bad = true;
+            k[r] = ncells;
         }
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, t);
-        const int leader = __ffs(peers) - 1;
-        uint32_t b = 0;
-        if (ok && lane == leader) b = atomicAdd(&tcount[t], (uint32_t)__popc(peers));
-        b = __shfl_sync(0xFFFFFFFFu, b, leader);
-        if (ok) slot[i] = b + (uint32_t)__popc(peers & lt);
+    }
+#pragma unroll
+    for (int r = 0; r < BS_ITEMS; ++r) {
+        const bool ok = base + r * 32 + lane < n;
+        int e, ts, te;
+        bs_run(k[r], ok, lane, st[r], e);
+        bs_run(k[r] >> 6, ok, lane, ts, te);
+        cb[r] = 0u;
+        if (ok && lane == st[r]) cb[r] = atomicAdd(&ccount[k[r]], (uint32_t)(e - st[r]));
+        if (ok && lane == ts) atomicAdd(&tcount[k[r] >> 6], (uint32_t)(te - ts));
+    }
+#pragma unroll
+    for (int r = 0; r < BS_ITEMS; ++r) {
+        const int64_t i = base + r * 32 + lane;
+        const uint32_t b = __shfl_sync(0xFFFFFFFFu, cb[r], st[r]);
+        if (i < n) slot[i] = b + (uint32_t)(lane - st[r]);
     }
     if (bad) atomicOr(&counters[CNT_FLAGS], FLAG_TILE_RANGE);
 }
@@ -269,103 +297,106 @@ __global__ void __launch_bounds__(BS_SCAN) bs_top(uint32_t* __restrict__ bsum, i
     }
 }
 
-__global__ void __launch_bounds__(BS_SCAN) bs_down(View V, const uint32_t* __restrict__ tcount, int64_t n,
-                                                   const uint32_t* __restrict__ bsum, uint32_t* __restrict__ toff) {
+// Warp-aggregated append of `item` (lanes with want) to list / counter.
+__device__ __forceinline__ void bs_append(uint32_t* list, uint32_t* counter, bool want, uint32_t item, int lane) {
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, want);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    uint32_t b = 0;
+    if (lane == leader) b = atomicAdd(counter, (uint32_t)__popc(m));
+    b = __shfl_sync(0xFFFFFFFFu, b, leader);
+    if (want) list[b + __popc(m & ((1u << lane) - 1u))] = item;
+}
+
+__global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict__ tcount, int64_t n,
+                                                   const uint32_t* __restrict__ bsum, uint32_t* __restrict__ toff,
+                                                   uint32_t* __restrict__ ccount_overflow) {
     __shared__ uint32_t sh[32];
+    const int lane = threadIdx.x & 31;
     const int64_t t = (int64_t)blockIdx.x * BS_SCAN + threadIdx.x;
     const uint32_t c = t < n ? tcount[t] : 0u;
     uint32_t tot;
     const uint32_t ex = block_excl_scan(c, sh, tot) + bsum[blockIdx.x];
-    if (t >= n) return;
-    toff[t] = ex;
-    if (c == 0 || t >= V.total_ct) return;  // empty, or the overflow bin
-    V.ctile_range[t] = make_uint2(ex, ex + c);
-    V.ctile_list[atomicAdd(&V.counters[CNT_CTILES], 1u)] = (uint32_t)t;
-    const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)t);
-    const SceneDev& sc = V.scenes[s];
-    const int lt = (int)t - sc.ct_base;
-    const int tx = lt % sc.ct[0], ty = (lt / sc.ct[0]) % sc.ct[1], tz = lt / (sc.ct[0] * sc.ct[1]);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int nx = tx + (k & 1), ny = ty + ((k >> 1) & 1), nz = tz + (k >> 2);
-        const uint32_t nt = (uint32_t)(sc.nt_base + (nz * sc.nt[1] + ny) * sc.nt[0] + nx);
-        if (atomicExch(&V.tile_flags[nt], 1u) == 0u) V.tile_list[atomicAdd(&V.counters[CNT_TILES], 1u)] = nt;
+    if (t < n) {
+        toff[t] = ex;
+        tcount[t] = 0u;  // left clear for the next step
     }
+    if (t == n - 1) *ccount_overflow = 0u;
+    const bool occ = t < (int64_t)V.total_ct && c > 0u;  // not the overflow bin
+    if (occ) V.ctile_range[t] = make_uint2(ex, ex + c);
+    bs_append(V.ctile_list, &V.counters[CNT_CTILES], occ, (uint32_t)t, lane);
 }
 
-__global__ void __launch_bounds__(BS_T) bs_scatter(const uint32_t* __restrict__ keys, int64_t n, uint32_t total_ct,
-                                                   const uint32_t* __restrict__ slot,
-                                                   const uint32_t* __restrict__ toff, uint32_t* __restrict__ tk,
-                                                   uint32_t* __restrict__ tv) {
-    const int64_t stride = (int64_t)gridDim.x * BS_T;
-    for (int64_t i = (int64_t)blockIdx.x * BS_T + threadIdx.x; i < n; i += stride) {
-        const uint32_t key = keys[i];
-        const uint32_t t = min(key >> 6, total_ct);
-        const uint32_t pos = toff[t] + slot[i];
-        if ((int64_t)pos < n) {
-            tk[pos] = key;
-            tv[pos] = (uint32_t)i;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(BS_T) bs_cells(View V, const uint32_t* __restrict__ tk,
-                                                 const uint32_t* __restrict__ tv, uint32_t* __restrict__ ok_,
-                                                 uint32_t* __restrict__ ov, uint2* __restrict__ cell_range) {
-    __shared__ uint32_t s_cnt[64];
-    __shared__ uint32_t s_off[64];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t ntiles = V.counters[CNT_CTILES];
-    for (uint32_t w = blockIdx.x; w < ntiles; w += gridDim.x) {
-        const uint32_t ct = V.ctile_list[w];
-        const uint2 rg = V.ctile_range[ct];
-        if (threadIdx.x < 64) s_cnt[threadIdx.x] = 0u;
-        __syncthreads();
-        for (uint32_t b = rg.x + warp * 32; b < rg.y; b += BS_T) {
-            const uint32_t i = b + lane;
-            const bool ok = i < rg.y;
-            const uint32_t c = ok ? (tk[i] & 63u) : 64u + lane;
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, c);
-            if (ok && lane == __ffs(peers) - 1) atomicAdd(&s_cnt[c], (uint32_t)__popc(peers));
-        }
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t a = s_cnt[2 * lane], b = s_cnt[2 * lane + 1];
-            uint32_t x = a + b;
+// Blocks [0, cell_blocks): (a), the rest: (b).  See the overview above.
+__global__ void __launch_bounds__(BS_T) bs_finish(View V, uint32_t* __restrict__ ccount,
+                                                  const uint32_t* __restrict__ toff, uint32_t* __restrict__ coff,
+                                                  uint2* __restrict__ cell_range, int cell_blocks) {
+    const int lane = threadIdx.x & 31;
+    if ((int)blockIdx.x < cell_blocks) {
+        const uint32_t ntiles = V.counters[CNT_CTILES];
+        const uint32_t nwarps = (uint32_t)cell_blocks * (BS_T / 32);
+        for (uint32_t w = (blockIdx.x * BS_T + threadIdx.x) >> 5; w < ntiles; w += nwarps) {
+            const uint32_t t = V.ctile_list[w];
+            uint2* cc2 = reinterpret_cast<uint2*>(ccount + (size_t)t * 64) + lane;
+            const uint2 cc = *cc2;
+            *cc2 = make_uint2(0u, 0u);  // left clear for the next step
+            uint32_t x = cc.x + cc.y;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
                 if (lane >= o) x += y;
             }
-            const uint32_t e = x - a - b;  // exclusive prefix of cell 2*lane
-            s_off[2 * lane] = e;
-            s_off[2 * lane + 1] = e + a;
+            const uint32_t e = toff[t] + x - cc.x - cc.y;  // first position of cell 2*lane
+            reinterpret_cast<uint2*>(coff + (size_t)t * 64)[lane] = make_uint2(e, e + cc.x);
             if (cell_range) {
-                cell_range[(size_t)ct * 64 + 2 * lane] = make_uint2(rg.x + e, rg.x + e + a);
-                cell_range[(size_t)ct * 64 + 2 * lane + 1] = make_uint2(rg.x + e + a, rg.x + e + a + b);
+                cell_range[(size_t)t * 64 + 2 * lane] = make_uint2(e, e + cc.x);
+                cell_range[(size_t)t * 64 + 2 * lane + 1] = make_uint2(e + cc.x, e + cc.x + cc.y);
             }
         }
-        __syncthreads();
-        for (uint32_t b = rg.x + warp * 32; b < rg.y; b += BS_T) {
-            const uint32_t i = b + lane;
-            const bool ok = i < rg.y;
-            const uint32_t key = ok ? tk[i] : 0u;
-            const uint32_t c = ok ? (key & 63u) : 64u + lane;
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, c);
-            const int leader = __ffs(peers) - 1;
-            uint32_t base = 0;
-            if (ok && lane == leader) base = atomicAdd(&s_off[c], (uint32_t)__popc(peers));
-            base = __shfl_sync(0xFFFFFFFFu, base, leader);
-            if (ok) {
-                const uint32_t pos = rg.x + base + (uint32_t)__popc(peers & lt);
-                if (pos < rg.y) {
-                    ok_[pos] = key;
-                    ov[pos] = tv[i];
-                }
-            }
+        return;
+    }
+    const int64_t nt = (int64_t)(blockIdx.x - cell_blocks) * BS_T + threadIdx.x;
+    bool act = false;
+    if (nt < V.total_nt) {
+        const int s = V.S == 1 ? 0 : scene_of_node_tile(V.scenes, V.S, (int)nt);
+        const SceneDev& sc = V.scenes[s];
+        const int l = (int)nt - sc.nt_base;
+        const int x = l % sc.nt[0], y = (l / sc.nt[0]) % sc.nt[1], z = l / (sc.nt[0] * sc.nt[1]);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int cx = x - (k & 1), cy = y - ((k >> 1) & 1), cz = z - (k >> 2);
+            if (cx < 0 || cy < 0 || cz < 0 || cx >= sc.ct[0] || cy >= sc.ct[1] || cz >= sc.ct[2]) continue;
+            const int ct = sc.ct_base + (cz * sc.ct[1] + cy) * sc.ct[0] + cx;
+            act |= toff[ct + 1] > toff[ct];
         }
-        __syncthreads();
+        V.tile_flags[nt] = act ? 1u : 0u;
+    }
+    bs_append(V.tile_list, &V.counters[CNT_TILES], act, (uint32_t)nt, lane);
+}
+
+__global__ void __launch_bounds__(BS_T) bs_scatter(const uint32_t* __restrict__ keys, int64_t n, uint32_t ncells,
+                                                   const uint32_t* __restrict__ slot,
+                                                   const uint32_t* __restrict__ coff,
+                                                   const uint32_t* __restrict__ toff_overflow,
+                                                   uint32_t* __restrict__ ok_, uint32_t* __restrict__ ov) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * BS_TILE + warp * (32 * BS_ITEMS);
+    uint32_t k[BS_ITEMS], sl[BS_ITEMS], pos[BS_ITEMS];
+#pragma unroll
+    for (int r = 0; r < BS_ITEMS; ++r) {
+        const int64_t i = base + r * 32 + lane;
+        k[r] = i < n ? keys[i] : 0u;
+        sl[r] = i < n ? slot[i] : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < BS_ITEMS; ++r) pos[r] = (k[r] < ncells ? coff[k[r]] : *toff_overflow) + sl[r];
+#pragma unroll
+    for (int r = 0; r < BS_ITEMS; ++r) {
+        const int64_t i = base + r * 32 + lane;
+        if (i < n && (int64_t)pos[r] < n) {
+            ok_[pos[r]] = k[r];
+            ov[pos[r]] = (uint32_t)i;
+        }
     }
 }
 }  // namespace
@@ -375,18 +406,18 @@ int64_t bin_sort_scan_blocks(int total_ct) { return ((int64_t)total_ct + 1 + BS_
 cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cudaStream_t st) {
     const int64_t n = V.N;
     if (n <= 0) return cudaSuccess;
-    const int64_t nbins = (int64_t)V.total_ct + 1;  // + overflow bin
+    const uint32_t ncells = (uint32_t)V.total_ct * 64u;
+    const int64_t ntb = (int64_t)V.total_ct + 1;  // tiles + overflow bin
     const int nb = (int)bin_sort_scan_blocks(V.total_ct);
-    cudaError_t e = cudaMemsetAsync(B.tcount, 0, sizeof(uint32_t) * nbins, st);
-    if (e != cudaSuccess) return e;
-    const int64_t g64 = (n + BS_T - 1) / BS_T;
-    const int g = (int)(g64 < (int64_t)num_sms * 8 ? g64 : (int64_t)num_sms * 8);
-    bs_count<<<g, BS_T, 0, st>>>(B.keys_in, n, (uint32_t)V.total_ct, B.tcount, B.slot, V.counters);
-    bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, nbins, B.bsum);
+    const int gk = (int)((n + BS_TILE - 1) / BS_TILE);
+    bs_count<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.ccount, B.tcount, B.slot, V.counters);
+    bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, ntb, B.bsum);
     bs_top<<<1, BS_SCAN, 0, st>>>(B.bsum, nb);
-    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, nbins, B.bsum, B.toff);
-    bs_scatter<<<g, BS_T, 0, st>>>(B.keys_in, n, (uint32_t)V.total_ct, B.slot, B.toff, B.tmp_k, B.tmp_v);
-    bs_cells<<<num_sms * 8, BS_T, 0, st>>>(V, B.tmp_k, B.tmp_v, B.out_k, B.out_v, B.cell_range);
+    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, B.bsum, B.toff, B.ccount + ncells);
+    const int cell_blocks = num_sms * 2;
+    const int node_blocks = (V.total_nt + BS_T - 1) / BS_T;
+    bs_finish<<<cell_blocks + node_blocks, BS_T, 0, st>>>(V, B.ccount, B.toff, B.coff, B.cell_range, cell_blocks);
+    bs_scatter<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.slot, B.coff, B.toff + V.total_ct, B.out_k, B.out_v);
     return cudaGetLastError();
 }
 
