@@ -80,6 +80,8 @@ int alloc_bin_sort(pgmpm_solver s) {
     CK(s->bs_bsum.alloc(sizeof(uint32_t) * (size_t)bin_sort_scan_blocks((int)ct)));
     CK(s->bs_slot.alloc(sizeof(uint32_t) * (size_t)std::max<int64_t>(s->N, 1)));
     CK(s->cell_range.alloc(sizeof(uint2) * 64 * std::max<size_t>(ct, 1)));
+    CK(s->ptile_list.alloc(sizeof(uint32_t) * std::max<size_t>(ct, 1)));
+    CK(s->tile_rank.alloc(sizeof(uint32_t) * std::max<size_t>(ct, 1)));
     // the counters start at zero and every sort leaves them zero
     CK(cudaMemset(s->bs_ccount.p, 0, s->bs_ccount.bytes));
     CK(cudaMemset(s->bs_tcount.p, 0, s->bs_tcount.bytes));
@@ -116,6 +118,8 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) 
         B.out_k = b.which ? b.kb : b.ka;  // where the step's readers look (View::skeys / order)
         B.out_v = b.which ? b.vb : b.va;
         B.cell_range = b.cell_range;
+        B.ptile_list = b.ptile_list;
+        B.tile_rank = s->tile_rank.as<uint32_t>();
         CK(bin_sort_step(V, B, s->num_sms, st));
     } else {
         int which = 0;

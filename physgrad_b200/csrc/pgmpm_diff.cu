@@ -78,6 +78,7 @@ StepBufs tape_bufs(pgmpm_solver s, int j) {
     b.ctile_list = s->tape_ctiles.as<uint32_t>() + (size_t)s->total_ct * j;
     b.ctile_range = s->tape_crange.as<uint2>() + (size_t)s->total_ct * j;
     b.cell_range = nullptr;  // replayed steps keep no cell table: P2G searches the sorted keys
+    b.ptile_list = nullptr;
     b.counters = s->tape_counters.as<uint32_t>() + CNT_WORDS * j;
     return b;
 }

@@ -9,19 +9,23 @@
 namespace pgmpm {
 
 // counters[] layout.  Words [0, CNT_RESET) are cleared every step:
-// active node tiles, occupied cell tiles, active node count (u64), and the
-// work cursors of the tile kernels.  CNT_FLAGS (sticky error flags) is
-// cleared only by pgmpm_check_status.
+// active node tiles, occupied cell tiles, active node count (u64), the
+// work cursors of the tile kernels, and the occupied cell tiles per size
+// class (CNT_BUCKETS classes, largest first).  CNT_FLAGS (sticky error
+// flags) is cleared only by pgmpm_check_status.
+constexpr int CNT_BUCKETS = 8;
 enum {
     CNT_TILES = 0,
     CNT_CTILES = 1,
     CNT_ACTIVE = 2,
     CNT_P2G_CURSOR = 4,
     CNT_G2P_CURSOR = 5,
-    CNT_RESET = 6,
-    CNT_FLAGS = 6,
-    CNT_WORDS = 8
+    CNT_BUCKET = 6,
+    CNT_RESET = CNT_BUCKET + CNT_BUCKETS,
+    CNT_FLAGS = CNT_RESET,
+    CNT_WORDS = 16
 };
+static_assert(CNT_FLAGS < CNT_WORDS, "counter layout");
 
 // Everything a step kernel needs, passed by value.
 struct View {
@@ -44,6 +48,7 @@ struct View {
     uint32_t* tile_flags;      // node tile active flags (per global node tile)
     uint32_t* tile_list;       // active node tiles
     uint32_t* ctile_list;      // occupied cell tiles (global cell tile ids)
+    const uint32_t* ptile_list;  // the same tiles, largest first (null: use ctile_list)
     uint2* ctile_range;        // per global cell tile: [begin, end) in sorted order
     const uint2* cell_range;   // per global cell: [begin, end) in sorted order (null: search skeys)
     uint32_t* counters;        // see CNT_*
@@ -96,6 +101,8 @@ struct BinSortBufs {
     uint32_t* slot;        // N words
     uint32_t *out_k, *out_v;  // N words each
     uint2* cell_range;     // total_ct * 64, or null
+    uint32_t* ptile_list;  // total_ct: occupied tiles by size class, largest first (null: not built)
+    uint32_t* tile_rank;   // total_ct: class and rank of each ctile_list entry (scratch, with ptile_list)
 };
 int64_t bin_sort_scan_blocks(int total_ct);
 cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cudaStream_t st);

@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V, AdjView AV) {
         __syncthreads();
         const uint32_t w = s_work;
         if (w >= ntiles) break;
-        const uint32_t ct = V.ctile_list[w];
+        const uint32_t ct = V.ptile_list ? V.ptile_list[w] : V.ctile_list[w];  // largest tiles first
         const uint2 rg = V.ctile_range[ct];
         const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
         const SceneDev& sc = scene_ref(V, s);
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
         __syncthreads();
         const uint32_t w = s_work;
         if (w >= ntiles) break;
-        const uint32_t ct = V.ctile_list[w];
+        const uint32_t ct = V.ptile_list ? V.ptile_list[w] : V.ctile_list[w];  // largest tiles first
         const uint2 rg = V.ctile_range[ct];
         const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
         const SceneDev& sc = scene_ref(V, s);

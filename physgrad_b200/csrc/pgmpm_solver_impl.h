@@ -70,6 +70,7 @@ struct StepBufs {
     uint32_t* ctile_list;
     uint2* ctile_range;
     uint2* cell_range;     // per-cell ranges written by the bin sort (null: not kept)
+    uint32_t* ptile_list;  // occupied tiles largest first, built by the bin sort (null: not kept)
     uint32_t* counters;
 };
 
@@ -114,6 +115,7 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf d_scenes, d_mats, q, pay, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
     pgmpm::DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
     pgmpm::DevBuf bs_ccount, bs_coff, bs_tcount, bs_toff, bs_bsum, bs_slot, cell_range;  // per-step bin sort
+    pgmpm::DevBuf ptile_list, tile_rank;  // largest-first occupied tile list (bin sort)
     uint32_t* h_counters = nullptr;  // pinned
 
     // graph
@@ -156,6 +158,7 @@ struct pgmpm_solver_s {
         b.ctile_list = ctile_list.as<uint32_t>();
         b.ctile_range = ctile_range.as<uint2>();
         b.cell_range = cell_range.as<uint2>();
+        b.ptile_list = ptile_list.as<uint32_t>();
         b.counters = counters.as<uint32_t>();
         return b;
     }
@@ -184,6 +187,7 @@ struct pgmpm_solver_s {
         V.ctile_list = b.ctile_list;
         V.ctile_range = b.ctile_range;
         V.cell_range = tune.step_sort == 0 ? b.cell_range : nullptr;
+        V.ptile_list = tune.step_sort == 0 ? b.ptile_list : nullptr;
         V.counters = b.counters;
         V.total_ct = total_ct;
         V.total_nt = total_nt;

@@ -210,10 +210,14 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
 //   bs_reduce / bs_top / bs_down
 //                exclusive scan of the tile counts; bs_down also emits each
 //                occupied tile (sorted range, entry in the occupied-tile
-//                list) and clears the tile counters it read.
+//                list, rank in its size class) and clears the tile counters
+//                it read.
 //   bs_finish    (a) one warp per occupied tile: scan of its 64 cell counts
 //                -> every cell's first sorted position and range, clearing
-//                the cell counters it read; (b) one thread per node tile:
+//                the cell counters it read, and the tile's slot in the
+//                largest-first list P2G takes work from (the last tiles a
+//                persistent P2G block picks up are then small ones, which
+//                shortens the kernel's tail); (b) one thread per node tile:
 //                active iff one of the 8 cell tiles around it is occupied.
 //   bs_scatter   particle -> cell offset + slot.
 // The counters are left zero for the next step by their readers, so a step
@@ -297,20 +301,32 @@ __global__ void __launch_bounds__(BS_SCAN) bs_top(uint32_t* __restrict__ bsum, i
     }
 }
 
-// Warp-aggregated append of `item` (lanes with want) to list / counter.
-__device__ __forceinline__ void bs_append(uint32_t* list, uint32_t* counter, bool want, uint32_t item, int lane) {
+// Warp-aggregated append of `item` (lanes with want) to list / counter;
+// returns the slot written (meaningful where want).
+__device__ __forceinline__ uint32_t bs_append(uint32_t* list, uint32_t* counter, bool want, uint32_t item,
+                                              int lane) {
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, want);
-    if (!m) return;
+    if (!m) return 0u;
     const int leader = __ffs(m) - 1;
     uint32_t b = 0;
     if (lane == leader) b = atomicAdd(counter, (uint32_t)__popc(m));
     b = __shfl_sync(0xFFFFFFFFu, b, leader);
-    if (want) list[b + __popc(m & ((1u << lane) - 1u))] = item;
+    const uint32_t slot = b + __popc(m & ((1u << lane) - 1u));
+    if (want) list[slot] = item;
+    return slot;
+}
+
+// Size class of an occupied tile, 0 = largest (>= 1024 particles) ...
+// CNT_BUCKETS - 1 = smallest (< 16).
+__device__ __forceinline__ int bs_class(uint32_t count) {
+    const int lg = 31 - __clz(count);  // count >= 1
+    return min(CNT_BUCKETS - 1, max(0, 10 - lg));
 }
 
 __global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict__ tcount, int64_t n,
                                                    const uint32_t* __restrict__ bsum, uint32_t* __restrict__ toff,
-                                                   uint32_t* __restrict__ ccount_overflow) {
+                                                   uint32_t* __restrict__ ccount_overflow,
+                                                   uint32_t* __restrict__ tile_rank) {
     __shared__ uint32_t sh[32];
     const int lane = threadIdx.x & 31;
     const int64_t t = (int64_t)blockIdx.x * BS_SCAN + threadIdx.x;
@@ -324,19 +340,47 @@ __global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict_
     if (t == n - 1) *ccount_overflow = 0u;
     const bool occ = t < (int64_t)V.total_ct && c > 0u;  // not the overflow bin
     if (occ) V.ctile_range[t] = make_uint2(ex, ex + c);
-    bs_append(V.ctile_list, &V.counters[CNT_CTILES], occ, (uint32_t)t, lane);
+    const uint32_t w = bs_append(V.ctile_list, &V.counters[CNT_CTILES], occ, (uint32_t)t, lane);
+    if (tile_rank) {
+        // rank inside the tile's size class (lanes of one class share an atomic)
+        const uint32_t cls = occ ? (uint32_t)bs_class(c) : (uint32_t)(CNT_BUCKETS + lane);
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, cls);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (occ && lane == leader) b = atomicAdd(&V.counters[CNT_BUCKET + cls], (uint32_t)__popc(peers));
+        b = __shfl_sync(0xFFFFFFFFu, b, leader);
+        if (occ) tile_rank[w] = (cls << 28) | (b + (uint32_t)__popc(peers & ((1u << lane) - 1u)));
+    }
 }
 
 // Blocks [0, cell_blocks): (a), the rest: (b).  See the overview above.
 __global__ void __launch_bounds__(BS_T) bs_finish(View V, uint32_t* __restrict__ ccount,
                                                   const uint32_t* __restrict__ toff, uint32_t* __restrict__ coff,
-                                                  uint2* __restrict__ cell_range, int cell_blocks) {
+                                                  uint2* __restrict__ cell_range, const uint32_t* __restrict__ tile_rank,
+                                                  uint32_t* __restrict__ ptile_list, int cell_blocks) {
     const int lane = threadIdx.x & 31;
     if ((int)blockIdx.x < cell_blocks) {
         const uint32_t ntiles = V.counters[CNT_CTILES];
         const uint32_t nwarps = (uint32_t)cell_blocks * (BS_T / 32);
+        // first slot of each size class in the largest-first list
+        uint32_t cls_off = 0u;
+        if (ptile_list) {
+            const uint32_t cnt = lane < CNT_BUCKETS ? V.counters[CNT_BUCKET + lane] : 0u;
+            uint32_t x = cnt;
+#pragma unroll
+            for (int o = 1; o < CNT_BUCKETS; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= o) x += y;
+            }
+            cls_off = x - cnt;
+        }
         for (uint32_t w = (blockIdx.x * BS_T + threadIdx.x) >> 5; w < ntiles; w += nwarps) {
             const uint32_t t = V.ctile_list[w];
+            if (ptile_list) {
+                const uint32_t tr = tile_rank[w];
+                const uint32_t off = __shfl_sync(0xFFFFFFFFu, cls_off, (int)(tr >> 28));
+                if (lane == 0) ptile_list[off + (tr & 0x0FFFFFFFu)] = t;
+            }
             uint2* cc2 = reinterpret_cast<uint2*>(ccount + (size_t)t * 64) + lane;
             const uint2 cc = *cc2;
             *cc2 = make_uint2(0u, 0u);  // left clear for the next step
@@ -413,10 +457,12 @@ cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cuda
     bs_count<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.ccount, B.tcount, B.slot, V.counters);
     bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, ntb, B.bsum);
     bs_top<<<1, BS_SCAN, 0, st>>>(B.bsum, nb);
-    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, B.bsum, B.toff, B.ccount + ncells);
+    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, B.bsum, B.toff, B.ccount + ncells,
+                                    B.ptile_list ? B.tile_rank : nullptr);
     const int cell_blocks = num_sms * 2;
     const int node_blocks = (V.total_nt + BS_T - 1) / BS_T;
-    bs_finish<<<cell_blocks + node_blocks, BS_T, 0, st>>>(V, B.ccount, B.toff, B.coff, B.cell_range, cell_blocks);
+    bs_finish<<<cell_blocks + node_blocks, BS_T, 0, st>>>(V, B.ccount, B.toff, B.coff, B.cell_range, B.tile_rank,
+                                                           B.ptile_list, cell_blocks);
     bs_scatter<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.slot, B.coff, B.toff + V.total_ct, B.out_k, B.out_v);
     return cudaGetLastError();
 }
