@@ -3,12 +3,15 @@
 // launcher launch_mpm_timestep_forward.
 //
 // Forward: the state (6 planes + keys) is copied to a checkpoint every k
-// steps (CheckpointStrategy::UNIFORM of src/differentiable_mpm.h:66).
-// Backward, segment by segment from the last: the segment is replayed from
-// its checkpoint into per-step tape slots (state j and j+1, keys, the sort's
-// order, tile lists, grid v and v before the walls) using the same step
-// kernels pointed at the tape, then the three reverse kernels run for each
-// step from the last to the first.  Tape depth = k steps.
+// steps (CheckpointStrategy::UNIFORM of src/differentiable_mpm.h:66); the
+// last segment runs straight into the tape.  Backward, segment by segment
+// from the last: the segment is replayed from its checkpoint into per-step
+// tape slots (state j and j+1, keys, the sort's order, tile lists, cell
+// ranges, grid v and v before the walls) using the same step kernels pointed
+// at the tape -- skipped for the segment the forward left in the tape --
+// then the three reverse kernels run for each step from the last to the
+// first.  Tape depth = k steps.  Each segment's work is one CUDA graph
+// (captured once per segment length; the checkpoint copies stay outside).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,6 +33,8 @@ int ensure_tape(pgmpm_solver s, int slots) {
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
     const size_t nodes = nodes_of(s);
     s->tape_slots = 0;
+    s->tape_has_last = false;
+    s->drop_tape_graphs();  // they hold the old tape's addresses
     CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1)));
     CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1)));
     if (s->pf.physics == PHYS_MLS) CK(s->tape_pay.alloc(sizeof(float4) * 4 * N));
@@ -42,6 +47,11 @@ int ensure_tape(pgmpm_solver s, int slots) {
     CK(s->tape_ctiles.alloc(sizeof(uint32_t) * (size_t)s->total_ct * slots));
     CK(s->tape_crange.alloc(sizeof(uint2) * (size_t)s->total_ct * slots));
     CK(s->tape_counters.alloc(sizeof(uint32_t) * CNT_WORDS * slots));
+    CK(cudaMemset(s->tape_counters.p, 0, s->tape_counters.bytes));
+    if (s->bs_ccount.p) {  // the bin sort is available: per-slot cell tables
+        CK(s->tape_cells.alloc(sizeof(uint2) * 64 * std::max<size_t>((size_t)s->total_ct, 1) * slots));
+        CK(s->tape_ptile.alloc(sizeof(uint32_t) * std::max<size_t>((size_t)s->total_ct, 1) * slots));
+    }
     s->tape_slots = slots;
     return PGMPM_OK;
 }
@@ -77,10 +87,60 @@ StepBufs tape_bufs(pgmpm_solver s, int j) {
     b.tile_list = s->tape_tiles.as<uint32_t>() + (size_t)s->total_nt * j;
     b.ctile_list = s->tape_ctiles.as<uint32_t>() + (size_t)s->total_ct * j;
     b.ctile_range = s->tape_crange.as<uint2>() + (size_t)s->total_ct * j;
-    b.cell_range = nullptr;  // replayed steps keep no cell table: P2G searches the sorted keys
-    b.ptile_list = nullptr;
+    const size_t ct = std::max<size_t>((size_t)s->total_ct, 1);
+    b.cell_range = s->tape_cells.p ? s->tape_cells.as<uint2>() + ct * 64 * j : nullptr;
+    b.ptile_list = s->tape_ptile.p ? s->tape_ptile.as<uint32_t>() + ct * j : nullptr;
     b.counters = s->tape_counters.as<uint32_t>() + CNT_WORDS * j;
     return b;
+}
+
+// Runs body(stream) under capture on the solver's capture stream and keeps
+// the instantiated graph in tape_exec[kind] (tagged with len).
+template <class Body>
+int tape_graph(pgmpm_solver s, int kind, int len, Body&& body) {
+    if (s->tape_exec[kind] && s->tape_exec_len[kind] == len) return PGMPM_OK;
+    if (s->tape_exec[kind]) cudaGraphExecDestroy(s->tape_exec[kind]);
+    s->tape_exec[kind] = nullptr;
+    s->tape_exec_len[kind] = -1;
+    CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = body(s->cap_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
+    if (rc != PGMPM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    CK(e);
+    e = cudaGraphInstantiate(&s->tape_exec[kind], g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    s->tape_exec_len[kind] = len;
+    return PGMPM_OK;
+}
+
+// Forward of tape slots 0..len-1 (state 0 and its payload already in place).
+int record_tape_forward(pgmpm_solver s, int len, cudaStream_t st) {
+    for (int j = 0; j < len; ++j) {
+        int rc = record_step(s, tape_bufs(s, j), st, false);
+        if (rc) return rc;
+    }
+    return PGMPM_OK;
+}
+
+// Reverse kernels of tape slots len-1 .. 0.
+int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t st) {
+    AdjView A = A0;
+    for (int j = len - 1; j >= 0; --j) {
+        StepBufs b = tape_bufs(s, j);
+        View V = s->view_for(b);
+        V.grid_mp = A.grid_gv;  // scatter target of the G2P reverse
+        A.q_next = b.q_out;
+        CK(cudaMemsetAsync(b.counters + CNT_P2G_CURSOR, 0, sizeof(uint32_t), st));
+        CK(launch_adj_scatter(V, A, s->pf, s->tune, s->num_sms, st));
+        CK(launch_adj_grid(V, A, s->tune, s->num_sms, st));
+        CK(launch_adj_gather(V, A, s->pf, s->tune, st));
+    }
+    return PGMPM_OK;
 }
 
 }  // namespace
@@ -98,15 +158,42 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
     CK(s->ck_q.ensure(sizeof(float4) * 6 * N * nseg));
     CK(s->ck_keys.ensure(sizeof(uint32_t) * N * nseg));
+    int rc = ensure_tape(s, k);
+    if (rc) return rc;
     s->ck_valid = false;
+    s->tape_has_last = false;
     for (int seg = 0; seg < nseg; ++seg) {
         CK(cudaMemcpyAsync(s->ck_q.as<float4>() + 6 * N * seg, s->q.p, sizeof(float4) * 6 * N,
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->ck_keys.as<uint32_t>() + N * seg, s->keys.p, sizeof(uint32_t) * N,
                            cudaMemcpyDeviceToDevice, st));
         const int len = std::min(k, n_steps - seg * k);
-        int rc = run_steps(s, len, st);
+        if (seg + 1 < nseg || s->N == 0) {
+            rc = run_steps(s, len, st);
+            if (rc) return rc;
+            continue;
+        }
+        // last segment: run it in the tape slots, so that the backward does
+        // not replay it, then hand the final state back to the live buffers
+        CK(cudaMemcpyAsync(s->tape_q.p, s->q.p, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->tape_keys.p, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->tape_pay.p, s->pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
+        rc = tape_graph(s, 1, len, [&](cudaStream_t cs) { return record_tape_forward(s, len, cs); });
         if (rc) return rc;
+        CK(cudaGraphLaunch(s->tape_exec[1], st));
+        const StepBufs last = tape_bufs(s, len - 1);
+        CK(cudaMemcpyAsync(s->q.p, last.q_out, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->keys.p, last.keys_out, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->pay.p, s->tape_pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
+        // what a live step leaves for pgmpm_download_grid and the metrics
+        CK(cudaMemcpyAsync(s->grid_v.p, last.grid_v, sizeof(float4) * nodes_of(s), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->tile_flags.p, last.tile_flags, sizeof(uint32_t) * (size_t)s->total_nt,
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->counters.as<uint32_t>() + CNT_ACTIVE, last.counters + CNT_ACTIVE, 2 * sizeof(uint32_t),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), len, s->counters.as<uint32_t>(), st));
+        s->met.total_steps += len;
+        s->tape_has_last = true;
     }
     s->ck_steps = n_steps;
     s->ck_every = k;
@@ -157,26 +244,29 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
     const int k = s->ck_every;
     for (int seg = s->ck_count - 1; seg >= 0 && N > 0; --seg) {
         const int len = std::min(k, s->ck_steps - seg * k);
+        if (seg == s->ck_count - 1 && s->tape_has_last) {
+            // the forward left this segment in the tape
+            rc = tape_graph(s, 2, len, [&](cudaStream_t cs) { return record_tape_reverse(s, A, len, cs); });
+            if (rc) return rc;
+            CK(cudaGraphLaunch(s->tape_exec[2], st));
+            s->tape_has_last = false;  // the replays below overwrite it
+            continue;
+        }
+        s->tape_has_last = false;
         CK(cudaMemcpyAsync(s->tape_q.p, s->ck_q.as<float4>() + 6 * Nz * seg, sizeof(float4) * 6 * Nz,
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_keys.p, s->ck_keys.as<uint32_t>() + Nz * seg, sizeof(uint32_t) * Nz,
                            cudaMemcpyDeviceToDevice, st));
-        CK(launch_payload(s->view_for(tape_bufs(s, 0)), s->pf, st));
-        for (int j = 0; j < len; ++j) {
-            rc = record_step(s, tape_bufs(s, j), st, false);
-            if (rc) return rc;
-        }
-        for (int j = len - 1; j >= 0; --j) {
-            StepBufs b = tape_bufs(s, j);
-            View V = s->view_for(b);
-            V.grid_mp = A.grid_gv;  // scatter target of the G2P reverse
-            A.q_next = b.q_out;
-            CK(cudaMemsetAsync(b.counters + CNT_P2G_CURSOR, 0, sizeof(uint32_t), st));
-            CK(launch_adj_scatter(V, A, s->pf, s->tune, s->num_sms, st));
-            CK(launch_adj_grid(V, A, s->tune, s->num_sms, st));
-            CK(launch_adj_gather(V, A, s->pf, s->tune, st));
-        }
+        rc = tape_graph(s, 0, len, [&](cudaStream_t cs) -> int {
+            CK(launch_payload(s->view_for(tape_bufs(s, 0)), s->pf, cs));
+            int r = record_tape_forward(s, len, cs);
+            if (r) return r;
+            return record_tape_reverse(s, A, len, cs);
+        });
+        if (rc) return rc;
+        CK(cudaGraphLaunch(s->tape_exec[0], st));
     }
+    CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), s->tape_slots, s->counters.as<uint32_t>(), st));
     // physical planes -> caller's arrays (upload order)
     if (ptr_kind == PGMPM_PTR_DEVICE) {
         CK(launch_planes_to_state(A.g, s->user_of_phys.as<uint32_t>(), gx_in, gv_in, gC_in, gF_in, N, st));

@@ -124,6 +124,9 @@ cudaError_t launch_pack(const View& V, const float* x, const float* v, const flo
                         uint32_t* user_of_phys, float2* mV_out, int32_t* mat_out, cudaStream_t st);
 cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x, float* v, float* C, float* F,
                           cudaStream_t st);
+// ORs the error flags of `slots` counter blocks (stride CNT_WORDS) into
+// live[CNT_FLAGS] and clears them.
+cudaError_t launch_merge_flags(uint32_t* slots_counters, int slots, uint32_t* live, cudaStream_t st);
 cudaError_t launch_grid_download(const View& V, int scene, const SceneDev& sc, float* mass, float* vel,
                                  cudaStream_t st);
 

@@ -567,10 +567,10 @@ __device__ __forceinline__ void adj_payload(const View& V, const AdjView& AV, co
 // ------------------------------------------------ P2G, one thread per cell
 // Variant 2: one 64-thread block per occupied cell tile, thread c owns cell
 // c and all 27 nodes of its stencil (108 register accumulators).  The
-// thread walks its cell's particles (sorted, contiguous), computes each
-// particle's stress / affine payload itself and accumulates: no shared
-// payload staging and no barriers until the flush.  The flush is the same
-// shared-memory transpose + one vector atomic per tile node.
+// thread walks its cell's particles (sorted, contiguous) and accumulates
+// their payloads (precomputed by G2P for MLS; computed here from the state
+// for REF and the adjoint): no shared payload staging and no barriers until
+// the flush, a shared-memory transpose + one vector atomic per tile node.
 constexpr int P2GC_T = 64;
 
 template <int MODE, bool MULTI, bool FLUID>
@@ -582,12 +582,18 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
     const int64_t N = V.N;
     uint32_t flags = 0;
     const uint32_t ntiles = V.counters[CNT_CTILES];
+    // Few occupied tiles (a small, dense scene) leave most blocks idle: then
+    // each cell's run is split into S interleaved slices, one work item per
+    // (tile, slice), each flushing its own partial sums.
+    const uint32_t S = ntiles ? min(8u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
+    const uint32_t nwork = ntiles * S;
     for (;;) {
         if (c == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
         __syncthreads();
         const uint32_t w = s_work;
-        if (w >= ntiles) break;
-        const uint32_t ct = V.ptile_list ? V.ptile_list[w] : V.ctile_list[w];  // largest tiles first
+        if (w >= nwork) break;
+        const uint32_t wt = w / S, slice = w - wt * S;
+        const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];  // largest tiles first
         const uint2 rg = V.ctile_range[ct];
         const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
         const SceneDev& sc = scene_ref(V, s);
@@ -619,7 +625,7 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
         float acc[27][4];
 #pragma unroll
         for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = acc[o][3] = 0.f;
-        for (uint32_t i = cb; i < ce; ++i) {
+        for (uint32_t i = cb + slice; i < ce; i += S) {
             const uint32_t p = V.order[i];
             if (p >= (uint32_t)N) {
                 flags |= FLAG_TILE_RANGE;
@@ -1281,6 +1287,23 @@ cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x,
                           cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     k_unpack<<<grid_for(V.N, 256), 256, 0, st>>>(V, user_of_phys, x, v, C, F);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void k_merge_flags(uint32_t* c, int slots, uint32_t* live) {
+    uint32_t f = 0;
+    for (int j = threadIdx.x; j < slots; j += blockDim.x) {
+        f |= c[(size_t)j * CNT_WORDS + CNT_FLAGS];
+        c[(size_t)j * CNT_WORDS + CNT_FLAGS] = 0u;
+    }
+    if (f) atomicOr(&live[CNT_FLAGS], f);
+}
+}  // namespace
+
+cudaError_t launch_merge_flags(uint32_t* slots_counters, int slots, uint32_t* live, cudaStream_t st) {
+    if (slots <= 0) return cudaSuccess;
+    k_merge_flags<<<1, 128, 0, st>>>(slots_counters, slots, live);
     return cudaGetLastError();
 }
 

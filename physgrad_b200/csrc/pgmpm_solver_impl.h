@@ -137,6 +137,12 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf tape_sk, tape_ord;     // slots x N sorted keys / order
     pgmpm::DevBuf tape_gv, tape_gvpre;   // slots x nodes float4
     pgmpm::DevBuf tape_flags, tape_tiles, tape_ctiles, tape_crange, tape_counters;
+    pgmpm::DevBuf tape_cells, tape_ptile;  // per slot: cell ranges and largest-first tile list (bin sort)
+    bool tape_has_last = false;           // the tape holds the forward's last segment (no replay needed)
+    // captured tape work: [0] replay + reverse of a segment, [1] forward of a
+    // segment into the tape, [2] reverse only; each for one segment length
+    cudaGraphExec_t tape_exec[3] = {};
+    int tape_exec_len[3] = {-1, -1, -1};
     pgmpm::DevBuf adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;
 
     pgmpm::StepBufs live_bufs() const {
@@ -196,11 +202,20 @@ struct pgmpm_solver_s {
 
     pgmpm::View view() const { return view_for(live_bufs()); }
 
+    void drop_tape_graphs() {
+        for (int i = 0; i < 3; ++i) {
+            if (tape_exec[i]) cudaGraphExecDestroy(tape_exec[i]);
+            tape_exec[i] = nullptr;
+            tape_exec_len[i] = -1;
+        }
+    }
+
     void drop_graph() {
         if (step_exec) cudaGraphExecDestroy(step_exec);
         if (step_graph) cudaGraphDestroy(step_graph);
         step_exec = nullptr;
         step_graph = nullptr;
+        drop_tape_graphs();
     }
 
     ~pgmpm_solver_s() {
