@@ -67,12 +67,8 @@ __global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     uint32_t flags = 0;
-    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < N; ii += stride) {
-        const uint32_t p = V.order[ii];
-        if (p >= (uint32_t)N) {
-            flags |= FLAG_TILE_RANGE;
-            continue;
-        }
+    // particles in physical order (the order of the state planes)
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
         const int s = V.S == 1 ? 0 : scene_of_particle(V.scenes, V.S, (int)p);
         const SceneDev& sc = scene_ref(V, s);
         const int mid = MULTI ? V.mat[p] : 0;
@@ -115,53 +111,112 @@ __global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
         for (int a = 0; a < 3; ++a) gvt[a] = gv[a] + sc.dt * gx[a];
 #pragma unroll
         for (int a = 0; a < 9; ++a) gCt[a] = gC[a] + sc.dt * gFFt[a];
-        // forward affine matrix
-        float tau[9], Am[9];
-        kirchhoff(F, mt, tau);
+        // forward affine matrix (R kept for the stress adjoint)
+        float tau[9], Am[9], R[9];
+        kirchhoff(F, mt, tau, R);
         const float kk = -sc.dt * mv.y * sc.D;
 #pragma unroll
         for (int a = 0; a < 9; ++a) Am[a] = kk * tau[a] + m * C[a];
         const float dx = sc.dx, D = sc.D, idx_ = 1.f / dx;
+        // Per node i (offset o, d_i = (o - f) dx, weight w_i, gradient gw_i):
+        //   wb_i = m gm_i + v_i . (gvt + D gCt d_i) + gp_i . (m v + Am d_i)
+        //   gx  += wb_i gw_i - w_i (D gCt^T v_i + Am^T gp_i)
+        //   gv  += w_i m gp_i,   Ab += w_i gp_i d_i^T
+        // The bracketed vectors are affine in o: they start at o = 0 and
+        // advance by one matrix column per node step.  The second gx term,
+        // gv and Ab need only sum w v, sum w gp and sum w gp o^T.
+        float Gp[9], Ap[9];  // dx D gCt, dx Am
+#pragma unroll
+        for (int a = 0; a < 9; ++a) {
+            Gp[a] = dx * D * gCt[a];
+            Ap[a] = dx * Am[a];
+        }
+        float b1[3], b2[3];  // at o = 0: gvt - Gp f,  m v - Ap f
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            b1[a] = gvt[a] - (Gp[3 * a] * st.f[0] + Gp[3 * a + 1] * st.f[1] + Gp[3 * a + 2] * st.f[2]);
+            b2[a] = m * v[a] - (Ap[3 * a] * st.f[0] + Ap[3 * a + 1] * st.f[1] + Ap[3 * a + 2] * st.f[2]);
+        }
+        // separable tiled node index: idx = X[i] + Y[j] + Z[k]
+        int X[3], Y[3], Z[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int gi = st.s[0] + a, gj = st.s[1] + a, gk = st.s[2] + a;
+            X[a] = ((gi >> 2) << 6) + (gi & 3);
+            Y[a] = (gj >> 2) * (sc.nt[0] << 6) + ((gj & 3) << 2);
+            Z[a] = (gk >> 2) * ((sc.nt[0] * sc.nt[1]) << 6) + ((gk & 3) << 4) + (sc.nt_base << 6);
+        }
         float ox[3] = {gx[0], gx[1], gx[2]};
-        float ogv[3] = {0.f, 0.f, 0.f};
-        float Ab[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float SWv[3] = {0.f, 0.f, 0.f}, SWg[3] = {0.f, 0.f, 0.f};
+        float Sg[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};  // [axis b][a] = sum w gp_a o_b
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float dk = ((float)k - st.f[2]) * dx;
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                const float dj = ((float)j - st.f[1]) * dx;
+                float h1[3], h2[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    h1[a] = b1[a] + (float)j * Gp[3 * a + 1] + (float)k * Gp[3 * a + 2];
+                    h2[a] = b2[a] + (float)j * Ap[3 * a + 1] + (float)k * Ap[3 * a + 2];
+                }
+                float P0 = 0.f, P1 = 0.f;
+                float rv[3] = {0.f, 0.f, 0.f}, rg[3] = {0.f, 0.f, 0.f}, rgx[3] = {0.f, 0.f, 0.f};
+                const int row = Y[j] + Z[k];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    const float di = ((float)i - st.f[0]) * dx;
-                    const int64_t n = node_index(sc, st.s[0] + i, st.s[1] + j, st.s[2] + k);
+                    const int64_t n = (int64_t)(row + X[i]);
                     const float4 vi = __ldg(&V.grid_v[n]);
                     const float4 gpm = A.grid_gpm[n];
-                    const float w = st.w[0][i] * st.w[1][j] * st.w[2][k];
-                    const float d[3] = {di, dj, dk};
-                    const float vv[3] = {vi.x, vi.y, vi.z};
-                    const float gp[3] = {gpm.x, gpm.y, gpm.z};
-                    float wb = gpm.w * m;
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        const float Cd = gCt[3 * a] * d[0] + gCt[3 * a + 1] * d[1] + gCt[3 * a + 2] * d[2];
-                        const float Ad = Am[3 * a] * d[0] + Am[3 * a + 1] * d[1] + Am[3 * a + 2] * d[2];
-                        wb += gvt[a] * vv[a] + D * vv[a] * Cd + gp[a] * (m * v[a] + Ad);
+                    const float wb = m * gpm.w + vi.x * h1[0] + vi.y * h1[1] + vi.z * h1[2] + gpm.x * h2[0] +
+                                     gpm.y * h2[1] + gpm.z * h2[2];
+                    const float wx = st.w[0][i];
+                    P0 += dw[0][i] * wb;
+                    P1 += wx * wb;
+                    rv[0] += wx * vi.x;
+                    rv[1] += wx * vi.y;
+                    rv[2] += wx * vi.z;
+                    const float t0 = wx * gpm.x, t1 = wx * gpm.y, t2 = wx * gpm.z;
+                    rg[0] += t0;
+                    rg[1] += t1;
+                    rg[2] += t2;
+                    if (i) {
+                        const float fi = (float)i;
+                        rgx[0] += fi * t0;
+                        rgx[1] += fi * t1;
+                        rgx[2] += fi * t2;
                     }
-                    const float gw[3] = {dw[0][i] * st.w[1][j] * st.w[2][k] * idx_,
-                                         st.w[0][i] * dw[1][j] * st.w[2][k] * idx_,
-                                         st.w[0][i] * st.w[1][j] * dw[2][k] * idx_};
+                    if (i < 2) {
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        const float t1 = gCt[a] * vv[0] + gCt[3 + a] * vv[1] + gCt[6 + a] * vv[2];
-                        const float t2 = Am[a] * gp[0] + Am[3 + a] * gp[1] + Am[6 + a] * gp[2];
-                        ox[a] += wb * gw[a] - w * (D * t1 + t2);
-                        ogv[a] += w * m * gp[a];
-#pragma unroll
-                        for (int b = 0; b < 3; ++b) Ab[3 * a + b] += w * gp[a] * d[b];
+                        for (int a = 0; a < 3; ++a) {
+                            h1[a] += Gp[3 * a];
+                            h2[a] += Ap[3 * a];
+                        }
                     }
                 }
+                const float wyz = st.w[1][j] * st.w[2][k];
+                const float R0 = wyz * idx_, R1 = dw[1][j] * st.w[2][k] * idx_, R2 = st.w[1][j] * dw[2][k] * idx_;
+                ox[0] += P0 * R0;
+                ox[1] += P1 * R1;
+                ox[2] += P1 * R2;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    SWv[a] += wyz * rv[a];
+                    SWg[a] += wyz * rg[a];
+                    Sg[0][a] += wyz * rgx[a];
+                    if (j) Sg[1][a] += ((float)j * wyz) * rg[a];
+                    if (k) Sg[2][a] += ((float)k * wyz) * rg[a];
+                }
             }
+        }
+        float ogv[3], Ab[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float t1 = gCt[a] * SWv[0] + gCt[3 + a] * SWv[1] + gCt[6 + a] * SWv[2];
+            const float t2 = Am[a] * SWg[0] + Am[3 + a] * SWg[1] + Am[6 + a] * SWg[2];
+            ox[a] -= D * t1 + t2;
+            ogv[a] = m * SWg[a];
+#pragma unroll
+            for (int bb = 0; bb < 3; ++bb) Ab[3 * a + bb] = dx * (Sg[bb][a] - SWg[a] * st.f[bb]);
         }
         // F' = M F  ->  gF_in = M^T gF'raw, plus the stress adjoint
         float oF[9];
@@ -169,7 +224,7 @@ __global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
         float tb[9];
 #pragma unroll
         for (int a = 0; a < 9; ++a) tb[a] = kk * Ab[a];
-        const float dE = kirchhoff_adjoint(F, mt, tb, oF);
+        const float dE = kirchhoff_adjoint(F, R, mt, tb, oF);
         float oC[9];
 #pragma unroll
         for (int a = 0; a < 9; ++a) oC[a] = m * Ab[a];

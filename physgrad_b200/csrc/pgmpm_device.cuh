@@ -254,10 +254,12 @@ __device__ __forceinline__ void polar_rotation(const float F[9], float R[9]) {
 //   NH : mu (F F^T - I) + lam ln(J) I   (J times the Cauchy form of
 //        src/mpm_kernels.cu:113-127)
 //   EOS: K J (J - 1) I  with K carried in E (p = -K (J - 1))
-__device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, float tau[9]) {
+// R receives the rotation of F's polar decomposition for the fixed-corotated
+// model (and is left unset otherwise), for kirchhoff_adjoint to reuse.
+__device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, float tau[9], float R[9]) {
     const float J = m3_det(F);
     if (m.model == MODEL_FCR) {
-        float R[9], D[9];
+        float D[9];
         polar_rotation(F, R);
 #pragma unroll
         for (int i = 0; i < 9; ++i) D[i] = F[i] - R[i];
@@ -278,6 +280,11 @@ __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, flo
     }
 }
 
+__device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, float tau[9]) {
+    float R[9];
+    kirchhoff(F, m, tau, R);
+}
+
 // Adjoint of kirchhoff(): gF += d<tb, tau(F)>/dF; returns d<tb, tau>/dE.
 // The rotation's derivative follows from F = R S: with M = R^T dF,
 // Omega = R^T dR is skew with axial vector (tr(S) I - S)^{-1} axial(M - M^T),
@@ -285,14 +292,15 @@ __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, flo
 // axial(R^T Rb - Rb^T R).  tr(S) I - S has eigenvalues s_i + s_j (sums of
 // singular values) and stays invertible for det F > 0; no 1/(s_i^2 - s_j^2)
 // terms appear.
-__device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const MatDev& m, const float tb[9], float gF[9]) {
+// R: the rotation kirchhoff(F, m, tau, R) returned (fixed-corotated only).
+__device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const float R[9], const MatDev& m,
+                                                   const float tb[9], float gF[9]) {
     float cofF[9];
     m3_cof(F, cofF);
     const float J = F[0] * cofF[0] + F[1] * cofF[1] + F[2] * cofF[2];  // cof = J F^{-T}
     const float trt = tb[0] + tb[4] + tb[8];
     if (m.model == MODEL_FCR) {
-        float R[9], D[9], tbF[9], tbTD[9];
-        polar_rotation(F, R);
+        float D[9], tbF[9], tbTD[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) D[i] = F[i] - R[i];
         m3_mul(tb, F, tbF);
@@ -350,6 +358,12 @@ __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const MatDe
         for (int i = 0; i < 9; ++i) gF[i] += c * cofF[i];
         return trt * J * (J - 1.f);
     }
+}
+
+__device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const MatDev& m, const float tb[9], float gF[9]) {
+    float R[9];
+    if (m.model == MODEL_FCR) polar_rotation(F, R);
+    return kirchhoff_adjoint(F, R, m, tb, gF);
 }
 
 // --------------------------------------------------------- P2G payload
