@@ -59,7 +59,7 @@ constexpr int GATHER_T = 128;
 constexpr int MAX_SMEM_MATS = 64;
 
 template <bool MULTI, bool FLUID>
-__global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
+__global__ void __launch_bounds__(GATHER_T, 3) k_adj_gather(View V, AdjView A) {
     __shared__ float sE[MAX_SMEM_MATS];
     const bool smem_e = V.M <= MAX_SMEM_MATS;
     for (int m = threadIdx.x; m < MAX_SMEM_MATS; m += blockDim.x) sE[m] = 0.f;
@@ -125,12 +125,15 @@ __global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
         // The bracketed vectors are affine in o: they start at o = 0 and
         // advance by one matrix column per node step.  The second gx term,
         // gv and Ab need only sum w v, sum w gp and sum w gp o^T.
-        float Gp[9], Ap[9];  // dx D gCt, dx Am
+        float Gp[9], Ap[9];  // dx D gCt, dx Am (gCt and Am are not needed past this point)
 #pragma unroll
         for (int a = 0; a < 9; ++a) {
             Gp[a] = dx * D * gCt[a];
             Ap[a] = dx * Am[a];
         }
+        // F' = M F  ->  gF_in = M^T gF'raw (the stress adjoint adds to it after the loop)
+        float oF[9];
+        m3_Tmul(M, gF, oF);
         float b1[3], b2[3];  // at o = 0: gvt - Gp f,  m v - Ap f
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -211,16 +214,15 @@ __global__ void __launch_bounds__(GATHER_T) k_adj_gather(View V, AdjView A) {
         float ogv[3], Ab[9];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float t1 = gCt[a] * SWv[0] + gCt[3 + a] * SWv[1] + gCt[6 + a] * SWv[2];
-            const float t2 = Am[a] * SWg[0] + Am[3 + a] * SWg[1] + Am[6 + a] * SWg[2];
-            ox[a] -= D * t1 + t2;
+            // D gCt^T sum(w v) + Am^T sum(w gp), from Gp = dx D gCt and Ap = dx Am
+            const float t1 = Gp[a] * SWv[0] + Gp[3 + a] * SWv[1] + Gp[6 + a] * SWv[2];
+            const float t2 = Ap[a] * SWg[0] + Ap[3 + a] * SWg[1] + Ap[6 + a] * SWg[2];
+            ox[a] -= (t1 + t2) * idx_;
             ogv[a] = m * SWg[a];
 #pragma unroll
             for (int bb = 0; bb < 3; ++bb) Ab[3 * a + bb] = dx * (Sg[bb][a] - SWg[a] * st.f[bb]);
         }
-        // F' = M F  ->  gF_in = M^T gF'raw, plus the stress adjoint
-        float oF[9];
-        m3_Tmul(M, gF, oF);
+        // plus the stress adjoint
         float tb[9];
 #pragma unroll
         for (int a = 0; a < 9; ++a) tb[a] = kk * Ab[a];
