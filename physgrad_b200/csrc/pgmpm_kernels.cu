@@ -584,8 +584,10 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
     const uint32_t ntiles = V.counters[CNT_CTILES];
     // Few occupied tiles (a small, dense scene) leave most blocks idle: then
     // each cell's run is split into S interleaved slices, one work item per
-    // (tile, slice), each flushing its own partial sums.
-    const uint32_t S = ntiles ? min(8u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
+    // (tile, slice), each flushing its own partial sums.  S stops at 4: a
+    // work item's flush (216 node sums) outweighs a handful of particles
+    // per thread.
+    const uint32_t S = ntiles ? min(4u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
     const uint32_t nwork = ntiles * S;
     for (;;) {
         if (c == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
