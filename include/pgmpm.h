@@ -184,7 +184,10 @@ PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, i
 /* Kernel variants.  p2g_variant 0: (cell, z-slice) register accumulation
  * over occupied 4^3 cell tiles (persistent, p2g_tiles_per_sm blocks per SM);
  * 1: per-particle shared-memory atomics over chunks of ppt particles;
- * 2: one thread per cell with 108 register accumulators (default).
+ * 2: one thread per cell with 108 register accumulators;
+ * 3: variant 2 with each cell's accumulators split over two lanes (MLS
+ * forward; p2g_tiles_per_sm capped at 5).  pgmpm_create picks 3 for MLS
+ * solvers of at least 2^20 particles, 2 otherwise.
  * g2p_variant 0: tile-staged gather (g2p_tiles_per_sm blocks per SM);
  * 1: direct gather in sorted order; 2: direct gather in physical order.
  * Negative keeps a value. */

@@ -57,7 +57,9 @@ struct View {
 
 // P2G variants: 0 = (cell, z-slice) register accumulation with a staged
 // payload, 1 = per-particle shared-memory atomics over fixed chunks,
-// 2 = one thread per cell, 108 register accumulators, no staging (default).
+// 2 = one thread per cell, 108 register accumulators, no staging,
+// 3 = variant 2 with a cell's accumulators split over two lanes (MLS
+// forward; the REF physics and the adjoint scatter run variant 2).
 // G2P variant 2 = direct gather in physical particle order (default).
 // G2P variants: 0 = node tile staged in shared memory, 1 = direct gather.
 struct Tuning {
@@ -70,6 +72,7 @@ struct Tuning {
     int tile_blocks_per_sm = 3;  // persistent P2G tile kernel: blocks per SM
     int g2p_tiles_per_sm = 2;    // persistent G2P tile kernel: blocks per SM (256 threads)
     int cell_blocks_per_sm = 6;  // persistent P2G thread-per-cell kernel (variant 2): blocks per SM
+    int pair_blocks_per_sm = 5;  // persistent P2G two-threads-per-cell kernel (variant 3): blocks per SM
     int step_sort = 0;           // per-step sort: 0 = bin sort (counting sorts by tile, then cell), 1 = radix sort
 };
 

@@ -760,6 +760,126 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// ------------------------------------- P2G, two threads per cell (MLS)
+// Variant 3: variant 2 with each cell's 108 accumulators split over a pair
+// of adjacent lanes -- lane 2c+0 holds (m, p_x), lane 2c+1 holds (p_y, p_z)
+// of the 27 nodes -- so that a 128-thread block of ~100 registers per
+// thread fits 5 times per SM (20 warps against variant 2's 12).  Both lanes
+// of a pair read the same payload (one memory request), compute the
+// weights, and accumulate their two channels; the flush is variant 2's.
+constexpr int P2GP_T = 128;
+
+__global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
+    __shared__ float T[27 * 4 * 64];
+    __shared__ uint32_t s_work;
+    const int c = threadIdx.x >> 1, h = threadIdx.x & 1;
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    // slices of a cell's run when tiles are few (see k_p2g_cells)
+    const uint32_t S = ntiles ? min(4u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
+    const uint32_t nwork = ntiles * S;
+    for (;;) {
+        if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= nwork) break;
+        const uint32_t wt = w / S, slice = w - wt * S;
+        const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        uint32_t cb, ce;
+        if (V.cell_range) {
+            const uint2 cr = V.cell_range[(size_t)ct * 64 + c];
+            cb = max(cr.x, rg.x);
+            ce = min(cr.y, rg.y);
+        } else {
+            const uint32_t kc = (ct << 6) | (uint32_t)c;
+            uint32_t lo = rg.x, hi = rg.y;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (V.skeys[mid] < kc) lo = mid + 1; else hi = mid;
+            }
+            cb = lo;
+            hi = rg.y;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (V.skeys[mid] <= kc) lo = mid + 1; else hi = mid;
+            }
+            ce = lo;
+        }
+        float accA[27], accB[27];
+#pragma unroll
+        for (int o = 0; o < 27; ++o) accA[o] = accB[o] = 0.f;
+        for (uint32_t i = cb + slice; i < ce; i += S) {
+            const uint32_t p = V.order[i];
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            const float4 a0 = V.pay[p], a1 = V.pay[N + p], a2 = V.pay[2 * N + p], a3 = V.pay[3 * N + p];
+            // channel value at offset o: beta + gamma . o
+            //   lane 0: A = m (gamma 0), B = p_x (b_x, Ad row 0)
+            //   lane 1: A = p_y (b_y, Ad row 1), B = p_z (b_z, Ad row 2)
+            const float bA = h ? a0.y : a0.w, bB = h ? a0.z : a0.x;
+            const float gAx = h ? a1.w : 0.f, gAy = h ? a2.x : 0.f, gAz = h ? a2.y : 0.f;
+            const float gBx = h ? a2.z : a1.x, gBy = h ? a2.w : a1.y, gBz = h ? a3.x : a1.z;
+            float wt[3][3];
+            mls_weights(a3.y, wt[0]);
+            mls_weights(a3.z, wt[1]);
+            mls_weights(a3.w, wt[2]);
+#pragma unroll
+            for (int zz = 0; zz < 3; ++zz) {
+                const float zA = bA + gAz * (float)zz, zB = bB + gBz * (float)zz;
+#pragma unroll
+                for (int yy = 0; yy < 3; ++yy) {
+                    const float wyz = wt[1][yy] * wt[2][zz];
+                    float vA = zA + gAy * (float)yy, vB = zB + gBy * (float)yy;
+#pragma unroll
+                    for (int xx = 0; xx < 3; ++xx) {
+                        const int o = xx + 3 * yy + 9 * zz;
+                        const float wgt = wt[0][xx] * wyz;
+                        accA[o] += wgt * vA;
+                        accB[o] += wgt * vB;
+                        vA += gAx;
+                        vB += gBx;
+                    }
+                }
+            }
+        }
+        // flush: transpose through shared memory, one vector atomic per node
+#pragma unroll
+        for (int o = 0; o < 27; ++o) {
+            T[(o * 4 + 2 * h) * 64 + c] = accA[o];
+            T[(o * 4 + 2 * h + 1) * 64 + c] = accB[o];
+        }
+        __syncthreads();
+        for (int n = threadIdx.x; n < TILE_NODES; n += P2GP_T) {
+            const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int zz = max(0, nz - 3); zz <= min(2, nz); ++zz)
+                for (int yy = max(0, ny - 3); yy <= min(2, ny); ++yy)
+                    for (int xx = max(0, nx - 3); xx <= min(2, nx); ++xx) {
+                        const int cc = (nx - xx) + 4 * (ny - yy) + 16 * (nz - zz);
+                        const int o = xx + 3 * yy + 9 * zz;
+                        a4.x += T[(o * 4 + 0) * 64 + cc];
+                        a4.y += T[(o * 4 + 1) * 64 + cc];
+                        a4.z += T[(o * 4 + 2) * 64 + cc];
+                        a4.w += T[(o * 4 + 3) * 64 + cc];
+                    }
+            const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
+            if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+        }
+        __syncthreads();
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
 // ------------------------------------------------------------ grid update
 template <int PHYS>
 __global__ void k_grid(View V) {
@@ -1158,7 +1278,7 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
                                cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
-    if (t.p2g_variant == 2) {
+    if (t.p2g_variant == 2 || t.p2g_variant == 3) {  // the adjoint scatter of variant 3 is variant 2's
         const int nb = num_sms * t.cell_blocks_per_sm;
         if (pf.multi_mat) {
             if (pf.has_fluid)
@@ -1190,7 +1310,12 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
 
 cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
-    if (t.p2g_variant == 2) {
+    if (t.p2g_variant == 3 && pf.physics == PHYS_MLS) {
+        if (!V.pay) return cudaErrorInvalidValue;
+        k_p2g_pairs<<<num_sms * t.pair_blocks_per_sm, P2GP_T, 0, st>>>(V);
+        return cudaGetLastError();
+    }
+    if (t.p2g_variant == 2 || t.p2g_variant == 3) {  // REF physics: variant 3 runs variant 2
         const int nb = num_sms * t.cell_blocks_per_sm;
         const AdjView none{};
         if (pf.physics == PHYS_MLS) {

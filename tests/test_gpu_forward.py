@@ -253,7 +253,7 @@ def test_batched_scenes_equal_single_scenes(gpu):
         off += c
 
 
-@pytest.mark.parametrize("p2g_variant,g2p_variant", [(0, 0), (1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (2, 2), (0, 2)])
+@pytest.mark.parametrize("p2g_variant,g2p_variant", [(0, 0), (1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (2, 2), (0, 2), (3, 2), (3, 0)])
 @pytest.mark.parametrize("physics", [0, 1])
 def test_kernel_variants_agree(gpu, oracle, p2g_variant, g2p_variant, physics):
     """Every P2G/G2P variant matches the checkers (MLS: FP64 oracle; REF:
