@@ -1100,8 +1100,10 @@ template <int PHYS, bool MULTI, bool FLUID>
 __global__ void k_g2p(View V) {
     k_g2p_impl<PHYS, MULTI, FLUID, false>(V);
 }
+// 64 registers (4 blocks of 256 threads per SM): the gathers' latency wants
+// the occupancy more than the few spilled words cost
 template <int PHYS, bool MULTI, bool FLUID>
-__global__ void k_g2p_phys(View V) {
+__global__ void __launch_bounds__(512, 2) k_g2p_phys(View V) {
     k_g2p_impl<PHYS, MULTI, FLUID, true>(V);
 }
 
