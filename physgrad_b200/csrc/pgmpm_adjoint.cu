@@ -294,13 +294,14 @@ __global__ void k_state_to_planes(const float* __restrict__ x, const float* __re
     }
 }
 
-__global__ void k_planes_to_state(const float4* __restrict__ g, const uint32_t* __restrict__ user_of_phys,
+__global__ void k_planes_to_state(const float4* __restrict__ g, const uint32_t* __restrict__ phys_of_user,
                                   float* __restrict__ x, float* __restrict__ v, float* __restrict__ C,
                                   float* __restrict__ F, int64_t N) {
+    // upload order: contiguous writes of the caller's records, gathered planes
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-        const int64_t u = user_of_phys[i];
-        if (u >= N) continue;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < N; u += stride) {
+        const int64_t i = phys_of_user[u];
+        if (i >= N) continue;
         float xx[3], FF[9], vv[3], CC[9];
         unpack_xF(g[i], g[N + i], g[2 * N + i], xx, FF);
         unpack_vC(g[3 * N + i], g[4 * N + i], g[5 * N + i], vv, CC);
@@ -360,10 +361,10 @@ cudaError_t launch_state_to_planes(const float* x, const float* v, const float* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_planes_to_state(const float4* g, const uint32_t* user_of_phys, float* x, float* v, float* C,
+cudaError_t launch_planes_to_state(const float4* g, const uint32_t* phys_of_user, float* x, float* v, float* C,
                                    float* F, int64_t N, cudaStream_t st) {
     if (N == 0) return cudaSuccess;
-    k_planes_to_state<<<blocks_for(N, 256), 256, 0, st>>>(g, user_of_phys, x, v, C, F, N);
+    k_planes_to_state<<<blocks_for(N, 256), 256, 0, st>>>(g, phys_of_user, x, v, C, F, N);
     return cudaGetLastError();
 }
 

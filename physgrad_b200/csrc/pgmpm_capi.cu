@@ -310,6 +310,7 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->mV, sizeof(float2) * (size_t)std::max<int64_t>(N, 1));
     if (s->pf.multi_mat) AL(s->mat, n4);
     AL(s->user_of_phys, n4);
+    AL(s->phys_of_user, n4);
     AL(s->keys, n4);
     AL(s->ka, n4);
     AL(s->va, n4);
@@ -435,7 +436,7 @@ int pgmpm_upload(pgmpm_solver s, const float* x, const float* v, const float* C,
                             s->kb.as<uint32_t>(), s->vb.as<uint32_t>(), s->sort_scratch.as<uint32_t>(), N, 1, &w0,
                             st));
         const uint32_t* iota = w0 ? s->vb.as<uint32_t>() : s->va.as<uint32_t>();
-        CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, iota, s->user_of_phys.as<uint32_t>(), s->mV.as<float2>(),
+        CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, iota, s->user_of_phys.as<uint32_t>(), s->phys_of_user.as<uint32_t>(), s->mV.as<float2>(),
                        s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr, st));
         // 2. keys of the user-order positions, stable sort -> physical order
         CK(launch_keys(V, s->pf, st));
@@ -446,7 +447,7 @@ int pgmpm_upload(pgmpm_solver s, const float* x, const float* v, const float* C,
         const uint32_t* ord = which ? s->vb.as<uint32_t>() : s->va.as<uint32_t>();
         const uint32_t* sk = which ? s->kb.as<uint32_t>() : s->ka.as<uint32_t>();
         // 3. pack in sorted order; the sorted keys are the keys of the physical order
-        CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, ord, s->user_of_phys.as<uint32_t>(), s->mV.as<float2>(),
+        CK(launch_pack(V, dx_, dv, dC, dF, dm, dV0, dmat, ord, s->user_of_phys.as<uint32_t>(), s->phys_of_user.as<uint32_t>(), s->mV.as<float2>(),
                        s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr, st));
         CK(cudaMemcpyAsync(s->keys.p, sk, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         int rc = refresh_payload(s, st);
@@ -465,7 +466,7 @@ int pgmpm_download(pgmpm_solver s, float* x, float* v, float* C, float* F, int32
     if (N == 0) return PGMPM_OK;
     View V = s->view();
     if (ptr_kind == PGMPM_PTR_DEVICE) {
-        CK(launch_unpack(V, s->user_of_phys.as<uint32_t>(), x, v, C, F, st));
+        CK(launch_unpack(V, s->phys_of_user.as<uint32_t>(), x, v, C, F, st));
         return PGMPM_OK;
     }
     if (ptr_kind != PGMPM_PTR_HOST) return fail(PGMPM_ERR_ARG, "bad ptr_kind");
@@ -474,7 +475,7 @@ int pgmpm_download(pgmpm_solver s, float* x, float* v, float* C, float* F, int32
     float* sv = sx + 3 * N;
     float* sC = sv + 3 * N;
     float* sF = sC + 9 * N;
-    CK(launch_unpack(V, s->user_of_phys.as<uint32_t>(), x ? sx : nullptr, v ? sv : nullptr, C ? sC : nullptr,
+    CK(launch_unpack(V, s->phys_of_user.as<uint32_t>(), x ? sx : nullptr, v ? sv : nullptr, C ? sC : nullptr,
                      F ? sF : nullptr, st));
     if (x) CK(cudaMemcpyAsync(x, sx, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
     if (v) CK(cudaMemcpyAsync(v, sv, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));

@@ -269,14 +269,14 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
     CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), s->tape_slots, s->counters.as<uint32_t>(), st));
     // physical planes -> caller's arrays (upload order)
     if (ptr_kind == PGMPM_PTR_DEVICE) {
-        CK(launch_planes_to_state(A.g, s->user_of_phys.as<uint32_t>(), gx_in, gv_in, gC_in, gF_in, N, st));
+        CK(launch_planes_to_state(A.g, s->phys_of_user.as<uint32_t>(), gx_in, gv_in, gC_in, gF_in, N, st));
         if (gE) CK(cudaMemcpyAsync(gE, A.gE, sizeof(float) * M, cudaMemcpyDeviceToDevice, st));
         return PGMPM_OK;
     }
     CK(s->adj_stage.ensure(sizeof(float) * 24 * Nz));
     float* b = s->adj_stage.as<float>();
     float *sx = b, *sv = b + 3 * N, *sC = b + 6 * N, *sF = b + 15 * N;
-    CK(launch_planes_to_state(A.g, s->user_of_phys.as<uint32_t>(), gx_in ? sx : nullptr, gv_in ? sv : nullptr,
+    CK(launch_planes_to_state(A.g, s->phys_of_user.as<uint32_t>(), gx_in ? sx : nullptr, gv_in ? sv : nullptr,
                               gC_in ? sC : nullptr, gF_in ? sF : nullptr, N, st));
     if (gx_in && N) CK(cudaMemcpyAsync(gx_in, sx, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
     if (gv_in && N) CK(cudaMemcpyAsync(gv_in, sv, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));

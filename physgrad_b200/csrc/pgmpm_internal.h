@@ -124,8 +124,10 @@ cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int
 cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_pack(const View& V, const float* x, const float* v, const float* C, const float* F,
                         const float* m, const float* V0, const int32_t* mat, const uint32_t* order,
-                        uint32_t* user_of_phys, float2* mV_out, int32_t* mat_out, cudaStream_t st);
-cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x, float* v, float* C, float* F,
+                        uint32_t* user_of_phys, uint32_t* phys_of_user, float2* mV_out, int32_t* mat_out,
+                        cudaStream_t st);
+// phys_of_user: upload index -> physical slot (written by launch_pack)
+cudaError_t launch_unpack(const View& V, const uint32_t* phys_of_user, float* x, float* v, float* C, float* F,
                           cudaStream_t st);
 // ORs the error flags of `slots` counter blocks (stride CNT_WORDS) into
 // live[CNT_FLAGS] and clears them.
@@ -153,7 +155,7 @@ cudaError_t launch_adj_gather(const View& V, const AdjView& A, const PhysFlags& 
                               cudaStream_t st);
 cudaError_t launch_state_to_planes(const float* x, const float* v, const float* C, const float* F,
                                    const uint32_t* user_of_phys, float4* g, int64_t N, cudaStream_t st);
-cudaError_t launch_planes_to_state(const float4* g, const uint32_t* user_of_phys, float* x, float* v, float* C,
+cudaError_t launch_planes_to_state(const float4* g, const uint32_t* phys_of_user, float* x, float* v, float* C,
                                    float* F, int64_t N, cudaStream_t st);
 
 }  // namespace pgmpm

@@ -1159,7 +1159,8 @@ __global__ void k_pack(View V, const float* __restrict__ x, const float* __restr
                        const float* __restrict__ C, const float* __restrict__ F, const float* __restrict__ m,
                        const float* __restrict__ V0, const int32_t* __restrict__ mat,
                        const uint32_t* __restrict__ order, uint32_t* __restrict__ user_of_phys,
-                       float2* __restrict__ mV_out, int32_t* __restrict__ mat_out) {
+                       uint32_t* __restrict__ phys_of_user, float2* __restrict__ mV_out,
+                       int32_t* __restrict__ mat_out) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
@@ -1198,16 +1199,19 @@ __global__ void k_pack(View V, const float* __restrict__ x, const float* __restr
             mat_out[i] = mid;
         }
         user_of_phys[i] = u;
+        phys_of_user[u] = (uint32_t)i;
     }
 }
 
-__global__ void k_unpack(View V, const uint32_t* __restrict__ user_of_phys, float* __restrict__ x,
+// Walks the upload order: the caller's records are written contiguously and
+// the state planes are gathered (scattered partial-sector writes cost more).
+__global__ void k_unpack(View V, const uint32_t* __restrict__ phys_of_user, float* __restrict__ x,
                          float* __restrict__ v, float* __restrict__ C, float* __restrict__ F) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-        const int64_t u = user_of_phys[i];
-        if (u >= N) continue;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < N; u += stride) {
+        const int64_t i = phys_of_user[u];
+        if (i >= N) continue;
         float xx[3], FF[9], vv[3], CC[9];
         unpack_xF(V.q[i], V.q[N + i], V.q[2 * N + i], xx, FF);
         unpack_vC(V.q[3 * N + i], V.q[4 * N + i], V.q[5 * N + i], vv, CC);
@@ -1406,16 +1410,18 @@ cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int 
 
 cudaError_t launch_pack(const View& V, const float* x, const float* v, const float* C, const float* F,
                         const float* m, const float* V0, const int32_t* mat, const uint32_t* order,
-                        uint32_t* user_of_phys, float2* mV_out, int32_t* mat_out, cudaStream_t st) {
+                        uint32_t* user_of_phys, uint32_t* phys_of_user, float2* mV_out, int32_t* mat_out,
+                        cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
-    k_pack<<<grid_for(V.N, 256), 256, 0, st>>>(V, x, v, C, F, m, V0, mat, order, user_of_phys, mV_out, mat_out);
+    k_pack<<<grid_for(V.N, 256), 256, 0, st>>>(V, x, v, C, F, m, V0, mat, order, user_of_phys, phys_of_user, mV_out,
+                                               mat_out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_unpack(const View& V, const uint32_t* user_of_phys, float* x, float* v, float* C, float* F,
+cudaError_t launch_unpack(const View& V, const uint32_t* phys_of_user, float* x, float* v, float* C, float* F,
                           cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
-    k_unpack<<<grid_for(V.N, 256), 256, 0, st>>>(V, user_of_phys, x, v, C, F);
+    k_unpack<<<grid_for(V.N, 256), 256, 0, st>>>(V, phys_of_user, x, v, C, F);
     return cudaGetLastError();
 }
 

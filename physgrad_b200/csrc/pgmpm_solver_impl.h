@@ -112,7 +112,7 @@ struct pgmpm_solver_s {
     bool uploaded = false;
 
     // device buffers
-    pgmpm::DevBuf d_scenes, d_mats, q, pay, mV, mat, user_of_phys, keys, ka, va, kb, vb, sort_scratch;
+    pgmpm::DevBuf d_scenes, d_mats, q, pay, mV, mat, user_of_phys, phys_of_user, keys, ka, va, kb, vb, sort_scratch;
     pgmpm::DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
     pgmpm::DevBuf bs_ccount, bs_coff, bs_tcount, bs_toff, bs_bsum, bs_slot, cell_range;  // per-step bin sort
     pgmpm::DevBuf ptile_list, tile_rank;  // largest-first occupied tile list (bin sort)
