@@ -185,3 +185,50 @@ def test_batched_adjoint_equals_single_scenes(gpu):
         assert np.abs(gb["v"][sl] - g1["v"]).max() <= 1e-3 * np.abs(g1["v"]).max()
         assert abs(gb["E"][s] - g1["E"][0]) <= 1e-3 * abs(g1["E"][0]) + 1e-12
         off += c
+
+
+def test_checkpointed_forward_leaves_the_stepped_state(gpu):
+    """forward_checkpointed runs its last segment in the tape and hands the
+    state back: the live state, the grid and later steps match plain
+    stepping (to FP32 summation-order tolerance: atomic order differs)."""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.two_material_drop(n_particles=30000, n=32, seed=5)
+    outs = []
+    for mode in ("plain", "checkpointed"):
+        sim = gpu.Simulator(scenes, counts, mats)
+        sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st["mat"])
+        if mode == "plain":
+            sim.step(13)
+        else:
+            sim.forward_checkpointed(13, 5)  # segments of 5, 5, 3: the last runs in the tape
+        grid = sim.grid(0)
+        mid = sim.download()
+        sim.step(4)  # stepping continues from the handed-back state
+        outs.append((mid, grid, sim.download(), sim.metrics()["total_steps"]))
+        assert sim.status() == 0
+        sim.close()
+    (m0, g0, e0, n0), (m1, g1, e1, n1) = outs
+    assert n0 == n1 == 17
+    for key in ("x", "v", "C", "F"):
+        for a, b in ((m0, m1), (e0, e1)):
+            err = np.abs(a[key] - b[key]).max() / max(np.abs(a[key]).max(), 1e-30)
+            assert err < 1e-4, (key, err)
+    (gm0, gv0), (gm1, gv1) = g0, g1
+    assert np.abs(gm0 - gm1).max() <= 1e-4 * np.abs(gm0).max()
+    assert np.abs(gv0 - gv1).max() <= 1e-3 * (np.abs(gv0).max() + 1e-6)
+
+
+def test_tape_steps_report_error_flags(gpu):
+    """A particle leaving the grid inside the segment the forward runs in the
+    tape still raises PGMPM_FLAG_ESCAPE on the solver."""
+    from physgrad_b200 import _capi as C
+
+    s = gpu.Scene((16, 16, 16), 1 / 16, 1e-3, boundary=C.BC_NONE)
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3)]
+    sim = gpu.Simulator([s], [2], mats)
+    x = np.array([[0.5, 0.5, 0.5], [0.5, 0.5, 0.5]], np.float32)
+    v = np.array([[0, 0, 0], [0, 0, 300.0]], np.float32)
+    sim.upload(x, v, None, None, np.full(2, 1e-3, np.float32), np.full(2, 1e-6, np.float32))
+    sim.forward_checkpointed(30, 30)  # one segment: every step runs in the tape
+    assert sim.status() & C.FLAG_ESCAPE

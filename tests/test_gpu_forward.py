@@ -232,11 +232,15 @@ def test_mls_grid_download_matches_oracle(gpu, oracle):
 
 
 # --------------------------------------------------------- batching / misc
-def test_batched_scenes_equal_single_scenes(gpu):
+@pytest.mark.parametrize("p2g_variant", [2, 3])
+def test_batched_scenes_equal_single_scenes(gpu, p2g_variant):
+    """One batched solver over scenes of uneven sizes and grids gives each
+    scene's single-scene result (both per-cell P2G kernels)."""
     from physgrad_b200 import workloads as W
 
     scenes, counts, mats, st, _ = W.batched_scenes(n_scenes=5, lo=500, hi=20000, seed=6, v_sigma=0.3)
     sim = _sim(gpu, scenes, counts, mats, st)
+    sim.set_variants(p2g_variant=p2g_variant)
     sim.step(20)
     out = sim.download()
     off = 0
