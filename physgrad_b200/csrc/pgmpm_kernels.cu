@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
 constexpr int P2GP_T = 128;
 
 __global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
-    __shared__ float T[27 * 4 * 64];
+    __shared__ float4 T4[27 * 64];  // [offset o][cell]: the 4 channels of cell's node o
     __shared__ uint32_t s_work;
     const int c = threadIdx.x >> 1, h = threadIdx.x & 1;
     const int64_t N = V.N;
@@ -851,25 +851,39 @@ __global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
                 }
             }
         }
-        // flush: transpose through shared memory, one vector atomic per node
+        // flush: each lane stores its two channels of node o as one float2 of
+        // T4[o][c]; then node n sums T4[o][n - o] over the offsets o whose
+        // cell lies in the tile (all 27 offsets walked by every lane, the
+        // shared-memory offsets compile-time) and issues one vector atomic
 #pragma unroll
-        for (int o = 0; o < 27; ++o) {
-            T[(o * 4 + 2 * h) * 64 + c] = accA[o];
-            T[(o * 4 + 2 * h + 1) * 64 + c] = accB[o];
-        }
+        for (int o = 0; o < 27; ++o)
+            reinterpret_cast<float2*>(&T4[o * 64 + c])[h] = make_float2(accA[o], accB[o]);
         __syncthreads();
         for (int n = threadIdx.x; n < TILE_NODES; n += P2GP_T) {
             const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            // bit d of vx: cell x = nx - d is inside the tile (0..3); same for y, z
+            const uint32_t vx = (nx <= 3 ? 1u : 0u) | (nx >= 1 && nx <= 4 ? 2u : 0u) | (nx >= 2 ? 4u : 0u);
+            const uint32_t vy = (ny <= 3 ? 1u : 0u) | (ny >= 1 && ny <= 4 ? 2u : 0u) | (ny >= 2 ? 4u : 0u);
+            const uint32_t vz = (nz <= 3 ? 1u : 0u) | (nz >= 1 && nz <= 4 ? 2u : 0u) | (nz >= 2 ? 4u : 0u);
+            const int cn = nx + 4 * ny + 16 * nz;
             float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int zz = max(0, nz - 3); zz <= min(2, nz); ++zz)
-                for (int yy = max(0, ny - 3); yy <= min(2, ny); ++yy)
-                    for (int xx = max(0, nx - 3); xx <= min(2, nx); ++xx) {
-                        const int cc = (nx - xx) + 4 * (ny - yy) + 16 * (nz - zz);
-                        const int o = xx + 3 * yy + 9 * zz;
-                        a4.x += T[(o * 4 + 0) * 64 + cc];
-                        a4.y += T[(o * 4 + 1) * 64 + cc];
-                        a4.z += T[(o * 4 + 2) * 64 + cc];
-                        a4.w += T[(o * 4 + 3) * 64 + cc];
+#pragma unroll
+            for (int zz = 0; zz < 3; ++zz)
+#pragma unroll
+                for (int yy = 0; yy < 3; ++yy)
+#pragma unroll
+                    for (int xx = 0; xx < 3; ++xx) {
+                        const bool valid = ((vx >> xx) & (vy >> yy) & (vz >> zz) & 1u) != 0u;
+                        // cell n - o when it is in the tile, else slot 0 (read, not added):
+                        // the address stays inside the table either way
+                        const int cell = valid ? cn - (xx + 4 * yy + 16 * zz) : 0;
+                        const float4 t = T4[(xx + 3 * yy + 9 * zz) * 64 + cell];
+                        if (valid) {
+                            a4.x += t.x;
+                            a4.y += t.y;
+                            a4.z += t.z;
+                            a4.w += t.w;
+                        }
                     }
             const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
             if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
