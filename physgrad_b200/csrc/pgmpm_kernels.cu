@@ -564,6 +564,37 @@ __device__ __forceinline__ void adj_payload(const View& V, const AdjView& AV, co
         b[a] = (gv[a] + sc.dt * gx[a]) - (Ad[3 * a] * st.f[0] + Ad[3 * a + 1] * st.f[1] + Ad[3 * a + 2] * st.f[2]);
 }
 
+// Sum of the contributions to node (nx, ny, nz) of the 6^3 node block of a
+// 4^3 cell tile, from T4[o * 64 + cell] = cell's accumulators for its
+// stencil offset o.  Every offset is walked (compile-time shared offsets,
+// no divergence); an offset whose cell falls outside the tile reads slot 0
+// and is not added, so the address stays inside the table.
+__device__ __forceinline__ float4 tile_node_sum(const float4* T4, int nx, int ny, int nz) {
+    // bit d of vx: cell x = nx - d lies in the tile (0..3); same for y, z
+    const uint32_t vx = (nx <= 3 ? 1u : 0u) | (nx >= 1 && nx <= 4 ? 2u : 0u) | (nx >= 2 ? 4u : 0u);
+    const uint32_t vy = (ny <= 3 ? 1u : 0u) | (ny >= 1 && ny <= 4 ? 2u : 0u) | (ny >= 2 ? 4u : 0u);
+    const uint32_t vz = (nz <= 3 ? 1u : 0u) | (nz >= 1 && nz <= 4 ? 2u : 0u) | (nz >= 2 ? 4u : 0u);
+    const int cn = nx + 4 * ny + 16 * nz;
+    float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int zz = 0; zz < 3; ++zz)
+#pragma unroll
+        for (int yy = 0; yy < 3; ++yy)
+#pragma unroll
+            for (int xx = 0; xx < 3; ++xx) {
+                const bool valid = ((vx >> xx) & (vy >> yy) & (vz >> zz) & 1u) != 0u;
+                const int cell = valid ? cn - (xx + 4 * yy + 16 * zz) : 0;
+                const float4 t = T4[(xx + 3 * yy + 9 * zz) * 64 + cell];
+                if (valid) {
+                    a4.x += t.x;
+                    a4.y += t.y;
+                    a4.z += t.z;
+                    a4.w += t.w;
+                }
+            }
+    return a4;
+}
+
 // ------------------------------------------------ P2G, one thread per cell
 // Variant 2: one 64-thread block per occupied cell tile, thread c owns cell
 // c and all 27 nodes of its stencil (108 register accumulators).  The
@@ -576,7 +607,7 @@ constexpr int P2GC_T = 64;
 template <int MODE, bool MULTI, bool FLUID>
 __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
     constexpr int PHYS = MODE == MODE_REF ? PHYS_REF : PHYS_MLS;
-    __shared__ float T[27 * 4 * 64];
+    __shared__ float4 T4[27 * 64];  // [offset o][cell]: the 4 channels of cell's node o
     __shared__ uint32_t s_work;
     const int c = threadIdx.x;
     const int64_t N = V.N;
@@ -728,28 +759,15 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
                 }
             }
         }
-        // flush: transpose through shared memory, one vector atomic per node
+        // flush: the thread stores its cell's node o as T4[o][c]; then node n
+        // sums T4[o][n - o] over the offsets whose cell lies in the tile and
+        // issues one vector atomic (see k_p2g_pairs)
 #pragma unroll
-        for (int o = 0; o < 27; ++o) {
-            T[(o * 4 + 0) * 64 + c] = acc[o][0];
-            T[(o * 4 + 1) * 64 + c] = acc[o][1];
-            T[(o * 4 + 2) * 64 + c] = acc[o][2];
-            T[(o * 4 + 3) * 64 + c] = acc[o][3];
-        }
+        for (int o = 0; o < 27; ++o) T4[o * 64 + c] = make_float4(acc[o][0], acc[o][1], acc[o][2], acc[o][3]);
         __syncthreads();
         for (int n = c; n < TILE_NODES; n += P2GC_T) {
             const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
-            float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int zz = max(0, nz - 3); zz <= min(2, nz); ++zz)
-                for (int yy = max(0, ny - 3); yy <= min(2, ny); ++yy)
-                    for (int xx = max(0, nx - 3); xx <= min(2, nx); ++xx) {
-                        const int cc = (nx - xx) + 4 * (ny - yy) + 16 * (nz - zz);
-                        const int o = xx + 3 * yy + 9 * zz;
-                        a4.x += T[(o * 4 + 0) * 64 + cc];
-                        a4.y += T[(o * 4 + 1) * 64 + cc];
-                        a4.z += T[(o * 4 + 2) * 64 + cc];
-                        a4.w += T[(o * 4 + 3) * 64 + cc];
-                    }
+            const float4 a4 = tile_node_sum(T4, nx, ny, nz);
             const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
             const bool any = MODE == MODE_ADJ ? (a4.y != 0.f || a4.z != 0.f || a4.w != 0.f) : a4.x != 0.f;
             if (any && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
@@ -861,30 +879,7 @@ __global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
         __syncthreads();
         for (int n = threadIdx.x; n < TILE_NODES; n += P2GP_T) {
             const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
-            // bit d of vx: cell x = nx - d is inside the tile (0..3); same for y, z
-            const uint32_t vx = (nx <= 3 ? 1u : 0u) | (nx >= 1 && nx <= 4 ? 2u : 0u) | (nx >= 2 ? 4u : 0u);
-            const uint32_t vy = (ny <= 3 ? 1u : 0u) | (ny >= 1 && ny <= 4 ? 2u : 0u) | (ny >= 2 ? 4u : 0u);
-            const uint32_t vz = (nz <= 3 ? 1u : 0u) | (nz >= 1 && nz <= 4 ? 2u : 0u) | (nz >= 2 ? 4u : 0u);
-            const int cn = nx + 4 * ny + 16 * nz;
-            float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int zz = 0; zz < 3; ++zz)
-#pragma unroll
-                for (int yy = 0; yy < 3; ++yy)
-#pragma unroll
-                    for (int xx = 0; xx < 3; ++xx) {
-                        const bool valid = ((vx >> xx) & (vy >> yy) & (vz >> zz) & 1u) != 0u;
-                        // cell n - o when it is in the tile, else slot 0 (read, not added):
-                        // the address stays inside the table either way
-                        const int cell = valid ? cn - (xx + 4 * yy + 16 * zz) : 0;
-                        const float4 t = T4[(xx + 3 * yy + 9 * zz) * 64 + cell];
-                        if (valid) {
-                            a4.x += t.x;
-                            a4.y += t.y;
-                            a4.z += t.z;
-                            a4.w += t.w;
-                        }
-                    }
+            const float4 a4 = tile_node_sum(T4, nx, ny, nz);
             const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
             if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
                 atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
