@@ -88,14 +88,14 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 def kernel_launches_per_step(scenes, n_particles):
     """Our kernels per step: the sort, then P2G, the grid update and G2P.
-    The solver sorts with the bin sort (6 kernels: count, 3-kernel scan of
+    The solver sorts with the bin sort (5 kernels: count, 2-kernel scan of
     the tile counts, cell offsets + node tiles, scatter) when the grids hold
     at most about 8 cells per particle, else with the radix sort (3 kernels
     per 8-bit pass + the tile marking)."""
     cells = sum(((int(s.n[0]) - 3) // 4 + 1) * ((int(s.n[1]) - 3) // 4 + 1) * ((int(s.n[2]) - 3) // 4 + 1)
                 for s in scenes) * 64
     if cells <= 8 * max(n_particles, 1) + (1 << 20):
-        return 6 + 3
+        return 5 + 3
     bits = max(1, int(np.ceil(np.log2(max(2, cells)))))
     passes = (bits + 7) // 8
     return 3 * passes + 1 + 3

@@ -620,11 +620,17 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
     // per thread.
     const uint32_t S = ntiles ? min(4u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
     const uint32_t nwork = ntiles * S;
+    // with at least two work items per block, the next one is claimed while
+    // this one runs (thread 0 holds it); with fewer, claiming early would
+    // leave blocks idle, so it is claimed at the end of the item
+    const bool early = nwork >= 2u * gridDim.x;
+    uint32_t next_work = 0;
+    if (c == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
     for (;;) {
-        if (c == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
         __syncthreads();
         const uint32_t w = s_work;
         if (w >= nwork) break;
+        if (early && c == 0) next_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
         const uint32_t wt = w / S, slice = w - wt * S;
         const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];  // largest tiles first
         const uint2 rg = V.ctile_range[ct];
@@ -774,6 +780,7 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
                 atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
         }
         __syncthreads();
+        if (c == 0) s_work = early ? next_work : atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
@@ -797,11 +804,17 @@ __global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
     // slices of a cell's run when tiles are few (see k_p2g_cells)
     const uint32_t S = ntiles ? min(4u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
     const uint32_t nwork = ntiles * S;
+    // with at least two work items per block, the next one is claimed while
+    // this one runs (thread 0 holds it); with fewer, claiming early would
+    // leave blocks idle, so it is claimed at the end of the item
+    const bool early = nwork >= 2u * gridDim.x;
+    uint32_t next_work = 0;
+    if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
     for (;;) {
-        if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
         __syncthreads();
         const uint32_t w = s_work;
         if (w >= nwork) break;
+        if (early && threadIdx.x == 0) next_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
         const uint32_t wt = w / S, slice = w - wt * S;
         const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];
         const uint2 rg = V.ctile_range[ct];
@@ -885,6 +898,7 @@ __global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
                 atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
         }
         __syncthreads();
+        if (threadIdx.x == 0) s_work = early ? next_work : atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }

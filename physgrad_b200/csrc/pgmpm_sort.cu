@@ -207,8 +207,9 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
 //                physical order stays close to cell order) share one atomic:
 //                the run's first lane adds the run length.  8 keys per thread
 //                with their loads and atomics issued back to back.
-//   bs_reduce / bs_top / bs_down
-//                exclusive scan of the tile counts; bs_down also emits each
+//   bs_reduce / bs_down
+//                exclusive scan of the tile counts (block totals, then each
+//                block adds the totals before it); bs_down also emits each
 //                occupied tile (sorted range, entry in the occupied-tile
 //                list, rank in its size class) and clears the tile counters
 //                it read.
@@ -288,19 +289,6 @@ __global__ void __launch_bounds__(BS_SCAN) bs_reduce(const uint32_t* __restrict_
     if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(BS_SCAN) bs_top(uint32_t* __restrict__ bsum, int nb) {
-    __shared__ uint32_t sh[32];
-    uint32_t carry = 0;
-    for (int b0 = 0; b0 < nb; b0 += BS_SCAN) {
-        const int b = b0 + threadIdx.x;
-        const uint32_t v = b < nb ? bsum[b] : 0u;
-        uint32_t tot;
-        const uint32_t ex = block_excl_scan(v, sh, tot);
-        if (b < nb) bsum[b] = carry + ex;
-        carry += tot;
-    }
-}
-
 // Warp-aggregated append of `item` (lanes with want) to list / counter;
 // returns the slot written (meaningful where want).
 __device__ __forceinline__ uint32_t bs_append(uint32_t* list, uint32_t* counter, bool want, uint32_t item,
@@ -329,10 +317,15 @@ __global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict_
                                                    uint32_t* __restrict__ tile_rank) {
     __shared__ uint32_t sh[32];
     const int lane = threadIdx.x & 31;
+    // this block's first position: the tile totals of the blocks before it
+    uint32_t part = 0u;
+    for (uint32_t b = threadIdx.x; b < blockIdx.x; b += BS_SCAN) part += bsum[b];
+    uint32_t base;
+    block_excl_scan(part, sh, base);
     const int64_t t = (int64_t)blockIdx.x * BS_SCAN + threadIdx.x;
     const uint32_t c = t < n ? tcount[t] : 0u;
     uint32_t tot;
-    const uint32_t ex = block_excl_scan(c, sh, tot) + bsum[blockIdx.x];
+    const uint32_t ex = block_excl_scan(c, sh, tot) + base;
     if (t < n) {
         toff[t] = ex;
         tcount[t] = 0u;  // left clear for the next step
@@ -456,7 +449,6 @@ cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cuda
     const int gk = (int)((n + BS_TILE - 1) / BS_TILE);
     bs_count<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.ccount, B.tcount, B.slot, V.counters);
     bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, ntb, B.bsum);
-    bs_top<<<1, BS_SCAN, 0, st>>>(B.bsum, nb);
     bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, B.bsum, B.toff, B.ccount + ncells,
                                     B.ptile_list ? B.tile_rank : nullptr);
     const int cell_blocks = num_sms * 2;
