@@ -944,10 +944,18 @@ __global__ void k_grid(View V) {
         V.grid_v[idx] = make_float4(v[0], v[1], v[2], mp.x);
         V.grid_mp[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    unsigned long long a = active;
+    // active node count: warp sums, then one atomic per block (a single
+    // counter word takes every block's add)
+    __shared__ uint32_t s_active;
+    if (threadIdx.x == 0) s_active = 0u;
+    __syncthreads();
+    uint32_t a = active;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, o);
-    if ((threadIdx.x & 31) == 0 && a) atomicAdd(reinterpret_cast<unsigned long long*>(&V.counters[CNT_ACTIVE]), a);
+    if ((threadIdx.x & 31) == 0 && a) atomicAdd(&s_active, a);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_active)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&V.counters[CNT_ACTIVE]), (unsigned long long)s_active);
 }
 
 // ------------------------------------------------------------------- G2P
