@@ -186,8 +186,12 @@ PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, i
  * 1: per-particle shared-memory atomics over chunks of ppt particles;
  * 2: one thread per cell with 108 register accumulators;
  * 3: variant 2 with each cell's accumulators split over two lanes (MLS
- * forward; p2g_tiles_per_sm capped at 5).  pgmpm_create picks 3 for MLS
- * solvers of at least 2^20 particles, 2 otherwise.
+ * forward; p2g_tiles_per_sm capped at 5);
+ * 4: variant 3's lane pairs walking equal runs of each tile's sorted
+ * particles instead of one cell each, cells shared by runs merged in shared
+ * memory (MLS forward with the bin sort; with the radix step sort it runs
+ * variant 3).  pgmpm_create picks 4 for MLS solvers that use the bin sort,
+ * else 3 from 2^20 particles and 2 below; REF_COMPAT runs variant 2 for 2-4.
  * g2p_variant 0: tile-staged gather (g2p_tiles_per_sm blocks per SM);
  * 1: direct gather in sorted order; 2: direct gather in physical order.
  * Negative keeps a value. */

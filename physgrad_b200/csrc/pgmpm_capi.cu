@@ -325,12 +325,16 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->ctile_range, sizeof(uint2) * (size_t)ct_base);
     AL(s->counters, sizeof(uint32_t) * CNT_WORDS);
 #undef AL
-    // P2G: two lanes per cell pays off when the occupied tiles outnumber the
-    // resident blocks (many particles); one lane per cell otherwise
-    s->tune.p2g_variant = s->pf.physics == PHYS_MLS && N >= (int64_t)1 << 20 ? 3 : 2;
     // the bin sort keeps 8 bytes per cell: default for grids with at most ~8
     // cells per particle, the radix sort (O(N) per pass) for sparser ones
     s->tune.step_sort = (int64_t)ct_base * 64 <= 8 * std::max<int64_t>(N, 1) + (1 << 20) ? 0 : 1;
+    // P2G (MLS): balanced particle runs over the bin sort's cell table;
+    // without it, two lanes per cell pays off when the occupied tiles
+    // outnumber the resident blocks (many particles), one lane otherwise
+    s->tune.p2g_variant = s->pf.physics != PHYS_MLS ? 2
+                          : s->tune.step_sort == 0  ? 4
+                          : N >= (int64_t)1 << 20   ? 3
+                                                    : 2;
     if (e == cudaSuccess && s->tune.step_sort == 0 && alloc_bin_sort(s) != PGMPM_OK) e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = cudaMemcpy(s->d_scenes.p, s->scenes.data(), sizeof(SceneDev) * n_scenes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice);
@@ -554,14 +558,14 @@ int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p
 int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant, int32_t p2g_tiles_per_sm,
                               int32_t g2p_tiles_per_sm) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
-    if (p2g_variant > 3 || g2p_variant > 2 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
-        return fail(PGMPM_ERR_ARG, "p2g_variant 0..3, g2p_variant 0..2; blocks per SM at most 16");
+    if (p2g_variant > 4 || g2p_variant > 2 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
+        return fail(PGMPM_ERR_ARG, "p2g_variant 0..4, g2p_variant 0..2; blocks per SM at most 16");
     if (p2g_variant >= 0) s->tune.p2g_variant = p2g_variant;
     if (g2p_variant >= 0) s->tune.g2p_variant = g2p_variant;
     if (p2g_tiles_per_sm > 0) {
         if (s->tune.p2g_variant == 2)
             s->tune.cell_blocks_per_sm = p2g_tiles_per_sm;
-        else if (s->tune.p2g_variant == 3)
+        else if (s->tune.p2g_variant >= 3)
             s->tune.pair_blocks_per_sm = std::min(p2g_tiles_per_sm, 5);
         else
             s->tune.tile_blocks_per_sm = p2g_tiles_per_sm;
@@ -600,7 +604,7 @@ int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out) {
     s->met.p2g_variant = s->tune.p2g_variant;
     s->met.g2p_variant = s->tune.g2p_variant;
     s->met.p2g_tiles_per_sm = s->tune.p2g_variant == 2   ? s->tune.cell_blocks_per_sm
-                              : s->tune.p2g_variant == 3 ? s->tune.pair_blocks_per_sm
+                              : s->tune.p2g_variant >= 3 ? s->tune.pair_blocks_per_sm
                                                          : s->tune.tile_blocks_per_sm;
     s->met.g2p_tiles_per_sm = s->tune.g2p_tiles_per_sm;
     *out = s->met;
@@ -629,7 +633,7 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
     struct Cand {
         int variant, block, ppt, tiles_per_sm;
     };
-    const Cand p2g_c[] = {{3, 128, 0, 4}, {3, 128, 0, 5}, {2, 64, 0, 4}, {2, 64, 0, 6}, {2, 64, 0, 8},
+    const Cand p2g_c[] = {{4, 128, 0, 4}, {4, 128, 0, 5}, {3, 128, 0, 4}, {3, 128, 0, 5}, {2, 64, 0, 4}, {2, 64, 0, 6}, {2, 64, 0, 8},
                           {0, 192, 0, 2}, {0, 192, 0, 3}, {1, 256, 512, 0}, {1, 256, 1024, 0}};
     const Cand g2p_c[] = {{2, 128, 0, 0}, {2, 256, 0, 0}, {2, 512, 0, 0}, {0, 256, 0, 2},
                           {1, 128, 0, 0}, {1, 256, 0, 0}};
@@ -657,7 +661,7 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
             t.tile_blocks_per_sm = c.tiles_per_sm;
         } else if (c.variant == 2) {
             t.cell_blocks_per_sm = c.tiles_per_sm;
-        } else if (c.variant == 3) {
+        } else if (c.variant >= 3) {
             t.pair_blocks_per_sm = c.tiles_per_sm;
         } else {
             t.p2g_block = c.block;

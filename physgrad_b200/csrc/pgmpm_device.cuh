@@ -391,6 +391,21 @@ __device__ __forceinline__ void mls_payload(const SceneDev& sc, const MatDev& mt
     p3 = make_float4(Ad[8], f[0], f[1], f[2]);
 }
 
+// The whole payload of one particle from its 4 planes (see mls_payload).
+__device__ __forceinline__ void unpack_payload(const float4& p0, const float4& p1, const float4& p2, const float4& p3,
+                                               float& m, float b[3], float Ad[9], float f[3]) {
+    m = p0.w;
+    b[0] = p0.x;
+    b[1] = p0.y;
+    b[2] = p0.z;
+    Ad[0] = p1.x; Ad[1] = p1.y; Ad[2] = p1.z; Ad[3] = p1.w;
+    Ad[4] = p2.x; Ad[5] = p2.y; Ad[6] = p2.z; Ad[7] = p2.w;
+    Ad[8] = p3.x;
+    f[0] = p3.y;
+    f[1] = p3.z;
+    f[2] = p3.w;
+}
+
 // ----------------------------------------------------------- grid update
 __device__ __forceinline__ bool in_wall(const SceneDev& sc, int a, int idx, int& side) {
     if (idx < sc.bthick) { side = -1; return true; }

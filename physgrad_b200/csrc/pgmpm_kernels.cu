@@ -396,11 +396,12 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g_tiles(View V, AdjView AV) {
                 } else if (PHYS == PHYS_MLS) {
                     // precomputed payload (G2P of the previous step / k_payload)
                     const float4 a0 = V.pay[p], a1 = V.pay[N + p], a2 = V.pay[2 * N + p], a3 = V.pay[3 * N + p];
-                    sm[PAY_M * P2G_SC + j] = a0.w;
-                    sm[(PAY_B + 0) * P2G_SC + j] = a0.x;
-                    sm[(PAY_B + 1) * P2G_SC + j] = a0.y;
-                    sm[(PAY_B + 2) * P2G_SC + j] = a0.z;
-                    const float Ad[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+                    float m, b[3], Ad[9], f[3];
+                    unpack_payload(a0, a1, a2, a3, m, b, Ad, f);
+                    sm[PAY_M * P2G_SC + j] = m;
+                    sm[(PAY_B + 0) * P2G_SC + j] = b[0];
+                    sm[(PAY_B + 1) * P2G_SC + j] = b[1];
+                    sm[(PAY_B + 2) * P2G_SC + j] = b[2];
 #pragma unroll
                     for (int a = 0; a < 9; ++a) sm[(PAY_A + a) * P2G_SC + j] = Ad[a];
                 } else {
@@ -675,16 +676,7 @@ __global__ void __launch_bounds__(P2GC_T, 6) k_p2g_cells(View V, AdjView AV) {
             if (MODE == MODE_MLS) {
                 // precomputed payload (G2P of the previous step / k_payload)
                 const float4 a0 = V.pay[p], a1 = V.pay[N + p], a2 = V.pay[2 * N + p], a3 = V.pay[3 * N + p];
-                m = a0.w;
-                b[0] = a0.x;
-                b[1] = a0.y;
-                b[2] = a0.z;
-                Ad[0] = a1.x; Ad[1] = a1.y; Ad[2] = a1.z; Ad[3] = a1.w;
-                Ad[4] = a2.x; Ad[5] = a2.y; Ad[6] = a2.z; Ad[7] = a2.w;
-                Ad[8] = a3.x;
-                st.f[0] = a3.y;
-                st.f[1] = a3.z;
-                st.f[2] = a3.w;
+                unpack_payload(a0, a1, a2, a3, m, b, Ad, st.f);
 #pragma unroll
                 for (int a = 0; a < 3; ++a) mls_weights(st.f[a], st.w[a]);
             } else if (MODE == MODE_ADJ) {
@@ -891,6 +883,195 @@ __global__ void __launch_bounds__(P2GP_T, 5) k_p2g_pairs(View V) {
             reinterpret_cast<float2*>(&T4[o * 64 + c])[h] = make_float2(accA[o], accB[o]);
         __syncthreads();
         for (int n = threadIdx.x; n < TILE_NODES; n += P2GP_T) {
+            const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            const float4 a4 = tile_node_sum(T4, nx, ny, nz);
+            const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
+            if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_work = early ? next_work : atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+// ------------------------------------ P2G, balanced particle runs (MLS)
+// Variant 4: variant 3's lane pairs and accumulators, with the work split by
+// particles instead of by cells.  A work item's sorted particles (a tile, or
+// a slice of one) are cut into 4 warp parts at the cell boundaries nearest
+// the quarter points, and each warp cuts its part into 16 equal runs, one per
+// lane pair.  A pair walks its run in key order; when it passes the last
+// particle of a cell it owns that cell and writes the cell's 27 node sums to
+// the flush table (one writer per cell).  A run that ends inside a cell
+// leaves a partial sum: after the walk, a segmented scan over the warp's
+// pairs (shuffles) gathers each cell's partials into the last of them, which
+// adds them to the owner's entry.  Warp parts end at cell boundaries, so a
+// cell never spans two warps.  A tile's longest walk is then about its
+// particle count / 64 instead of its fullest cell's count.  Needs the sort's
+// cell table (contiguous ranges of the tile's 64 cells).
+constexpr int P2GR_T = 128;
+
+__device__ __forceinline__ void runs_store(float4* T4, uint32_t c, int h, const float* accA, const float* accB) {
+#pragma unroll
+    for (int o = 0; o < 27; ++o) reinterpret_cast<float2*>(&T4[o * 64 + c])[h] = make_float2(accA[o], accB[o]);
+}
+
+__global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
+    __shared__ float4 T4[27 * 64];                // [offset o][cell]: the 4 channels of cell's node o
+    __shared__ uint32_t s_end[P2GR_T / 32][64];   // per warp: end of each cell's range in the item
+    __shared__ uint32_t s_work;
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int q = lane >> 1, h = lane & 1;
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    uint32_t* const wend = s_end[wp];
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    // slices of a tile's particles when tiles are few (see k_p2g_cells)
+    const uint32_t S = ntiles ? min(4u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
+    const uint32_t nwork = ntiles * S;
+    const bool early = nwork >= 2u * gridDim.x;
+    uint32_t next_work = 0;
+    if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+    for (;;) {
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= nwork) break;
+        if (early && threadIdx.x == 0) next_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+        const uint32_t wt = w / S, slice = w - wt * S;
+        const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        // the item's particles [lo, hi) and its cells' ranges clamped to them
+        // (lane holds cells lane and lane + 32)
+        const uint32_t P = rg.y > rg.x ? rg.y - rg.x : 0u;
+        const uint32_t lo = rg.x + (uint32_t)(((uint64_t)P * slice) / S);
+        const uint32_t hi = rg.x + (uint32_t)(((uint64_t)P * (slice + 1)) / S);
+        const uint2 r0 = V.cell_range[(size_t)ct * 64 + lane], r1 = V.cell_range[(size_t)ct * 64 + 32 + lane];
+        const uint32_t s0 = min(max(r0.x, lo), hi), s1 = min(max(r1.x, lo), hi);
+        const uint32_t e0 = min(max(r0.y, lo), hi), e1 = min(max(r1.y, lo), hi);
+        if ((lane == 0 && s0 != lo) || (lane == 31 && e1 != hi)) flags |= FLAG_TILE_RANGE;
+        wend[lane] = e0;
+        wend[lane + 32] = e1;
+        // warp part [b0, b1): the cell starts nearest the quarter points
+        auto bound = [&](int k) -> uint32_t {
+            if (k == 0) return lo;
+            if (k == 4) return hi;
+            const uint32_t t = lo + (uint32_t)(((uint64_t)(hi - lo) * (uint32_t)k) / 4u);
+            const uint32_t a = __reduce_max_sync(FULL, max(s0 <= t ? s0 : lo, s1 <= t ? s1 : lo));
+            const uint32_t b = __reduce_min_sync(FULL, min(s0 >= t ? s0 : hi, s1 >= t ? s1 : hi));
+            return t - a <= b - t ? a : b;
+        };
+        const uint32_t b0 = bound(wp), b1 = max(bound(wp + 1), b0);
+        const uint32_t len = (b1 - b0 + 15u) >> 4;
+        const uint32_t i0 = min(b0 + (uint32_t)q * len, b1), i1 = min(i0 + len, b1);
+        __syncwarp();
+        // cells without particles in the item get a zero entry (warp wp: cells
+        // 16 wp .. 16 wp + 15, the half-warps take alternate offsets)
+        {
+            const int zc = 16 * wp + (lane & 15);
+            const uint32_t zs = zc == 0 ? lo : wend[zc - 1];
+            if (wend[zc] == zs)
+                for (int o = lane >> 4; o < 27; o += 2) T4[o * 64 + zc] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        float accA[27], accB[27];
+#pragma unroll
+        for (int o = 0; o < 27; ++o) accA[o] = accB[o] = 0.f;
+        // the cell of particle i0: the first cell whose range ends after it
+        uint32_t c = 0, cend = 0;
+        if (i0 < i1) {
+            uint32_t l = 0, r = 63;
+            while (l < r) {
+                const uint32_t m = (l + r) >> 1;
+                if (wend[m] > i0) r = m; else l = m + 1;
+            }
+            c = l;
+            cend = wend[c];
+        }
+        for (uint32_t i = i0; i < i1; ++i) {
+            if (i == cend) {
+                // the run passed the last particle of cell c: its sums are final
+                runs_store(T4, c, h, accA, accB);
+#pragma unroll
+                for (int o = 0; o < 27; ++o) accA[o] = accB[o] = 0.f;
+                while (c < 63) {  // next cell with particles (c stays a cell index)
+                    ++c;
+                    if (wend[c] > i) break;
+                }
+                cend = wend[c];
+            }
+            const uint32_t p = V.order[i];
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            const float4 a0 = V.pay[p], a1 = V.pay[N + p], a2 = V.pay[2 * N + p], a3 = V.pay[3 * N + p];
+            // channels as in k_p2g_pairs (lane 0: m, p_x; lane 1: p_y, p_z)
+            const float bA = h ? a0.y : a0.w, bB = h ? a0.z : a0.x;
+            const float gAx = h ? a1.w : 0.f, gAy = h ? a2.x : 0.f, gAz = h ? a2.y : 0.f;
+            const float gBx = h ? a2.z : a1.x, gBy = h ? a2.w : a1.y, gBz = h ? a3.x : a1.z;
+            float wt[3][3];
+            mls_weights(a3.y, wt[0]);
+            mls_weights(a3.z, wt[1]);
+            mls_weights(a3.w, wt[2]);
+#pragma unroll
+            for (int zz = 0; zz < 3; ++zz) {
+                const float zA = bA + gAz * (float)zz, zB = bB + gBz * (float)zz;
+#pragma unroll
+                for (int yy = 0; yy < 3; ++yy) {
+                    const float wyz = wt[1][yy] * wt[2][zz];
+                    float vA = zA + gAy * (float)yy, vB = zB + gBy * (float)yy;
+#pragma unroll
+                    for (int xx = 0; xx < 3; ++xx) {
+                        const int o = xx + 3 * yy + 9 * zz;
+                        const float wgt = wt[0][xx] * wyz;
+                        accA[o] += wgt * vA;
+                        accB[o] += wgt * vB;
+                        vA += gAx;
+                        vB += gBx;
+                    }
+                }
+            }
+        }
+        // a run that ends where its cell ends owns that cell; otherwise the
+        // cell's owner is a later pair of this warp and the sum is partial
+        const bool open = i0 < i1 && i1 != cend;
+        if (i0 < i1 && !open) runs_store(T4, c, h, accA, accB);
+        __syncwarp();
+        // segmented inclusive scan of the partial sums over consecutive pairs
+        // of the same cell; the last pair of a segment then holds its total
+        const uint32_t key = open ? c : FULL;
+        const uint32_t pkey = __shfl_up_sync(FULL, key, 2), nkey = __shfl_down_sync(FULL, key, 2);
+        const bool head = open && (q == 0 || pkey != key);
+        const uint32_t heads = __ballot_sync(FULL, head && h == 0);
+        const int dist = open ? q - ((31 - __clz(heads & (FULL >> (31 - lane)))) >> 1) : 0;
+        const int maxd = __reduce_max_sync(FULL, dist);
+        for (int d = 1; d <= maxd; d <<= 1) {
+            const bool take = dist >= d;
+#pragma unroll
+            for (int o = 0; o < 27; ++o) {
+                const float a = __shfl_up_sync(FULL, accA[o], 2 * d);
+                const float b = __shfl_up_sync(FULL, accB[o], 2 * d);
+                if (take) {
+                    accA[o] += a;
+                    accB[o] += b;
+                }
+            }
+        }
+        if (open && (q == 15 || nkey != key)) {
+#pragma unroll
+            for (int o = 0; o < 27; ++o) {
+                float2* t = reinterpret_cast<float2*>(&T4[o * 64 + c]) + h;
+                const float2 v = *t;
+                *t = make_float2(v.x + accA[o], v.y + accB[o]);
+            }
+        }
+        __syncthreads();
+        for (int n = threadIdx.x; n < TILE_NODES; n += P2GR_T) {
             const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
             const float4 a4 = tile_node_sum(T4, nx, ny, nz);
             const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
@@ -1315,7 +1496,7 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
                                cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
-    if (t.p2g_variant == 2 || t.p2g_variant == 3) {  // the adjoint scatter of variant 3 is variant 2's
+    if (t.p2g_variant >= 2) {  // the adjoint scatter of variants 3 and 4 is variant 2's
         const int nb = num_sms * t.cell_blocks_per_sm;
         if (pf.multi_mat) {
             if (pf.has_fluid)
@@ -1347,12 +1528,15 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
 
 cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
-    if (t.p2g_variant == 3 && pf.physics == PHYS_MLS) {
+    if (t.p2g_variant >= 3 && pf.physics == PHYS_MLS) {
         if (!V.pay) return cudaErrorInvalidValue;
-        k_p2g_pairs<<<num_sms * t.pair_blocks_per_sm, P2GP_T, 0, st>>>(V);
+        if (t.p2g_variant == 4 && V.cell_range)  // without the sort's cell table: variant 3
+            k_p2g_runs<<<num_sms * t.pair_blocks_per_sm, P2GR_T, 0, st>>>(V);
+        else
+            k_p2g_pairs<<<num_sms * t.pair_blocks_per_sm, P2GP_T, 0, st>>>(V);
         return cudaGetLastError();
     }
-    if (t.p2g_variant == 2 || t.p2g_variant == 3) {  // REF physics: variant 3 runs variant 2
+    if (t.p2g_variant >= 2) {  // REF physics: variants 3 and 4 run variant 2
         const int nb = num_sms * t.cell_blocks_per_sm;
         const AdjView none{};
         if (pf.physics == PHYS_MLS) {

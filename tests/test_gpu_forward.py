@@ -232,10 +232,10 @@ def test_mls_grid_download_matches_oracle(gpu, oracle):
 
 
 # --------------------------------------------------------- batching / misc
-@pytest.mark.parametrize("p2g_variant", [2, 3])
+@pytest.mark.parametrize("p2g_variant", [2, 3, 4])
 def test_batched_scenes_equal_single_scenes(gpu, p2g_variant):
     """One batched solver over scenes of uneven sizes and grids gives each
-    scene's single-scene result (both per-cell P2G kernels)."""
+    scene's single-scene result (the per-cell and balanced-run P2G kernels)."""
     from physgrad_b200 import workloads as W
 
     scenes, counts, mats, st, _ = W.batched_scenes(n_scenes=5, lo=500, hi=20000, seed=6, v_sigma=0.3)
@@ -257,7 +257,7 @@ def test_batched_scenes_equal_single_scenes(gpu, p2g_variant):
         off += c
 
 
-@pytest.mark.parametrize("p2g_variant,g2p_variant", [(0, 0), (1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (2, 2), (0, 2), (3, 2), (3, 0)])
+@pytest.mark.parametrize("p2g_variant,g2p_variant", [(0, 0), (1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (2, 2), (0, 2), (3, 2), (3, 0), (4, 2), (4, 0)])
 @pytest.mark.parametrize("physics", [0, 1])
 def test_kernel_variants_agree(gpu, oracle, p2g_variant, g2p_variant, physics):
     """Every P2G/G2P variant matches the checkers (MLS: FP64 oracle; REF:
@@ -285,6 +285,51 @@ def test_kernel_variants_agree(gpu, oracle, p2g_variant, g2p_variant, physics):
         assert ex <= 1e-6 and ev <= 1e-4, (ex, ev)
 
 
+@pytest.mark.parametrize("case", ["many_tiles", "dense_cell", "radix_sort"])
+def test_balanced_runs_match_cells(gpu, case):
+    """P2G variant 4 (tile particles split into equal runs, cells shared by
+    runs merged by a segmented scan) against variant 2 (one thread per
+    cell): tiles processed whole (more tiles than resident blocks), one cell
+    holding thousands of particles (its run spans many lane pairs), and the
+    radix step sort (no cell table: variant 3 runs instead)."""
+    from physgrad_b200 import _capi as C
+    from physgrad_b200 import workloads as W
+
+    if case == "many_tiles":
+        scenes, counts, mats, st, _ = W.two_material_drop(n_particles=600000, n=128, seed=5)
+    else:
+        scenes, counts, mats, st, _ = W.elastic_cube(n_particles=20000, n=32, v_sigma=0.3, seed=13)
+        if case == "dense_cell":
+            rng = np.random.default_rng(13)
+            k = 3000
+            dx = float(scenes[0].dx)
+            xc = ((np.array([15, 16, 14]) + 0.5 + rng.random((k, 3))) * dx).astype(np.float32)
+            st = dict(st)
+            st["x"] = np.concatenate([st["x"], xc])
+            st["v"] = np.concatenate([st["v"], (0.1 * rng.standard_normal((k, 3))).astype(np.float32)])
+            for key in ("m", "V0"):
+                st[key] = np.concatenate([st[key], np.full(k, st[key][0], np.float32)])
+            for key in ("C", "F"):
+                if st.get(key) is not None:
+                    st[key] = np.concatenate([st[key], np.repeat(st[key][:1], k, axis=0)])
+            if st.get("mat") is not None:
+                st["mat"] = np.concatenate([st["mat"], np.zeros(k, st["mat"].dtype)])
+            counts = [counts[0] + k]
+    out = {}
+    for variant in (2, 4):
+        sim = _sim(gpu, scenes, counts, mats, st)
+        sim.set_variants(p2g_variant=variant)
+        if case == "radix_sort":
+            sim.set_step_sort(C.SORT_RADIX)
+        sim.step(10)
+        assert sim.status() == 0
+        out[variant] = sim.download()
+    a, b = out[2], out[4]
+    assert np.abs(a["x"] - b["x"]).max() <= 1e-6
+    assert np.abs(a["v"] - b["v"]).max() <= 1e-4 * (np.abs(a["v"]).max() + 1e-3)
+    assert np.abs(a["F"] - b["F"]).max() <= 1e-5
+
+
 def test_graph_and_eager_agree(gpu):
     from physgrad_b200 import workloads as W
 
@@ -309,7 +354,7 @@ def test_autotune_restores_state(gpu):
     after = sim.download()
     for k in ("x", "v", "C", "F"):
         assert np.array_equal(before[k], after[k])
-    assert best["p2g_variant"] in (0, 1, 2, 3) and best["g2p_variant"] in (0, 1, 2)
+    assert best["p2g_variant"] in (0, 1, 2, 3, 4) and best["g2p_variant"] in (0, 1, 2)
     ref = _sim(gpu, scenes, counts, mats, st)
     ref.step(5)
     sim.step(2)
