@@ -94,13 +94,15 @@ int refresh_payload(pgmpm_solver s, cudaStream_t st) {
     return PGMPM_OK;
 }
 
-int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) {
+int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc) {
     if (s->N == 0) {  // nothing to move; keep the timing events consistent
         if (timed)
             for (int i = 0; i < 5; ++i) CK(cudaEventRecord(s->ev[i], st));
         return PGMPM_OK;
     }
     View V = s->view_for(b);
+    // P2G variant 1 builds its payload from the state's v and C
+    V.write_vc = write_vc || s->pf.physics != PHYS_MLS || s->tune.p2g_variant == 1 ? 1 : 0;
     // per-step resets: tile counts, active node count, work cursors, and the
     // active node tile flags (the bin sort writes every flag itself)
     if (s->tune.step_sort != 0) CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
@@ -142,10 +144,17 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed) 
 
 namespace {
 
-int build_graph(pgmpm_solver s) {
-    s->drop_graph();
+// The step graph (mid = false) or the graph of a step that another step of
+// the same call follows (mid = true: v and C are not stored).
+int build_graph(pgmpm_solver s, bool mid) {
+    cudaGraph_t& graph = mid ? s->step_graph_mid : s->step_graph;
+    cudaGraphExec_t& exec = mid ? s->step_exec_mid : s->step_exec;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
     CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
-    int rc = record_step(s, s->live_bufs(), s->cap_stream, false);
+    int rc = record_step(s, s->live_bufs(), s->cap_stream, false, !mid);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
     if (rc != PGMPM_OK) {
@@ -153,8 +162,8 @@ int build_graph(pgmpm_solver s) {
         return rc;
     }
     CK(e);
-    s->step_graph = g;
-    CK(cudaGraphInstantiate(&s->step_exec, g, 0));
+    graph = g;
+    CK(cudaGraphInstantiate(&exec, g, 0));
     return PGMPM_OK;
 }
 
@@ -182,13 +191,14 @@ int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
                 (s->met.average_step_ms * s->met.total_steps + s->met.last_step_ms) / (s->met.total_steps + 1);
             s->met.particle_steps_per_s = s->met.average_step_ms > 0 ? s->N / (s->met.average_step_ms * 1e-3) : 0;
         } else if (s->use_graph) {
-            if (!s->step_exec) {
-                int rc = build_graph(s);
+            const bool mid = k + 1 < n_steps;
+            if (!(mid ? s->step_exec_mid : s->step_exec)) {
+                int rc = build_graph(s, mid);
                 if (rc) return rc;
             }
-            CK(cudaGraphLaunch(s->step_exec, st));
+            CK(cudaGraphLaunch(mid ? s->step_exec_mid : s->step_exec, st));
         } else {
-            int rc = record_step(s, s->live_bufs(), st, false);
+            int rc = record_step(s, s->live_bufs(), st, false, k + 1 == n_steps);
             if (rc) return rc;
         }
         s->met.total_steps++;

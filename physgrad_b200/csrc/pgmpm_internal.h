@@ -37,6 +37,8 @@ struct View {
     float4* q_out;             // where G2P writes the new state (== q in place; MLS only otherwise)
     float4* pay;               // MLS P2G payload of the state in q (4 planes), read by P2G
     float4* pay_out;           // payload of the state G2P writes (null: G2P does not write one)
+    int write_vc;              // MLS G2P stores v and C (planes 3-5); 0 between the steps of one
+                               // call, where the next step reads them only through the payload
     const float2* mV;          // (mass, V0)
     const int32_t* mat;        // material id (null when M == 1)
     uint32_t* keys;            // cell key per particle (physical order), input of the next sort

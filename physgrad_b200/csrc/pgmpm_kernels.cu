@@ -1201,6 +1201,14 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
                 C[3 * a + b] = sc.D * dx * (S[3 * a + b] - nv[a] * st.f[b]);
                 M[3 * a + b] = sc.dt * C[3 * a + b] + (a == b ? 1.f : 0.f);
             }
+        float4* qo = V.q_out;
+        if (V.write_vc) {  // else the next step of the call reads v, C from the payload only
+            float4 o3, o4, o5;
+            pack_vC(nv, C, o3, o4, o5);
+            qo[3 * N + p] = o3;
+            qo[4 * N + p] = o4;
+            qo[5 * N + p] = o5;
+        }
         m3_mul(M, F, Fn);
         if (FLUID) {
             const int mid = MULTI ? V.mat[p] : 0;
@@ -1212,16 +1220,11 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) x[a] = x[a] + sc.dt * nv[a];
-        float4 o0, o1, o2, o3, o4, o5;
+        float4 o0, o1, o2;
         pack_xF(x, Fn, o0, o1, o2);
-        pack_vC(nv, C, o3, o4, o5);
-        float4* qo = V.q_out;
         qo[p] = o0;
         qo[N + p] = o1;
         qo[2 * N + p] = o2;
-        qo[3 * N + p] = o3;
-        qo[4 * N + p] = o4;
-        qo[5 * N + p] = o5;
         // key and P2G payload of the new state for the next step
         int so[3];
         float fn[3];

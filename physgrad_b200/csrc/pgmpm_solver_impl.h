@@ -120,8 +120,10 @@ struct pgmpm_solver_s {
 
     // graph
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t step_exec = nullptr;
+    cudaGraphExec_t step_exec = nullptr;      // one step
     cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_exec_mid = nullptr;  // one step followed by another (v, C not stored)
+    cudaGraph_t step_graph_mid = nullptr;
     cudaEvent_t ev[6] = {};
 
     // metrics
@@ -180,6 +182,7 @@ struct pgmpm_solver_s {
         V.q_out = b.q_out;
         V.pay = b.pay;
         V.pay_out = b.pay;
+        V.write_vc = 1;
         V.mV = mV.as<float2>();
         V.mat = pf.multi_mat ? mat.as<int32_t>() : nullptr;
         V.keys = b.keys_out;
@@ -213,8 +216,10 @@ struct pgmpm_solver_s {
     void drop_graph() {
         if (step_exec) cudaGraphExecDestroy(step_exec);
         if (step_graph) cudaGraphDestroy(step_graph);
-        step_exec = nullptr;
-        step_graph = nullptr;
+        if (step_exec_mid) cudaGraphExecDestroy(step_exec_mid);
+        if (step_graph_mid) cudaGraphDestroy(step_graph_mid);
+        step_exec = step_exec_mid = nullptr;
+        step_graph = step_graph_mid = nullptr;
         drop_tape_graphs();
     }
 
@@ -238,7 +243,10 @@ int refresh_payload(pgmpm_solver s, cudaStream_t st);
 // Allocate the bin sort's buffers (8 bytes per cell, counters cleared).
 int alloc_bin_sort(pgmpm_solver s);
 // Enqueue one step on `st` using buffers `b` (events ev[0..4] when timed).
-int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed);
+// write_vc = false lets an MLS step leave v and C (state planes 3-5) unwritten
+// when the next step follows in the same call: that step reads them only
+// through the payload, and the call's last step writes them.
+int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc = true);
 // Run n steps of the live state (graph, eager or profiled).
 int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st);
 }  // namespace pgmpm
