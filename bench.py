@@ -76,7 +76,10 @@ def compulsory_bytes(N, A, multi_mat):
     """What each kernel as split here must move: P2G reads the sorted order
     (4 B) and the payload G2P precomputed (64 B) per particle and adds 16 B
     per active node; G2P reads x, F, (m, V0) (+ material id), writes x, v,
-    C, F, the next key and the next payload, and reads 12 B per node."""
+    C, F, the next key and the next payload, and reads 12 B per node.  The
+    per-kernel times are taken on single-step calls, whose G2P stores v and
+    C; inside a multi-step call (the timed region) the steps before the last
+    leave them unstored, 48 B per particle less."""
     mm = 4 if multi_mat else 0
     return {"p2g": 68 * N + 16 * A, "g2p": (220 + mm) * N + 12 * A, "grid": 28 * A}
 
