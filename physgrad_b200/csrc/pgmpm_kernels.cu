@@ -1084,6 +1084,190 @@ __global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// ------------------------------ adjoint scatter, balanced particle runs
+// Reverse of G2P (the adjoint payload scattered to the grid adjoint) with
+// k_p2g_runs' work split at one lane per run: a particle's adjoint payload
+// takes a whole thread's registers.  A 64-thread block takes a tile (or a
+// slice of one); its two warps take the halves split at the cell boundary
+// nearest the midpoint, and each lane an equal run of its half.  A run
+// stores the sums of each cell whose last particle it passes (one writer
+// per cell); partial sums of runs that end inside a cell are gathered by a
+// segmented scan over the warp's lanes into the last of them, which adds
+// them to the owner's entry.  Against one thread per cell, a tile's longest
+// walk drops from its fullest cell's count to about count/64.
+constexpr int ADJR_T = 64;
+
+__device__ __forceinline__ void adj_runs_store(float4* T4, uint32_t c, const float (*acc)[3]) {
+#pragma unroll
+    for (int o = 0; o < 27; ++o) T4[o * 64 + c] = make_float4(0.f, acc[o][0], acc[o][1], acc[o][2]);
+}
+
+template <bool MULTI, bool FLUID>
+__global__ void __launch_bounds__(ADJR_T, 6) k_adj_runs(View V, AdjView AV) {
+    __shared__ float4 T4[27 * 64];                // [offset o][cell]: (0, adjoint of p) of cell's node o
+    __shared__ uint32_t s_end[ADJR_T / 32][64];   // per warp: end of each cell's range in the item
+    __shared__ uint32_t s_work;
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    uint32_t* const wend = s_end[wp];
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    // slices of a tile's particles when tiles are few (see k_p2g_cells)
+    const uint32_t S = ntiles ? min(4u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
+    const uint32_t nwork = ntiles * S;
+    const bool early = nwork >= 2u * gridDim.x;
+    uint32_t next_work = 0;
+    if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+    for (;;) {
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= nwork) break;
+        if (early && threadIdx.x == 0) next_work = atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+        const uint32_t wt = w / S, slice = w - wt * S;
+        const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        // the item's particles [lo, hi) and its cells' ranges clamped to them
+        // (lane holds cells lane and lane + 32)
+        const uint32_t P = rg.y > rg.x ? rg.y - rg.x : 0u;
+        const uint32_t lo = rg.x + (uint32_t)(((uint64_t)P * slice) / S);
+        const uint32_t hi = rg.x + (uint32_t)(((uint64_t)P * (slice + 1)) / S);
+        const uint2 r0 = V.cell_range[(size_t)ct * 64 + lane], r1 = V.cell_range[(size_t)ct * 64 + 32 + lane];
+        const uint32_t s0 = min(max(r0.x, lo), hi), s1 = min(max(r1.x, lo), hi);
+        const uint32_t e0 = min(max(r0.y, lo), hi), e1 = min(max(r1.y, lo), hi);
+        if ((lane == 0 && s0 != lo) || (lane == 31 && e1 != hi)) flags |= FLAG_TILE_RANGE;
+        wend[lane] = e0;
+        wend[lane + 32] = e1;
+        // warp half [b0, b1): split at the cell start nearest the midpoint
+        uint32_t mid;
+        {
+            const uint32_t t = lo + ((hi - lo) >> 1);
+            const uint32_t a = __reduce_max_sync(FULL, max(s0 <= t ? s0 : lo, s1 <= t ? s1 : lo));
+            const uint32_t b = __reduce_min_sync(FULL, min(s0 >= t ? s0 : hi, s1 >= t ? s1 : hi));
+            mid = t - a <= b - t ? a : b;
+        }
+        const uint32_t b0 = wp == 0 ? lo : mid, b1 = wp == 0 ? mid : hi;
+        const uint32_t len = (b1 - b0 + 31u) >> 5;
+        const uint32_t i0 = min(b0 + (uint32_t)lane * len, b1), i1 = min(i0 + len, b1);
+        __syncwarp();
+        // cells without particles in the item get a zero entry (warp wp:
+        // cells 32 wp .. 32 wp + 31)
+        {
+            const int zc = 32 * wp + lane;
+            const uint32_t zs = zc == 0 ? lo : wend[zc - 1];
+            if (wend[zc] == zs)
+                for (int o = 0; o < 27; ++o) T4[o * 64 + zc] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        float acc[27][3];
+#pragma unroll
+        for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = 0.f;
+        // the cell of particle i0: the first cell whose range ends after it
+        uint32_t c = 0, cend = 0;
+        if (i0 < i1) {
+            uint32_t l = 0, r = 63;
+            while (l < r) {
+                const uint32_t m = (l + r) >> 1;
+                if (wend[m] > i0) r = m; else l = m + 1;
+            }
+            c = l;
+            cend = wend[c];
+        }
+        for (uint32_t i = i0; i < i1; ++i) {
+            if (i == cend) {
+                // the run passed the last particle of cell c: its sums are final
+                adj_runs_store(T4, c, acc);
+#pragma unroll
+                for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = 0.f;
+                while (c < 63) {  // next cell with particles (c stays a cell index)
+                    ++c;
+                    if (wend[c] > i) break;
+                }
+                cend = wend[c];
+            }
+            const uint32_t p = V.order[i];
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            Stencil st;
+            float b[3], Ad[9];
+            adj_payload<MULTI, FLUID>(V, AV, sc, p, st, flags, b, Ad);
+            // node o gets w_o (b + Ad o)
+#pragma unroll
+            for (int zz = 0; zz < 3; ++zz) {
+                const float bz0 = b[0] + Ad[2] * (float)zz, bz1 = b[1] + Ad[5] * (float)zz,
+                            bz2 = b[2] + Ad[8] * (float)zz;
+#pragma unroll
+                for (int yy = 0; yy < 3; ++yy) {
+                    const float wyz = st.w[1][yy] * st.w[2][zz];
+                    float v0 = bz0 + Ad[1] * (float)yy, v1 = bz1 + Ad[4] * (float)yy, v2 = bz2 + Ad[7] * (float)yy;
+#pragma unroll
+                    for (int xx = 0; xx < 3; ++xx) {
+                        const int o = xx + 3 * yy + 9 * zz;
+                        const float wgt = st.w[0][xx] * wyz;
+                        acc[o][0] += wgt * v0;
+                        acc[o][1] += wgt * v1;
+                        acc[o][2] += wgt * v2;
+                        v0 += Ad[0];
+                        v1 += Ad[3];
+                        v2 += Ad[6];
+                    }
+                }
+            }
+        }
+        // a run that ends where its cell ends owns that cell; otherwise the
+        // cell's owner is a later lane of this warp and the sum is partial
+        const bool open = i0 < i1 && i1 != cend;
+        if (i0 < i1 && !open) adj_runs_store(T4, c, acc);
+        __syncwarp();
+        // segmented inclusive scan of the partial sums over consecutive lanes
+        // of the same cell; the last lane of a segment then holds its total
+        const uint32_t key = open ? c : FULL;
+        const uint32_t pkey = __shfl_up_sync(FULL, key, 1), nkey = __shfl_down_sync(FULL, key, 1);
+        const bool head = open && (lane == 0 || pkey != key);
+        const uint32_t heads = __ballot_sync(FULL, head);
+        const int dist = open ? lane - (31 - __clz(heads & (FULL >> (31 - lane)))) : 0;
+        const int maxd = __reduce_max_sync(FULL, dist);
+        for (int d = 1; d <= maxd; d <<= 1) {
+            const bool take = dist >= d;
+#pragma unroll
+            for (int o = 0; o < 27; ++o) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float a = __shfl_up_sync(FULL, acc[o][k], d);
+                    if (take) acc[o][k] += a;
+                }
+            }
+        }
+        if (open && (lane == 31 || nkey != key)) {
+#pragma unroll
+            for (int o = 0; o < 27; ++o) {
+                float4 t = T4[o * 64 + c];
+                t.y += acc[o][0];
+                t.z += acc[o][1];
+                t.w += acc[o][2];
+                T4[o * 64 + c] = t;
+            }
+        }
+        __syncthreads();
+        for (int n = threadIdx.x; n < TILE_NODES; n += ADJR_T) {
+            const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            const float4 a4 = tile_node_sum(T4, nx, ny, nz);
+            const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
+            if ((a4.y != 0.f || a4.z != 0.f || a4.w != 0.f) && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_work = early ? next_work : atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
 // ------------------------------------------------------------ grid update
 template <int PHYS>
 __global__ void k_grid(View V) {
@@ -1499,7 +1683,22 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
                                cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
-    if (t.p2g_variant >= 2) {  // the adjoint scatter of variants 3 and 4 is variant 2's
+    if (t.p2g_variant == 4 && V.cell_range) {  // balanced runs over the sort's cell table
+        const int nb = num_sms * 6;
+        if (pf.multi_mat) {
+            if (pf.has_fluid)
+                k_adj_runs<true, true><<<nb, ADJR_T, 0, st>>>(V, A);
+            else
+                k_adj_runs<true, false><<<nb, ADJR_T, 0, st>>>(V, A);
+        } else {
+            if (pf.has_fluid)
+                k_adj_runs<false, true><<<nb, ADJR_T, 0, st>>>(V, A);
+            else
+                k_adj_runs<false, false><<<nb, ADJR_T, 0, st>>>(V, A);
+        }
+        return cudaGetLastError();
+    }
+    if (t.p2g_variant >= 2) {  // the adjoint scatter of variant 3 (and of 4 without a cell table) is variant 2's
         const int nb = num_sms * t.cell_blocks_per_sm;
         if (pf.multi_mat) {
             if (pf.has_fluid)

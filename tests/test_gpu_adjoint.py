@@ -55,13 +55,14 @@ def test_adjoint_matches_fp64_oracle(gpu, oracle, bc, k):
 
 def test_adjoint_scatter_variants_agree(gpu):
     """The G2P-reverse scatter runs on the P2G kernel variant in use; the
-    (cell, z-slice) and thread-per-cell variants give the same gradients."""
+    (cell, z-slice), thread-per-cell and balanced-run (variant 4) scatters
+    give the same gradients."""
     from physgrad_b200 import workloads as W
 
     scenes, counts, mats, st, _ = W.two_material_drop(n_particles=20000, n=32, seed=4)
     N = counts[0]
     res = []
-    for variant in (0, 2):
+    for variant in (0, 2, 4):
         sim = gpu.Simulator(scenes, counts, mats)
         sim.set_variants(p2g_variant=variant)
         sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st["mat"])
