@@ -10,8 +10,12 @@
 // ranges, grid v and v before the walls) using the same step kernels pointed
 // at the tape -- skipped for the segment the forward left in the tape --
 // then the three reverse kernels run for each step from the last to the
-// first.  Tape depth = k steps.  Each segment's work is one CUDA graph
-// (captured once per segment length; the checkpoint copies stay outside).
+// first.  Tape depth = k steps.  With the bin sort the tape has two sets of
+// k slots: segment s - 1 is replayed into one set on a side stream while
+// segment s is reversed from the other, both latency-bound and at low
+// occupancy.  With the radix step sort (whose ping-pong buffers the replay
+// shares) a segment's replay and reverse run in turn.  Each piece is one
+// CUDA graph (captured once per segment length; checkpoint copies outside).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,43 +33,51 @@ namespace {
 size_t nodes_of(pgmpm_solver s) { return (size_t)s->total_nt * 64; }
 
 int ensure_tape(pgmpm_solver s, int slots) {
-    if (s->tape_slots >= slots && s->tape_q.p) return PGMPM_OK;
+    const int sets = s->bs_ccount.p ? 2 : 1;  // the overlapped backward needs the bin sort
+    if (s->tape_slots >= slots && s->tape_sets == sets && s->tape_q.p) return PGMPM_OK;
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
     const size_t nodes = nodes_of(s);
+    const size_t ss = (size_t)slots * sets;  // slots over all sets
     s->tape_slots = 0;
+    s->tape_sets = 0;
     s->tape_has_last = false;
     s->drop_tape_graphs();  // they hold the old tape's addresses
-    CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1)));
-    CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1)));
+    CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1) * sets));
+    CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1) * sets));
     if (s->pf.physics == PHYS_MLS) CK(s->tape_pay.alloc(sizeof(float4) * 4 * N));
-    CK(s->tape_sk.alloc(sizeof(uint32_t) * N * slots));
-    CK(s->tape_ord.alloc(sizeof(uint32_t) * N * slots));
-    CK(s->tape_gv.alloc(sizeof(float4) * nodes * slots));
-    CK(s->tape_gvpre.alloc(sizeof(float4) * nodes * slots));
-    CK(s->tape_flags.alloc(sizeof(uint32_t) * (size_t)s->total_nt * slots));
-    CK(s->tape_tiles.alloc(sizeof(uint32_t) * (size_t)s->total_nt * slots));
-    CK(s->tape_ctiles.alloc(sizeof(uint32_t) * (size_t)s->total_ct * slots));
-    CK(s->tape_crange.alloc(sizeof(uint2) * (size_t)s->total_ct * slots));
-    CK(s->tape_counters.alloc(sizeof(uint32_t) * CNT_WORDS * slots));
+    CK(s->tape_sk.alloc(sizeof(uint32_t) * N * ss));
+    CK(s->tape_ord.alloc(sizeof(uint32_t) * N * ss));
+    CK(s->tape_gv.alloc(sizeof(float4) * nodes * ss));
+    CK(s->tape_gvpre.alloc(sizeof(float4) * nodes * ss));
+    CK(s->tape_flags.alloc(sizeof(uint32_t) * (size_t)s->total_nt * ss));
+    CK(s->tape_tiles.alloc(sizeof(uint32_t) * (size_t)s->total_nt * ss));
+    CK(s->tape_ctiles.alloc(sizeof(uint32_t) * (size_t)s->total_ct * ss));
+    CK(s->tape_crange.alloc(sizeof(uint2) * (size_t)s->total_ct * ss));
+    CK(s->tape_counters.alloc(sizeof(uint32_t) * CNT_WORDS * ss));
     CK(cudaMemset(s->tape_counters.p, 0, s->tape_counters.bytes));
     if (s->bs_ccount.p) {  // the bin sort is available: per-slot cell tables
-        CK(s->tape_cells.alloc(sizeof(uint2) * 64 * std::max<size_t>((size_t)s->total_ct, 1) * slots));
-        CK(s->tape_ptile.alloc(sizeof(uint32_t) * std::max<size_t>((size_t)s->total_ct, 1) * slots));
+        CK(s->tape_cells.alloc(sizeof(uint2) * 64 * std::max<size_t>((size_t)s->total_ct, 1) * ss));
+        CK(s->tape_ptile.alloc(sizeof(uint32_t) * std::max<size_t>((size_t)s->total_ct, 1) * ss));
     }
     s->tape_slots = slots;
+    s->tape_sets = sets;
     return PGMPM_OK;
 }
 
-// Buffers of tape slot j: the step from state j (tape_q[j]) to state j+1.
-StepBufs tape_bufs(pgmpm_solver s, int j) {
+// Buffers of slot j of tape set t: the step from state j to state j+1.
+// States (and keys) of set t are t (slots + 1) + j; the per-step data of
+// slot j is slot t slots + j.
+StepBufs tape_bufs(pgmpm_solver s, int j, int t = 0) {
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
     const size_t nodes = nodes_of(s);
+    const size_t qs = (size_t)t * (s->tape_slots + 1) + j;  // state j of set t
+    j += t * s->tape_slots;                                  // per-step slot of set t
     StepBufs b;
-    b.q = s->tape_q.as<float4>() + 6 * N * j;
-    b.q_out = s->tape_q.as<float4>() + 6 * N * (j + 1);
+    b.q = s->tape_q.as<float4>() + 6 * N * qs;
+    b.q_out = s->tape_q.as<float4>() + 6 * N * (qs + 1);
     b.pay = s->pf.physics == PHYS_MLS ? s->tape_pay.as<float4>() : nullptr;
-    b.keys_in = s->tape_keys.as<uint32_t>() + N * j;
-    b.keys_out = s->tape_keys.as<uint32_t>() + N * (j + 1);
+    b.keys_in = s->tape_keys.as<uint32_t>() + N * qs;
+    b.keys_out = s->tape_keys.as<uint32_t>() + N * (qs + 1);
     uint32_t* sk = s->tape_sk.as<uint32_t>() + N * j;
     uint32_t* so = s->tape_ord.as<uint32_t>() + N * j;
     // the sort's last pass must land in the slot: pair a when which == 0
@@ -118,20 +130,20 @@ int tape_graph(pgmpm_solver s, int kind, int len, Body&& body) {
     return PGMPM_OK;
 }
 
-// Forward of tape slots 0..len-1 (state 0 and its payload already in place).
-int record_tape_forward(pgmpm_solver s, int len, cudaStream_t st) {
+// Forward of slots 0..len-1 of tape set t (state 0 and its payload in place).
+int record_tape_forward(pgmpm_solver s, int len, cudaStream_t st, int t = 0) {
     for (int j = 0; j < len; ++j) {
-        int rc = record_step(s, tape_bufs(s, j), st, false);
+        int rc = record_step(s, tape_bufs(s, j, t), st, false);
         if (rc) return rc;
     }
     return PGMPM_OK;
 }
 
-// Reverse kernels of tape slots len-1 .. 0.
-int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t st) {
+// Reverse kernels of slots len-1 .. 0 of tape set t.
+int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t st, int t = 0) {
     AdjView A = A0;
     for (int j = len - 1; j >= 0; --j) {
-        StepBufs b = tape_bufs(s, j);
+        StepBufs b = tape_bufs(s, j, t);
         View V = s->view_for(b);
         V.grid_mp = A.grid_gv;  // scatter target of the G2P reverse
         A.q_next = b.q_out;
@@ -139,6 +151,68 @@ int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t
         CK(launch_adj_scatter(V, A, s->pf, s->tune, s->num_sms, st));
         CK(launch_adj_grid(V, A, s->tune, s->num_sms, st));
         CK(launch_adj_gather(V, A, s->pf, s->tune, st));
+    }
+    return PGMPM_OK;
+}
+
+// Backward over all segments with two tape sets: while segment seg is
+// reversed from set `cur` on st, segment seg - 1 is replayed into the other
+// set on the side stream (it starts after everything before it on st, so the
+// set's previous reverse is done; st waits for it before the next reverse).
+// The replay uses the payload buffer, the bin sort's scratch and the P2G
+// accumulator, which no reverse kernel touches.
+int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
+    const size_t Nz = (size_t)std::max<int64_t>(s->N, 1);
+    const int k = s->ck_every;
+    if (!s->side_stream) CK(cudaStreamCreateWithFlags(&s->side_stream, cudaStreamNonBlocking));
+    if (!s->ev_fork) CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+    if (!s->ev_join) CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    cudaStream_t side = s->side_stream;
+    auto seg_len = [&](int seg) { return std::min(k, s->ck_steps - seg * k); };
+    auto replay = [&](int seg, int t, cudaStream_t cs) -> int {
+        const int len = seg_len(seg);
+        const StepBufs b0 = tape_bufs(s, 0, t);
+        CK(cudaMemcpyAsync(b0.q, s->ck_q.as<float4>() + 6 * Nz * seg, sizeof(float4) * 6 * Nz,
+                           cudaMemcpyDeviceToDevice, cs));
+        CK(cudaMemcpyAsync(b0.keys_in, s->ck_keys.as<uint32_t>() + Nz * seg, sizeof(uint32_t) * Nz,
+                           cudaMemcpyDeviceToDevice, cs));
+        int rc = tape_graph(s, 4 + t, len, [&](cudaStream_t c) -> int {
+            CK(launch_payload(s->view_for(b0), s->pf, c));
+            return record_tape_forward(s, len, c, t);
+        });
+        if (rc) return rc;
+        CK(cudaGraphLaunch(s->tape_exec[4 + t], cs));
+        return PGMPM_OK;
+    };
+    auto reverse = [&](int seg, int t, cudaStream_t cs) -> int {
+        const int len = seg_len(seg);
+        int rc = tape_graph(s, 2 + t, len, [&](cudaStream_t c) { return record_tape_reverse(s, A, len, c, t); });
+        if (rc) return rc;
+        CK(cudaGraphLaunch(s->tape_exec[2 + t], cs));
+        return PGMPM_OK;
+    };
+    const int last = s->ck_count - 1;
+    int rc = PGMPM_OK;
+    if (!s->tape_has_last) {  // the forward did not leave the last segment in set 0
+        rc = replay(last, 0, st);
+        if (rc) return rc;
+    }
+    s->tape_has_last = false;  // the replays below overwrite it
+    int cur = 0;
+    for (int seg = last; seg >= 0; --seg) {
+        if (seg > 0) {
+            CK(cudaEventRecord(s->ev_fork, st));
+            CK(cudaStreamWaitEvent(side, s->ev_fork, 0));
+            rc = replay(seg - 1, 1 - cur, side);
+            if (rc) return rc;
+        }
+        rc = reverse(seg, cur, st);
+        if (rc) return rc;
+        if (seg > 0) {
+            CK(cudaEventRecord(s->ev_join, side));
+            CK(cudaStreamWaitEvent(st, s->ev_join, 0));
+        }
+        cur = 1 - cur;
     }
     return PGMPM_OK;
 }
@@ -242,7 +316,12 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
     A.grid_gpm = s->adj_grid_gpm.as<float4>();
     A.gE = s->adj_gE.as<float>();
     const int k = s->ck_every;
-    for (int seg = s->ck_count - 1; seg >= 0 && N > 0; --seg) {
+    const bool overlapped = s->tape_sets == 2 && s->tune.step_sort == 0;
+    if (overlapped && N > 0) {
+        rc = backward_overlapped(s, A, st);
+        if (rc) return rc;
+    }
+    for (int seg = s->ck_count - 1; seg >= 0 && N > 0 && !overlapped; --seg) {
         const int len = std::min(k, s->ck_steps - seg * k);
         if (seg == s->ck_count - 1 && s->tape_has_last) {
             // the forward left this segment in the tape
@@ -266,7 +345,8 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
         if (rc) return rc;
         CK(cudaGraphLaunch(s->tape_exec[0], st));
     }
-    CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), s->tape_slots, s->counters.as<uint32_t>(), st));
+    CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), s->tape_slots * s->tape_sets, s->counters.as<uint32_t>(),
+                          st));
     // physical planes -> caller's arrays (upload order)
     if (ptr_kind == PGMPM_PTR_DEVICE) {
         CK(launch_planes_to_state(A.g, s->phys_of_user.as<uint32_t>(), gx_in, gv_in, gC_in, gF_in, N, st));

@@ -134,17 +134,23 @@ struct pgmpm_solver_s {
     bool ck_valid = false;
     pgmpm::DevBuf ck_q, ck_keys;         // checkpoints: states (6N float4) + keys (N u32)
     int tape_slots = 0;                  // allocated tape depth (steps per segment)
-    pgmpm::DevBuf tape_q, tape_keys;     // (slots + 1) states and keys
+    int tape_sets = 0;                   // 2 with the bin sort: a segment is replayed into one
+                                         // set while the previous one is reversed from the other
+    pgmpm::DevBuf tape_q, tape_keys;     // per set: (slots + 1) states and keys
     pgmpm::DevBuf tape_pay;              // payload of the replayed state (one, reused by every slot)
-    pgmpm::DevBuf tape_sk, tape_ord;     // slots x N sorted keys / order
-    pgmpm::DevBuf tape_gv, tape_gvpre;   // slots x nodes float4
+    pgmpm::DevBuf tape_sk, tape_ord;     // per set: slots x N sorted keys / order
+    pgmpm::DevBuf tape_gv, tape_gvpre;   // per set: slots x nodes float4
     pgmpm::DevBuf tape_flags, tape_tiles, tape_ctiles, tape_crange, tape_counters;
     pgmpm::DevBuf tape_cells, tape_ptile;  // per slot: cell ranges and largest-first tile list (bin sort)
     bool tape_has_last = false;           // the tape holds the forward's last segment (no replay needed)
-    // captured tape work: [0] replay + reverse of a segment, [1] forward of a
-    // segment into the tape, [2] reverse only; each for one segment length
-    cudaGraphExec_t tape_exec[3] = {};
-    int tape_exec_len[3] = {-1, -1, -1};
+    // captured tape work, each for one segment length: [0] replay + reverse
+    // of a segment (set 0), [1] forward of a segment into set 0, [2], [3]
+    // reverse of set 0 / 1, [4], [5] replay into set 0 / 1
+    static constexpr int kTapeGraphs = 6;
+    cudaGraphExec_t tape_exec[kTapeGraphs] = {};
+    int tape_exec_len[kTapeGraphs] = {-1, -1, -1, -1, -1, -1};
+    cudaStream_t side_stream = nullptr;  // the replay that overlaps a segment's reverse
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     pgmpm::DevBuf adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;
 
     pgmpm::StepBufs live_bufs() const {
@@ -206,7 +212,7 @@ struct pgmpm_solver_s {
     pgmpm::View view() const { return view_for(live_bufs()); }
 
     void drop_tape_graphs() {
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < kTapeGraphs; ++i) {
             if (tape_exec[i]) cudaGraphExecDestroy(tape_exec[i]);
             tape_exec[i] = nullptr;
             tape_exec_len[i] = -1;
@@ -229,6 +235,9 @@ struct pgmpm_solver_s {
         cudaSetDevice(device);
         drop_graph();
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (side_stream) cudaStreamDestroy(side_stream);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_counters) cudaFreeHost(h_counters);
