@@ -51,7 +51,7 @@
 extern "C" {
 #endif
 
-#define PGMPM_ABI_VERSION 1
+#define PGMPM_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PGMPM_API __attribute__((visibility("default")))
@@ -114,13 +114,24 @@ typedef struct {
     float gravity[3];
 } pgmpm_scene_desc;
 
-/* Material (src/mpm_data_structures.h:63-75 MaterialParameters subset). */
+/* Material (src/mpm_data_structures.h:63-75 MaterialParameters subset).
+ * ELASTIC / JELLY: model FIXED_COROTATED or NEO_HOOKEAN.
+ * ELASTOPLASTIC: the neo-Hookean predictor with the von Mises return mapping
+ *   of src/material_point_method.h:375-402 (the deviatoric Cauchy stress is
+ *   scaled down to yield_stress; stateless, as there); model is ignored.
+ * FLUID: model EOS_FLUID, p = -K (J - 1), plus the Newtonian viscous stress
+ *   2 viscosity sym(grad v) of src/mpm_kernels.cu:131-149 (grad v = APIC C).
+ * SAND and SNOW have no implementation in the reference and return
+ * PGMPM_ERR_UNSUPPORTED.  Differentiation (pgmpm_forward_checkpointed,
+ * pgmpm_backward) supports ELASTIC, JELLY and inviscid FLUID. */
 typedef struct {
-    int32_t type;          /* PGMPM_MAT_ELASTIC, PGMPM_MAT_JELLY or PGMPM_MAT_FLUID */
+    int32_t type;          /* PGMPM_MAT_* */
     int32_t model;         /* PGMPM_MODEL_*; FLUID requires EOS_FLUID */
     float youngs_modulus;  /* E; the bulk modulus K for FLUID (reference convention) */
     float poisson_ratio;
     float density;
+    float yield_stress;    /* ELASTOPLASTIC: von Mises yield stress (Pa), > 0 */
+    float viscosity;       /* FLUID: dynamic viscosity (Pa s), >= 0 (0: inviscid) */
 } pgmpm_material;
 
 typedef struct {

@@ -198,7 +198,7 @@ public:
         std::vector<pgmpm_material> mats;
         for (const auto& m : config_.materials)
             mats.push_back(pgmpm_material{(int32_t)m.type, (int32_t)m.model, m.youngs_modulus, m.poisson_ratio,
-                                          m.density});
+                                          m.density, m.yield_stress, m.viscosity});
         const int64_t n = (int64_t)m_.size();
         physgrad_b200_detail::check(
             pgmpm_create(&d, 1, &n, mats.data(), (int32_t)mats.size(), config_.device, &h_));

@@ -148,7 +148,7 @@ template <class T> void polar3(const T F[9], T R[9], T S[9]) {
 
 template <class T> struct Mat {
     int model;
-    T E, nu, mu, lam, dmu_dE, dlam_dE;
+    T E, nu, mu, lam, dmu_dE, dlam_dE, yield, visc;
 };
 template <class T> Mat<T> make_mat(const oracle_material& m) {
     Mat<T> r;
@@ -160,6 +160,8 @@ template <class T> Mat<T> make_mat(const oracle_material& m) {
     r.lam = r.E * nu / ((T(1) + nu) * (T(1) - T(2) * nu));
     r.dmu_dE = T(1) / (T(2) * (T(1) + nu));
     r.dlam_dE = nu / ((T(1) + nu) * (T(1) - T(2) * nu));
+    r.yield = T(m.yield_stress);
+    r.visc = T(m.viscosity);
     return r;
 }
 
@@ -176,7 +178,7 @@ template <class T> void kirchhoff(const T F[9], const Mat<T>& mt, T tau[9]) {
         tau[0] += t;
         tau[4] += t;
         tau[8] += t;
-    } else if (mt.model == ORACLE_NEO_HOOKEAN) {
+    } else if (mt.model == ORACLE_NEO_HOOKEAN || mt.model == ORACLE_VON_MISES) {
         T B[9];
         mmT(F, F, B);
         T t = mt.lam * std::log(J);
@@ -184,6 +186,22 @@ template <class T> void kirchhoff(const T F[9], const Mat<T>& mt, T tau[9]) {
         tau[0] += t;
         tau[4] += t;
         tau[8] += t;
+        if (mt.model == ORACLE_VON_MISES) {
+            // von Mises return mapping of src/material_point_method.h:375-402 on the
+            // Cauchy stress sigma = tau / J: above the yield stress Y the
+            // deviatoric part is scaled by Y / vm(sigma).  vm(tau) = J vm(sigma).
+            const T p = (tau[0] + tau[4] + tau[8]) / T(3);
+            T dev[9], ss = T(0);
+            for (int i = 0; i < 9; ++i) {
+                dev[i] = tau[i] - ((i % 4 == 0) ? p : T(0));
+                ss += dev[i] * dev[i];
+            }
+            const T vm = std::sqrt(T(1.5) * ss);
+            if (vm > J * mt.yield) {
+                const T sc = J * mt.yield / vm;
+                for (int i = 0; i < 9; ++i) tau[i] = ((i % 4 == 0) ? p : T(0)) + sc * dev[i];
+            }
+        }
     } else {  // EOS fluid, K = E
         T t = mt.E * J * (J - T(1));
         for (int i = 0; i < 9; ++i) tau[i] = (i % 4 == 0) ? t : T(0);
@@ -491,6 +509,14 @@ template <class T> void mls_p2g(Sim<T>& S, const State<T>& st) {
         const Mat<T>& mt = S.mats[S.mat[p]];
         T tau[9];
         kirchhoff(&st.F[9 * p], mt, tau);
+        if (mt.model == ORACLE_EOS_FLUID && mt.visc > T(0)) {
+            // Newtonian viscosity (src/mpm_kernels.cu:131-149): sigma += mu_v (C + C^T)
+            // with the APIC C as the velocity gradient; tau = J sigma
+            const T* Cp = &st.C[9 * p];
+            const T J = det3(&st.F[9 * p]);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) tau[3 * i + j] += J * mt.visc * (Cp[3 * i + j] + Cp[3 * j + i]);
+        }
         T A[9];
         for (int i = 0; i < 9; ++i) A[i] = -dt * S.V0[p] * D * tau[i] + S.m[p] * st.C[9 * p + i];
         const T* vp = &st.v[3 * p];

@@ -23,7 +23,12 @@
  *     weakly compressible EOS fluid p = -K (J - 1) where K is carried in the
  *     youngs_modulus field as src/mpm_data_structures.h:87-94 does for
  *     FLUID, the F update (I + dt C) F of src/mpm_kernels.cu:384-397 and the
- *     grid update order of src/mpm_kernels.cu:511-544.
+ *     grid update order of src/mpm_kernels.cu:511-544.  ELASTOPLASTIC
+ *     (ORACLE_VON_MISES): the neo-Hookean predictor with the von Mises return
+ *     mapping of src/material_point_method.h:375-402 (deviatoric Cauchy stress
+ *     scaled down to the yield stress; stateless, as there).  FLUID viscosity:
+ *     the Newtonian stress 2 mu_v sym(grad v) of src/mpm_kernels.cu:131-149
+ *     with the APIC C as grad v, added to the EOS pressure (forward only).
  *   - The cell-key definition and a stable sort (std::stable_sort) that the
  *     GPU radix sort must reproduce bit for bit.
  *   - The reverse-mode adjoint of the MLS step (FP64), used to check the
@@ -47,7 +52,7 @@ extern "C" {
 
 enum { ORACLE_MLS = 0, ORACLE_REF_COMPAT = 1 };
 enum { ORACLE_BC_NONE = 0, ORACLE_BC_STICKY = 1, ORACLE_BC_SLIP = 2, ORACLE_BC_SEPARATE = 3 };
-enum { ORACLE_FIXED_COROTATED = 0, ORACLE_NEO_HOOKEAN = 1, ORACLE_EOS_FLUID = 2 };
+enum { ORACLE_FIXED_COROTATED = 0, ORACLE_NEO_HOOKEAN = 1, ORACLE_EOS_FLUID = 2, ORACLE_VON_MISES = 3 };
 
 typedef struct {
     int32_t n[3];        /* grid nodes per axis */
@@ -62,10 +67,12 @@ typedef struct {
 } oracle_scene;
 
 typedef struct {
-    int32_t model;       /* ORACLE_FIXED_COROTATED / NEO_HOOKEAN / EOS_FLUID */
+    int32_t model;       /* ORACLE_FIXED_COROTATED / NEO_HOOKEAN / EOS_FLUID / VON_MISES */
     int32_t pad;
     double E;            /* Young's modulus, or bulk modulus K for EOS_FLUID */
     double nu;
+    double yield_stress; /* VON_MISES: von Mises yield stress of the Cauchy stress */
+    double viscosity;    /* EOS_FLUID: dynamic viscosity (0: inviscid) */
 } oracle_material;
 
 /* Advance `steps` steps.  x,v: [n][3]; C,F: [n][9] row-major; m,V0: [n];

@@ -43,6 +43,8 @@ class Material(ctypes.Structure):
         ("pad", ctypes.c_int32),
         ("E", ctypes.c_double),
         ("nu", ctypes.c_double),
+        ("yield_stress", ctypes.c_double),
+        ("viscosity", ctypes.c_double),
     ]
 
 
@@ -115,11 +117,17 @@ def make_scene(n, dx, dt, gravity=(0.0, -9.8, 0.0), origin=(0.0, 0.0, 0.0), phys
 
 
 def make_materials(mats):
+    """Tuples (model, E, nu[, yield_stress[, viscosity]]); model 0 fixed-
+    corotated, 1 neo-Hookean, 2 EOS fluid (K in E), 3 von Mises
+    (neo-Hookean predictor, yield_stress on the Cauchy stress)."""
     arr = (Material * len(mats))()
-    for i, (model, E, nu) in enumerate(mats):
+    for i, m in enumerate(mats):
+        model, E, nu = m[:3]
         arr[i].model = int(model)
         arr[i].E = float(E)
         arr[i].nu = float(nu)
+        arr[i].yield_stress = float(m[3]) if len(m) > 3 else 0.0
+        arr[i].viscosity = float(m[4]) if len(m) > 4 else 0.0
     return arr
 
 

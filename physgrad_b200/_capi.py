@@ -76,6 +76,8 @@ class Material(ctypes.Structure):
         ("youngs_modulus", ctypes.c_float),
         ("poisson_ratio", ctypes.c_float),
         ("density", ctypes.c_float),
+        ("yield_stress", ctypes.c_float),
+        ("viscosity", ctypes.c_float),
     ]
 
 

@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(GATHER_T, 3) k_adj_gather(View V, AdjView A) {
         for (int a = 0; a < 9; ++a) gCt[a] = gC[a] + sc.dt * gFFt[a];
         // forward affine matrix (R kept for the stress adjoint)
         float tau[9], Am[9], R[9];
-        kirchhoff(F, mt, tau, R);
+        kirchhoff<false>(F, mt, tau, R);  // differentiation excludes ELASTOPLASTIC
         const float kk = -sc.dt * mv.y * sc.D;
 #pragma unroll
         for (int a = 0; a < 9; ++a) Am[a] = kk * tau[a] + m * C[a];

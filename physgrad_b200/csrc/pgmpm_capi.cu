@@ -44,22 +44,33 @@ int fail(int code, const char* fmt, ...) {
 }
 
 int material_to_dev(const pgmpm_material& m, MatDev& d) {
+    int model;
     if (m.type == PGMPM_MAT_FLUID) {
         if (m.model != PGMPM_MODEL_EOS_FLUID)
             return fail(PGMPM_ERR_UNSUPPORTED, "FLUID material requires PGMPM_MODEL_EOS_FLUID");
+        if (!(m.viscosity >= 0.f) || !std::isfinite(m.viscosity))
+            return fail(PGMPM_ERR_ARG, "FLUID viscosity must be finite and >= 0");
+        model = MODEL_EOS;
     } else if (m.type == PGMPM_MAT_ELASTIC || m.type == PGMPM_MAT_JELLY) {
         if (m.model != PGMPM_MODEL_FIXED_COROTATED && m.model != PGMPM_MODEL_NEO_HOOKEAN)
             return fail(PGMPM_ERR_UNSUPPORTED, "elastic material requires FIXED_COROTATED or NEO_HOOKEAN");
+        model = m.model == PGMPM_MODEL_FIXED_COROTATED ? MODEL_FCR : MODEL_NH;
+    } else if (m.type == PGMPM_MAT_ELASTOPLASTIC) {
+        if (!(m.yield_stress > 0.f) || !std::isfinite(m.yield_stress))
+            return fail(PGMPM_ERR_ARG, "ELASTOPLASTIC yield_stress must be finite and > 0");
+        model = MODEL_VM;
     } else {
-        return fail(PGMPM_ERR_UNSUPPORTED, "material type %d (ELASTOPLASTIC/SAND/SNOW) is not built", m.type);
+        return fail(PGMPM_ERR_UNSUPPORTED, "material type %d (SAND/SNOW) has no implementation", m.type);
     }
     if (!(m.youngs_modulus >= 0.f) || !std::isfinite(m.youngs_modulus))
         return fail(PGMPM_ERR_ARG, "invalid youngs_modulus");
     const double E = m.youngs_modulus, nu = m.poisson_ratio;
-    if (m.model != PGMPM_MODEL_EOS_FLUID && !(nu > -1.0 && nu < 0.5))
+    if (model != MODEL_EOS && !(nu > -1.0 && nu < 0.5))
         return fail(PGMPM_ERR_ARG, "poisson_ratio must be in (-1, 0.5)");
     std::memset(&d, 0, sizeof(d));
-    d.model = m.model == PGMPM_MODEL_FIXED_COROTATED ? MODEL_FCR : m.model == PGMPM_MODEL_NEO_HOOKEAN ? MODEL_NH : MODEL_EOS;
+    d.model = model;
+    d.yield = model == MODEL_VM ? m.yield_stress : 0.f;
+    d.visc = model == MODEL_EOS ? m.viscosity : 0.f;
     d.E = (float)E;
     if (d.model != MODEL_EOS) {
         d.mu = (float)(E / (2.0 * (1.0 + nu)));
@@ -294,6 +305,7 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     s->pf.physics = physics == PGMPM_PHYSICS_MLS ? PHYS_MLS : PHYS_REF;
     s->pf.multi_mat = n_materials > 1;
     s->pf.has_fluid = false;
+    s->pf.has_plastic = false;
     std::vector<MatDev> md(n_materials);
     for (int i = 0; i < n_materials; ++i) {
         int rc = material_to_dev(materials[i], md[i]);
@@ -302,6 +314,7 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
             return rc;
         }
         if (md[i].model == MODEL_EOS) s->pf.has_fluid = true;
+        if (md[i].model == MODEL_VM) s->pf.has_plastic = true;
     }
     int sw = 0;
     {
@@ -379,14 +392,16 @@ int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t
     if (!s || !materials || n_materials != s->M) return fail(PGMPM_ERR_ARG, "material count must match create()");
     DeviceGuard dg(s->device);
     std::vector<MatDev> md(n_materials);
-    bool fluid = false;
+    bool fluid = false, plastic = false;
     for (int i = 0; i < n_materials; ++i) {
         int rc = material_to_dev(materials[i], md[i]);
         if (rc) return rc;
         fluid |= md[i].model == MODEL_EOS;
+        plastic |= md[i].model == MODEL_VM;
     }
-    if (fluid != s->pf.has_fluid) {
+    if (fluid != s->pf.has_fluid || plastic != s->pf.has_plastic) {  // kernels are chosen by these
         s->pf.has_fluid = fluid;
+        s->pf.has_plastic = plastic;
         s->drop_graph();
     }
     // ordered with prior work on the legacy stream; graphs read the table at run time

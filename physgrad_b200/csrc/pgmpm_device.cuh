@@ -23,7 +23,7 @@ namespace pgmpm {
 
 enum { PHYS_MLS = 0, PHYS_REF = 1 };
 enum { BC_NONE = 0, BC_STICKY = 1, BC_SLIP = 2, BC_SEPARATE = 3 };
-enum { MODEL_FCR = 0, MODEL_NH = 1, MODEL_EOS = 2 };
+enum { MODEL_FCR = 0, MODEL_NH = 1, MODEL_EOS = 2, MODEL_VM = 3 };  // VM: neo-Hookean + von Mises
 enum { FLAG_ESCAPE = 1u, FLAG_NONFINITE = 2u, FLAG_TILE_RANGE = 4u, FLAG_BAD_MATERIAL = 8u };
 
 struct SceneDev {
@@ -44,7 +44,8 @@ struct SceneDev {
 struct MatDev {
     int model;
     float mu, lam, E, dmu_dE, dlam_dE;
-    float pad[2];
+    float yield;  // MODEL_VM: von Mises yield stress of the Cauchy stress
+    float visc;   // MODEL_EOS: dynamic viscosity (0: inviscid)
 };
 
 // ------------------------------------------------------------- 3x3 algebra
@@ -256,6 +257,9 @@ __device__ __forceinline__ void polar_rotation(const float F[9], float R[9]) {
 //   EOS: K J (J - 1) I  with K carried in E (p = -K (J - 1))
 // R receives the rotation of F's polar decomposition for the fixed-corotated
 // model (and is left unset otherwise), for kirchhoff_adjoint to reuse.
+// PLASTIC = false leaves out the von Mises cap (kernels launched only when no
+// ELASTOPLASTIC material is present, and the adjoint, which excludes it).
+template <bool PLASTIC = true>
 __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, float tau[9], float R[9]) {
     const float J = m3_det(F);
     if (m.model == MODEL_FCR) {
@@ -267,12 +271,31 @@ __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, flo
         const float c = 2.f * m.mu, t = m.lam * (J - 1.f) * J;
 #pragma unroll
         for (int i = 0; i < 9; ++i) tau[i] = c * tau[i] + ((i % 4 == 0) ? t : 0.f);
-    } else if (m.model == MODEL_NH) {
+    } else if (m.model == MODEL_NH || m.model == MODEL_VM) {
         float B[9];
         m3_mulT(F, F, B);
         const float t = m.lam * logf(J);
 #pragma unroll
         for (int i = 0; i < 9; ++i) tau[i] = m.mu * (B[i] - ((i % 4 == 0) ? 1.f : 0.f)) + ((i % 4 == 0) ? t : 0.f);
+        if (PLASTIC && m.model == MODEL_VM) {
+            // von Mises return mapping (src/material_point_method.h:375-402) on
+            // the Cauchy stress sigma = tau / J: above the yield stress Y its
+            // deviatoric part is scaled by Y / vm(sigma); vm(tau) = J vm(sigma)
+            const float p = (tau[0] + tau[4] + tau[8]) * (1.f / 3.f);
+            float ss = 0.f;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const float d = tau[i] - ((i % 4 == 0) ? p : 0.f);
+                ss += d * d;
+            }
+            const float vm = sqrtf(1.5f * ss);
+            if (vm > J * m.yield) {
+                const float sc = J * m.yield / vm;
+#pragma unroll
+                for (int i = 0; i < 9; ++i)
+                    tau[i] = (i % 4 == 0) ? p + sc * (tau[i] - p) : sc * tau[i];
+            }
+        }
     } else {
         const float t = m.E * J * (J - 1.f);
 #pragma unroll
@@ -280,9 +303,22 @@ __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, flo
     }
 }
 
+// Viscous fluid: the Newtonian stress 2 mu_v sym(grad v) of
+// src/mpm_kernels.cu:131-149 with the APIC C as grad v, added as Kirchhoff
+// stress J mu_v (C + C^T) to the EOS pressure.
+__device__ __forceinline__ void add_viscous(const float F[9], const float C[9], const MatDev& m, float tau[9]) {
+    if (m.model != MODEL_EOS || !(m.visc > 0.f)) return;
+    const float Jv = m3_det(F) * m.visc;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) tau[3 * i + j] += Jv * (C[3 * i + j] + C[3 * j + i]);
+}
+
+template <bool PLASTIC = true>
 __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, float tau[9]) {
     float R[9];
-    kirchhoff(F, m, tau, R);
+    kirchhoff<PLASTIC>(F, m, tau, R);
 }
 
 // Adjoint of kirchhoff(): gF += d<tb, tau(F)>/dF; returns d<tb, tau>/dE.
@@ -373,11 +409,13 @@ __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const MatDe
 //   Ad = dx * A, A = -dt V0 D tau(F) + m C, b = m v - Ad f.
 // Packed as 4 float4 planes: p0 = (b, m), p1 = Ad[0..3], p2 = Ad[4..7],
 // p3 = (Ad[8], f).
+template <bool PLASTIC = true>
 __device__ __forceinline__ void mls_payload(const SceneDev& sc, const MatDev& mt, const float f[3], const float F[9],
                                             const float v[3], const float C[9], float m, float V0, float4& p0,
                                             float4& p1, float4& p2, float4& p3) {
     float tau[9];
-    kirchhoff(F, mt, tau);
+    kirchhoff<PLASTIC>(F, mt, tau);
+    add_viscous(F, C, mt, tau);
     const float kk = -sc.dt * V0 * sc.D;
     float Ad[9];
 #pragma unroll

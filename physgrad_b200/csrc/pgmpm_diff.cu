@@ -217,6 +217,15 @@ int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
     return PGMPM_OK;
 }
 
+// The adjoint covers the elastic models and the inviscid EOS fluid.
+int check_differentiable(pgmpm_solver s) {
+    for (const pgmpm_material& m : s->mats_h)
+        if (m.type == PGMPM_MAT_ELASTOPLASTIC || (m.type == PGMPM_MAT_FLUID && m.viscosity > 0.f))
+            return fail(PGMPM_ERR_UNSUPPORTED,
+                        "differentiation of ELASTOPLASTIC materials and of viscous fluids is not built");
+    return PGMPM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -225,6 +234,7 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     if (!s || n_steps < 1 || checkpoint_every < 1) return fail(PGMPM_ERR_ARG, "need n_steps >= 1, checkpoint_every >= 1");
     if (s->pf.physics != PHYS_MLS) return fail(PGMPM_ERR_UNSUPPORTED, "differentiation needs PGMPM_PHYSICS_MLS");
     if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    if (int rc0 = check_differentiable(s)) return rc0;
     DeviceGuard dg(s->device);
     cudaStream_t st = ST(stream);
     const int k = std::min(checkpoint_every, n_steps);
@@ -280,6 +290,7 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
                    float* gx_in, float* gv_in, float* gC_in, float* gF_in, float* gE, int32_t ptr_kind, void* stream) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
     if (!s->ck_valid) return fail(PGMPM_ERR_STATE, "call pgmpm_forward_checkpointed first");
+    if (int rc0 = check_differentiable(s)) return rc0;
     if (ptr_kind != PGMPM_PTR_HOST && ptr_kind != PGMPM_PTR_DEVICE) return fail(PGMPM_ERR_ARG, "bad ptr_kind");
     DeviceGuard dg(s->device);
     cudaStream_t st = ST(stream);

@@ -117,6 +117,7 @@ struct PhysFlags {
     int physics;     // PHYS_MLS / PHYS_REF (same for every scene)
     bool multi_mat;  // per-particle material ids
     bool has_fluid;  // some material uses the EOS model
+    bool has_plastic;  // some material is ELASTOPLASTIC (von Mises)
 };
 cudaError_t launch_keys(const View& V, const PhysFlags& pf, cudaStream_t st);
 cudaError_t launch_payload(const View& V, const PhysFlags& pf, cudaStream_t st);

@@ -173,6 +173,7 @@ __global__ void __launch_bounds__(512) k_p2g(View V, int ppt) {
                 const MatDev mt = V.mats[MULTI ? V.mat[p] : 0];
                 float tau[9];
                 kirchhoff(F, mt, tau);
+                add_viscous(F, C, mt, tau);
                 const float kk = -sc.dt * mv.y * sc.D;
                 float A[9];
 #pragma unroll
@@ -1326,7 +1327,9 @@ __global__ void k_grid(View V) {
 // ------------------------------------------------------------------- G2P
 // Per-particle G2P update shared by both G2P variants; `fetch(i, j, k)`
 // returns the (v, m) float4 of grid node (i, j, k) of scene sc.
-template <int PHYS, bool MULTI, bool FLUID, class Fetch>
+// PLASTIC: the payload's stress includes the von Mises cap (launched when an
+// ELASTOPLASTIC material is present).
+template <int PHYS, bool MULTI, bool FLUID, bool PLASTIC, class Fetch>
 __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, uint32_t p, const Fetch& fetch,
                                              uint32_t& flags) {
     const int64_t N = V.N;
@@ -1422,7 +1425,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
         if (V.pay_out) {
             const float2 mv = V.mV[p];
             float4 a0, a1, a2, a3;
-            mls_payload(sc, V.mats[MULTI ? V.mat[p] : 0], fn, Fn, nv, C, mv.x, mv.y, a0, a1, a2, a3);
+            mls_payload<PLASTIC>(sc, V.mats[MULTI ? V.mat[p] : 0], fn, Fn, nv, C, mv.x, mv.y, a0, a1, a2, a3);
             V.pay_out[p] = a0;
             V.pay_out[N + p] = a1;
             V.pay_out[2 * N + p] = a2;
@@ -1475,7 +1478,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
 // sorted at upload and particles drift less than a cell per step, so
 // neighbouring threads still share grid nodes, and the state loads are fully
 // coalesced with no dependent load of the order array.
-template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER>
+template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER, bool PLASTIC>
 __device__ __forceinline__ void k_g2p_impl(const View& V) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1490,20 +1493,25 @@ __device__ __forceinline__ void k_g2p_impl(const View& V) {
         const SceneDev& sc = scene_ref(V, s);
         const float4* gv = V.grid_v;
         auto fetch = [&](int, int, int, int idx) { return __ldg(&gv[idx]); };
-        g2p_particle<PHYS, MULTI, FLUID>(V, sc, p, fetch, flags);
+        g2p_particle<PHYS, MULTI, FLUID, PLASTIC>(V, sc, p, fetch, flags);
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
 template <int PHYS, bool MULTI, bool FLUID>
 __global__ void k_g2p(View V) {
-    k_g2p_impl<PHYS, MULTI, FLUID, false>(V);
+    k_g2p_impl<PHYS, MULTI, FLUID, false, true>(V);
 }
 // 64 registers (4 blocks of 256 threads per SM): the gathers' latency wants
 // the occupancy more than the few spilled words cost
 template <int PHYS, bool MULTI, bool FLUID>
 __global__ void __launch_bounds__(512, 2) k_g2p_phys(View V) {
-    k_g2p_impl<PHYS, MULTI, FLUID, true>(V);
+    k_g2p_impl<PHYS, MULTI, FLUID, true, false>(V);
+}
+// the same with the von Mises cap (an ELASTOPLASTIC material is present)
+template <int PHYS, bool MULTI, bool FLUID>
+__global__ void __launch_bounds__(512, 2) k_g2p_phys_vm(View V) {
+    k_g2p_impl<PHYS, MULTI, FLUID, true, true>(V);
 }
 
 // G2P variant 0: one block per occupied cell tile; the tile's 6^3 node
@@ -1546,7 +1554,7 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(View V) {
                 flags |= FLAG_TILE_RANGE;
                 continue;
             }
-            g2p_particle<PHYS, MULTI, FLUID>(V, sc, p, fetch, flags);
+            g2p_particle<PHYS, MULTI, FLUID, true>(V, sc, p, fetch, flags);
         }
         __syncthreads();
     }
@@ -1820,7 +1828,10 @@ cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int 
         PGMPM_G2P_DISPATCH(k_g2p, nb, t.g2p_block);
     } else {
         const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
-        PGMPM_G2P_DISPATCH(k_g2p_phys, nb, t.g2p_block);
+        if (pf.has_plastic)
+            PGMPM_G2P_DISPATCH(k_g2p_phys_vm, nb, t.g2p_block);
+        else
+            PGMPM_G2P_DISPATCH(k_g2p_phys, nb, t.g2p_block);
     }
     return cudaGetLastError();
 }

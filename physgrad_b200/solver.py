@@ -51,15 +51,21 @@ class BoundaryType(enum.IntEnum):
 
 @dataclass
 class MaterialParameters:
-    """Subset of src/mpm_data_structures.h:63-75 used by the step.
+    """Subset of src/mpm_data_structures.h:63-75 used by the step, with the
+    reference's defaults.
 
     For FLUID the bulk modulus is carried in ``youngs_modulus`` (the
-    reference's convention, src/mpm_data_structures.h:87-94)."""
+    reference's convention, src/mpm_data_structures.h:87-94) and
+    ``viscosity`` adds a Newtonian viscous stress.  ELASTOPLASTIC is the
+    neo-Hookean predictor with a von Mises cap at ``yield_stress``
+    (``model`` is ignored for it)."""
     density: float = 1000.0
     youngs_modulus: float = 1e6
     poisson_ratio: float = 0.3
     type: MaterialType = MaterialType.ELASTIC
     model: ConstitutiveModel = ConstitutiveModel.FIXED_COROTATED
+    yield_stress: float = 1e5
+    viscosity: float = 0.001
 
     def to_c(self) -> C.Material:
         m = C.Material()
@@ -68,6 +74,8 @@ class MaterialParameters:
         m.youngs_modulus = float(self.youngs_modulus)
         m.poisson_ratio = float(self.poisson_ratio)
         m.density = float(self.density)
+        m.yield_stress = float(self.yield_stress)
+        m.viscosity = float(self.viscosity)
         return m
 
 
@@ -77,9 +85,11 @@ def createElasticMaterial(density, youngs_modulus, poisson_ratio,
     return MaterialParameters(density, youngs_modulus, poisson_ratio, MaterialType.ELASTIC, model)
 
 
-def createFluidMaterial(density, bulk_modulus) -> MaterialParameters:
-    """src/mpm_data_structures.h:87-94 (bulk modulus in youngs_modulus)."""
-    return MaterialParameters(density, bulk_modulus, 0.0, MaterialType.FLUID, ConstitutiveModel.EOS_FLUID)
+def createFluidMaterial(density, viscosity, gamma=7.0) -> MaterialParameters:
+    """src/mpm_data_structures.h:87-94: the third argument (the bulk modulus
+    K of p = -K (J - 1)) is stored in youngs_modulus, as there."""
+    return MaterialParameters(density, gamma, 0.0, MaterialType.FLUID, ConstitutiveModel.EOS_FLUID,
+                              viscosity=viscosity)
 
 
 @dataclass

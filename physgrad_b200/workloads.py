@@ -66,7 +66,7 @@ def two_material_drop(n_particles=2097152, n=128, seed=0, steps=1000, dt=5e-5):
     x = np.concatenate([xa, xb], 0).astype(np.float32)
     mat = np.concatenate([np.zeros(h, np.int32), np.ones(n_particles - h, np.int32)])
     scene = Scene((n, n, n), dx, dt, G, (0.0, 0.0, 0.0), C.PHYSICS_MLS, C.BC_SLIP, 3)
-    mats = [createElasticMaterial(RHO, 5e4, 0.3, ConstitutiveModel.NEO_HOOKEAN), createFluidMaterial(RHO, 1e4)]
+    mats = [createElasticMaterial(RHO, 5e4, 0.3, ConstitutiveModel.NEO_HOOKEAN), createFluidMaterial(RHO, 0.0, 1e4)]
     meta = {"workload": "two_material_drop", "grid": n, "n_particles": n_particles, "steps": steps, "seed": seed,
             "dt": dt, "rho": RHO, "V0": "(dx/2)^3", "gravity": G, "walls": "slip 3 nodes",
             "materials": "neo-Hookean E=5e4 nu=0.3 / EOS fluid K=1e4"}

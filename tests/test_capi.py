@@ -50,7 +50,7 @@ def test_struct_layout_matches_c(tmp_path):
 #include "pgmpm.h"
 int main(void){
  printf("%zu %zu %zu %zu\n", sizeof(pgmpm_scene_desc), offsetof(pgmpm_scene_desc, dx), offsetof(pgmpm_scene_desc, gravity), offsetof(pgmpm_scene_desc, dt));
- printf("%zu %zu\n", sizeof(pgmpm_material), offsetof(pgmpm_material, density));
+ printf("%zu %zu %zu\n", sizeof(pgmpm_material), offsetof(pgmpm_material, density), offsetof(pgmpm_material, viscosity));
  printf("%zu %zu %zu\n", sizeof(pgmpm_metrics), offsetof(pgmpm_metrics, p2g_block), offsetof(pgmpm_metrics, g2p_ms));
  return 0;}
 ''')
@@ -59,7 +59,7 @@ int main(void){
     got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     got = [int(g) for g in got]
     exp = [ctypes.sizeof(C.SceneDesc), C.SceneDesc.dx.offset, C.SceneDesc.gravity.offset, C.SceneDesc.dt.offset,
-           ctypes.sizeof(C.Material), C.Material.density.offset,
+           ctypes.sizeof(C.Material), C.Material.density.offset, C.Material.viscosity.offset,
            ctypes.sizeof(C.Metrics), C.Metrics.p2g_block.offset, C.Metrics.g2p_ms.offset]
     assert got == exp
 
@@ -67,7 +67,7 @@ int main(void){
 def test_header_compiles_as_c_and_cxx(tmp_path):
     for comp, ext in (("gcc", "c"), ("g++", "cpp")):
         f = tmp_path / f"h.{ext}"
-        f.write_text('#include "pgmpm.h"\nint main(void){ return PGMPM_ABI_VERSION == 1 ? 0 : 1; }\n')
+        f.write_text('#include "pgmpm.h"\nint main(void){ return PGMPM_ABI_VERSION == 2 ? 0 : 1; }\n')
         subprocess.run([comp, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(f), "-o",
                         str(tmp_path / f"h_{ext}")], check=True)
 
@@ -99,7 +99,7 @@ def test_argument_validation_without_gpu(built_lib):
     assert b"scene" in L.pgmpm_last_error()
     assert L.pgmpm_step(None, 1, None) == C.PGMPM_ERR_ARG
     assert L.pgmpm_radix_sort_pairs(None, None, None, None, 10, 8, None) == C.PGMPM_ERR_ARG
-    assert L.pgmpm_abi_version() == 1
+    assert L.pgmpm_abi_version() == 2
 
 
 def test_workloads_are_seeded_and_shaped():

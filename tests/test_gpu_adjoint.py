@@ -30,7 +30,7 @@ def test_adjoint_matches_fp64_oracle(gpu, oracle, bc, k):
     st = _case(rng, N, n)
     mats_o = [(oracle.FIXED_COROTATED, 1e4, 0.3), (oracle.NEO_HOOKEAN, 3e4, 0.25), (oracle.EOS_FLUID, 1e4, 0.0)]
     mats = [gpu.createElasticMaterial(1000, 1e4, 0.3), gpu.createElasticMaterial(1000, 3e4, 0.25, 1),
-            gpu.createFluidMaterial(1000, 1e4)]
+            gpu.createFluidMaterial(1000, 0.0, 1e4)]
     scene = gpu.Scene((n, n, n), 1.0 / n, dt, (0, -9.8, 0), (0, 0, 0), 0, bc, 3)
     sim = gpu.Simulator([scene], [N], mats)
     sim.upload(st["x"], st["v"], st["C"], st["F"], st["m"], st["V0"], st["mat"])

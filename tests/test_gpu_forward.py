@@ -180,7 +180,7 @@ def test_mls_golden_fixture(gpu):
     N = g["x0"].shape[0]
     scene = gpu.Scene(tuple(meta["n"]), meta["dx"], meta["dt"], tuple(meta["gravity"]), (0, 0, 0), 0, 1, 3)
     mats = [gpu.createElasticMaterial(1000, 1e4, 0.3), gpu.createElasticMaterial(1000, 3e4, 0.25, 1),
-            gpu.createFluidMaterial(1000, 1e4)]
+            gpu.createFluidMaterial(1000, 0.0, 1e4)]
     V0 = np.full(N, (meta["dx"] / 2) ** 3, np.float32)
     st = dict(x=g["x0"], v=g["v0"], C=np.zeros((N, 9), np.float32), F=np.tile(np.eye(3, dtype=np.float32).ravel(), (N, 1)),
               m=(1000 * V0).astype(np.float32), V0=V0, mat=g["mat"])
@@ -358,6 +358,68 @@ def test_multi_step_call_equals_single_steps(gpu, use_graph):
     b.step(2)
     b.step(1)
     same(a.download(), b.download())
+
+
+@pytest.mark.parametrize("case", ["plastic", "plastic_and_viscous"])
+def test_plastic_and_viscous_vs_fp64_oracle(gpu, oracle, case):
+    """ELASTOPLASTIC (neo-Hookean predictor with the von Mises cap of
+    src/material_point_method.h:375-402) and the viscous fluid (Newtonian
+    stress of src/mpm_kernels.cu:131-149) against the FP64 oracle: one
+    material, and the two mixed (the multi-material kernels).  The yield
+    stress and viscosity are low and high enough that both change the
+    result against the elastic / inviscid run."""
+    from physgrad_b200 import workloads as W
+
+    MT, CM = gpu.MaterialType, gpu.ConstitutiveModel
+    Y = 5.0
+    plastic = gpu.MaterialParameters(1000, 1e4, 0.3, MT.ELASTOPLASTIC, CM.NEO_HOOKEAN, yield_stress=Y)
+    elastic = gpu.createElasticMaterial(1000, 1e4, 0.3, CM.NEO_HOOKEAN)
+    if case == "plastic":
+        scenes, counts, _, st, _ = W.elastic_cube(n_particles=20000, n=32, v_sigma=0.5, seed=31)
+        st = dict(st)
+        st["F"] = (st["F"] + np.random.default_rng(31).normal(0, 0.02, st["F"].shape)).astype(np.float32)
+        mats, mats_el = [plastic], [elastic]
+        omats = [(3, 1e4, 0.3, Y)]
+        omats_el = [(1, 1e4, 0.3)]
+        steps = 40
+    else:
+        scenes, counts, _, st, _ = W.two_material_drop(n_particles=30000, n=32, seed=32)
+        st = dict(st)
+        st["v"] = (st["v"] + np.random.default_rng(32).normal(0, 0.3, st["v"].shape)).astype(np.float32)
+        mats = [plastic, gpu.createFluidMaterial(1000, 20.0, 1e4)]
+        mats_el = [elastic, gpu.createFluidMaterial(1000, 0.0, 1e4)]
+        omats = [(3, 1e4, 0.3, Y), (2, 1e4, 0.0, 0.0, 20.0)]
+        omats_el = [(1, 1e4, 0.3), (2, 1e4, 0.0)]
+        steps = 60
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(steps)
+    out = sim.download()
+    assert sim.status() == 0
+    osc = _oracle_scene(oracle, scenes[0])
+    ref = oracle.run(osc, oracle.make_materials(omats), _oracle_state(st), steps, prec=64)
+    _assert_mls(out, ref, case)
+    ref_el = oracle.run(osc, oracle.make_materials(omats_el), _oracle_state(st), steps, prec=64)
+    assert np.abs(ref["v"] - ref_el["v"]).max() > 100 * (np.abs(out["v"] - ref["v"]).max() + 1e-7)
+
+
+def test_plastic_and_viscous_reject_differentiation_and_bad_parameters(gpu):
+    """The adjoint covers the elastic models and the inviscid fluid: the
+    checkpointed forward refuses ELASTOPLASTIC and viscous materials; a
+    yield stress <= 0 or a negative viscosity is an argument error."""
+    from physgrad_b200 import workloads as W
+
+    MT, CM = gpu.MaterialType, gpu.ConstitutiveModel
+    scenes, counts, _, st, _ = W.elastic_cube(n_particles=2000, n=16, seed=33)
+    for mat in (gpu.MaterialParameters(1000, 1e4, 0.3, MT.ELASTOPLASTIC, CM.NEO_HOOKEAN, yield_stress=1e3),
+                gpu.createFluidMaterial(1000, 1.0, 1e4)):
+        sim = _sim(gpu, scenes, counts, [mat], st)
+        sim.step(2)
+        with pytest.raises(Exception, match="differentiation"):
+            sim.forward_checkpointed(4, 2)
+    for mat, word in ((gpu.MaterialParameters(1000, 1e4, 0.3, MT.ELASTOPLASTIC, yield_stress=0.0), "yield_stress"),
+                      (gpu.createFluidMaterial(1000, -1.0, 1e4), "viscosity")):
+        with pytest.raises(Exception, match=word):
+            gpu.Simulator(scenes, counts, [mat])
 
 
 def test_graph_and_eager_agree(gpu):

@@ -135,3 +135,29 @@ def test_oracle_fp32_mirror_close_to_fp64(oracle):
     b = oracle.run(sc, mats, st, 10, prec=32)
     assert np.abs(a["x"] - b["x"]).max() < 1e-6
     assert np.abs(a["F"] - b["F"]).max() < 1e-5
+
+
+def test_oracle_plastic_and_viscous_models(oracle):
+    """ELASTOPLASTIC (model 3: neo-Hookean + von Mises cap) with an unreachable
+    yield stress is the neo-Hookean run bit for bit, and with a low one it
+    differs; a FLUID viscosity of 0 is the inviscid run bit for bit, and a
+    positive one changes it."""
+    rng = np.random.default_rng(5)
+    n, N = 16, 600
+    dx = 1.0 / n
+    st = _small_state(rng, N, dx, spread=0.08)
+    st["mat"] = np.zeros(N, np.int32)
+    sc = oracle.make_scene((n, n, n), dx, 1e-4, gravity=(0, -9.8, 0), boundary=1, bthick=2)
+    run = lambda mats: oracle.run(sc, oracle.make_materials(mats), st, 20, prec=64)
+    nh = run([(1, 1e4, 0.3)])
+    same = run([(3, 1e4, 0.3, 1e30)])
+    capped = run([(3, 1e4, 0.3, 10.0)])
+    for k in ("x", "v", "C", "F"):
+        assert np.array_equal(nh[k], same[k]), k
+    assert np.abs(capped["x"] - nh["x"]).max() > 1e-9 and np.isfinite(capped["x"]).all()
+    eos = run([(2, 1e4, 0.0)])
+    eos0 = run([(2, 1e4, 0.0, 0.0, 0.0)])
+    visc = run([(2, 1e4, 0.0, 0.0, 5.0)])
+    for k in ("x", "v", "C", "F"):
+        assert np.array_equal(eos[k], eos0[k]), k
+    assert np.abs(visc["v"] - eos["v"]).max() > 1e-6 and np.isfinite(visc["v"]).all()
