@@ -237,6 +237,19 @@ PGMPM_API int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* g
                    const float* gF_out, float* gx_in, float* gv_in, float* gC_in, float* gF_in, float* gE,
                    int32_t ptr_kind, void* stream);
 
+/* ---- output ---------------------------------------------------------------------- */
+/* Particle output in the legacy VTK format (binary, POLYDATA): points x, one
+ * vertex per particle, and point data "velocity" (v), "J" (det F) and
+ * "material" (id), each written when its array is given.  Host arrays in
+ * upload order; x: [n][3], v: [n][3], F: [n][9] row-major, mat: [n].  Needs
+ * no GPU.  This is the data output that MPMSolver::outputData()
+ * (src/mpm_solver.h:501-504) leaves as a stub. */
+PGMPM_API int pgmpm_vtk_write_particles(const char* path, int64_t n, const float* x, const float* v, const float* F,
+                                        const int32_t* mat, double time);
+/* The solver's particles (downloaded, upload order) to `path` as above, with
+ * material ids when the solver has more than one material. */
+PGMPM_API int pgmpm_write_vtk(pgmpm_solver s, const char* path, double time, void* stream);
+
 /* ---- inspection ------------------------------------------------------------------ */
 #define PGMPM_ARRAY_USER_INDEX 0   /* physical slot -> upload index */
 #define PGMPM_ARRAY_KEYS 1         /* cell key per physical slot (input of the next sort) */

@@ -16,6 +16,8 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
+#include <filesystem>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -104,6 +106,13 @@ struct MPMSolverConfig {
     bool enable_g2p2g_fusion = true;
     bool enable_adaptive_timestep = false;
     bool enable_profiling = false;
+    // output (src/mpm_solver.h:57-60): run() writes the particles every
+    // output_frequency seconds of simulated time as
+    // output_directory/frame_NNNNN.vtk (legacy binary VTK).  Off by default
+    // here: the reference's outputData() only prints a line.
+    bool enable_output = false;
+    float output_frequency = 0.01f;
+    std::string output_directory = "./mpm_output";
     // additions of this implementation
     int physics = PGMPM_PHYSICS_MLS;
     int boundary = PGMPM_BC_STICKY;
@@ -243,9 +252,31 @@ public:
     void run() {
         initialize();
         const int n = (int)(config_.simulation_time / config_.time_step + 0.5f);
-        physgrad_b200_detail::check(pgmpm_step(h_, n, nullptr));
-        time_ += n * config_.time_step;
-        step_ += n;
+        if (!config_.enable_output) {
+            physgrad_b200_detail::check(pgmpm_step(h_, n, nullptr));
+            time_ += n * config_.time_step;
+            step_ += n;
+            return;
+        }
+        // the steps between outputs run as one call; a frame is written after
+        // each step that crosses a multiple of output_frequency (the
+        // reference's test, src/mpm_solver.h:306-311)
+        std::filesystem::create_directories(config_.output_directory);
+        int done = 0, frame = 0;
+        while (done < n) {
+            int k = 1;
+            while (done + k < n && !crosses_output(time_ + k * config_.time_step)) ++k;
+            physgrad_b200_detail::check(pgmpm_step(h_, k, nullptr));
+            done += k;
+            step_ += k;
+            time_ += k * config_.time_step;
+            if (crosses_output(time_)) {
+                char name[32];
+                std::snprintf(name, sizeof(name), "/frame_%05d.vtk", frame++);
+                physgrad_b200_detail::check(pgmpm_write_vtk(h_, (config_.output_directory + name).c_str(), time_,
+                                                            nullptr));
+            }
+        }
     }
 
     const particle_container& getParticles() {
@@ -289,6 +320,10 @@ public:
     }
 
     float getCurrentTime() const { return time_; }
+    // Write the particles now (legacy binary VTK; see pgmpm_write_vtk).
+    void outputData(const std::string& path) {
+        physgrad_b200_detail::check(pgmpm_write_vtk(h_, path.c_str(), time_, nullptr));
+    }
     int getCurrentStep() const { return step_; }
     pgmpm_solver handle() const { return h_; }
 
@@ -301,6 +336,11 @@ private:
     particle_container particles_;
     grid_container grid_;
     MPMPerformanceMetrics metrics_;
+    // the step that ended at simulated time t crossed a multiple of output_frequency
+    bool crosses_output(float t) const {
+        return config_.output_frequency > 0.f && (int)(t / config_.output_frequency) >
+                                                     (int)((t - config_.time_step) / config_.output_frequency);
+    }
     float time_ = 0.f;
     int step_ = 0;
 };

@@ -117,6 +117,8 @@ SIGNATURES = {
     "pgmpm_set_materials": (ctypes.c_int, [_vp, ctypes.POINTER(Material), _i32]),
     "pgmpm_upload": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "pgmpm_download": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "pgmpm_vtk_write_particles": (ctypes.c_int, [ctypes.c_char_p, _i64, _vp, _vp, _vp, _vp, ctypes.c_double]),
+    "pgmpm_write_vtk": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_double, _vp]),
     "pgmpm_download_grid": (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
     "pgmpm_step": (ctypes.c_int, [_vp, _i32, _vp]),
     "pgmpm_advance_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),

@@ -514,6 +514,87 @@ int pgmpm_download(pgmpm_solver s, float* x, float* v, float* C, float* F, int32
     return PGMPM_OK;
 }
 
+int pgmpm_vtk_write_particles(const char* path, int64_t n, const float* x, const float* v, const float* F,
+                              const int32_t* mat, double time) {
+    if (!path || n < 0 || (n > 0 && !x)) return fail(PGMPM_ERR_ARG, "vtk: need a path and positions");
+    if (n > ((int64_t)1 << 30)) return fail(PGMPM_ERR_ARG, "vtk: more than 2^30 particles (legacy VTK uses int32)");
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(PGMPM_ERR_ARG, "vtk: cannot open %s for writing", path);
+    // the legacy binary format is big-endian
+    std::vector<unsigned char> buf;
+    auto put = [&](uint32_t w) {
+        buf.push_back((unsigned char)(w >> 24));
+        buf.push_back((unsigned char)(w >> 16));
+        buf.push_back((unsigned char)(w >> 8));
+        buf.push_back((unsigned char)w);
+    };
+    auto putf = [&](float a) {
+        uint32_t w;
+        std::memcpy(&w, &a, 4);
+        put(w);
+    };
+    auto text = [&](const char* fmt, auto... a) {
+        char line[256];
+        const int k = std::snprintf(line, sizeof(line), fmt, a...);
+        buf.insert(buf.end(), line, line + k);
+    };
+    const long long nn = (long long)n;
+    buf.reserve((size_t)n * 36 + 512);
+    text("# vtk DataFile Version 3.0\nphysgrad_b200 MPM particles, t = %.9g\nBINARY\nDATASET POLYDATA\n", time);
+    text("POINTS %lld float\n", nn);
+    for (int64_t i = 0; i < 3 * n; ++i) putf(x[i]);
+    text("\nVERTICES %lld %lld\n", nn, 2 * nn);
+    for (int64_t i = 0; i < n; ++i) {
+        put(1u);
+        put((uint32_t)i);
+    }
+    text("\nPOINT_DATA %lld\n", nn);
+    if (v) {
+        text("VECTORS velocity float\n");
+        for (int64_t i = 0; i < 3 * n; ++i) putf(v[i]);
+        text("\n");
+    }
+    if (F) {
+        text("SCALARS J float 1\nLOOKUP_TABLE default\n");
+        for (int64_t i = 0; i < n; ++i) {
+            const float* a = F + 9 * i;
+            putf(a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                 a[2] * (a[3] * a[7] - a[4] * a[6]));
+        }
+        text("\n");
+    }
+    if (mat) {
+        text("SCALARS material int 1\nLOOKUP_TABLE default\n");
+        for (int64_t i = 0; i < n; ++i) put((uint32_t)mat[i]);
+        text("\n");
+    }
+    const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+    const bool closed = std::fclose(f) == 0;
+    if (!ok || !closed) return fail(PGMPM_ERR_ARG, "vtk: writing %s failed", path);
+    return PGMPM_OK;
+}
+
+int pgmpm_write_vtk(pgmpm_solver s, const char* path, double time, void* stream) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    const int64_t N = s->N;
+    std::vector<float> x(3 * N), v(3 * N), F(9 * N);
+    int rc = pgmpm_download(s, x.data(), v.data(), nullptr, F.data(), PGMPM_PTR_HOST, stream);
+    if (rc) return rc;
+    std::vector<int32_t> mat;
+    if (s->pf.multi_mat && N > 0) {  // physical order on the device -> upload order
+        DeviceGuard dg(s->device);
+        std::vector<int32_t> mp(N);
+        std::vector<uint32_t> u(N);
+        CK(cudaMemcpy(mp.data(), s->mat.p, sizeof(int32_t) * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(u.data(), s->user_of_phys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost));
+        mat.assign(N, 0);
+        for (int64_t i = 0; i < N; ++i)
+            if (u[i] < (uint64_t)N) mat[u[i]] = mp[i];
+    }
+    return pgmpm_vtk_write_particles(path, N, x.data(), v.data(), F.data(), mat.empty() ? nullptr : mat.data(), time);
+}
+
 int pgmpm_download_grid(pgmpm_solver s, int32_t scene, float* mass, float* velocity, int32_t ptr_kind,
                         void* stream) {
     if (!s || scene < 0 || scene >= s->S) return fail(PGMPM_ERR_ARG, "bad solver or scene");

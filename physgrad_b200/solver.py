@@ -11,6 +11,7 @@ src/material_point_method.h:430-506 (PIC physics of the reference CPU path).
 from __future__ import annotations
 
 import ctypes
+import os
 import enum
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
@@ -213,6 +214,11 @@ class Simulator:
             raise ValueError("mix of host and device inputs")
         k = kind[0] if kind else C.PTR_HOST
         check(lib().pgmpm_upload(self._h, px, pv, pC, pF, pm, pV, pmat, k, _stream_handle(stream)))
+
+    def write_vtk(self, path: str, time: float = 0.0, stream=None):
+        """The particles (upload order) as a legacy binary VTK file: points,
+        velocity, J = det F and, with several materials, the material id."""
+        check(lib().pgmpm_write_vtk(self._h, os.fsencode(path), float(time), _stream_handle(stream)))
 
     def download(self, out: Optional[dict] = None, stream=None):
         """State in upload order: numpy arrays, or into the CUDA tensors of ``out``."""

@@ -10,7 +10,24 @@
 
 using namespace physgrad::mpm;
 
-int main() {
+int main(int argc, char** argv) {
+    if (argc > 1) {
+        // output run: frames every 2.5e-4 s of simulated time into argv[1]
+        MPMSolverConfig oc;
+        oc.grid_dimensions = {32, 32, 32};
+        oc.grid_spacing = {1.f / 32, 1.f / 32, 1.f / 32};
+        oc.simulation_time = 1e-3f;
+        oc.enable_output = true;
+        oc.output_frequency = 2.5e-4f;
+        oc.output_directory = argv[1];
+        MPMSolver<float> os(oc);
+        std::vector<T3> ox(512, T3{0.5f, 0.5f, 0.5f}), ov(512, T3{0.f, 0.f, 0.f});
+        for (size_t i = 0; i < ox.size(); ++i) ox[i].x += 0.0005f * (float)(i % 64);
+        os.addParticles(ox, ov, std::vector<float>(512, 1.25e-4f), MaterialType::ELASTIC);
+        os.run();
+        std::printf("{\"output_steps\": %d}\n", os.getCurrentStep());
+        return 0;
+    }
     MPMSolverConfig cfg;
     cfg.grid_dimensions = {32, 32, 32};
     cfg.grid_spacing = {1.f / 32, 1.f / 32, 1.f / 32};

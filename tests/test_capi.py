@@ -116,3 +116,34 @@ def test_workloads_are_seeded_and_shaped():
     assert all(s.n[0] == (32 if c < 16384 else 64 if c < 131072 else 128) for s, c in zip(sc, counts))
     assert st["x"].shape[0] == sum(counts)
     assert np.array_equal(np.unique(st["mat"]), np.arange(64))
+
+
+def test_vtk_writer_round_trip(built_lib, read_vtk, tmp_path):
+    """pgmpm_vtk_write_particles (host arrays, no GPU): points, one vertex per
+    particle, velocity, J = det F and material ids read back exactly."""
+    import numpy as np
+
+    from physgrad_b200 import _capi as C
+
+    L = C.lib()
+    rng = np.random.default_rng(0)
+    n = 37
+    x = rng.random((n, 3), dtype=np.float32)
+    v = rng.standard_normal((n, 3)).astype(np.float32)
+    F = (np.eye(3) + 0.1 * rng.standard_normal((n, 3, 3))).astype(np.float32)
+    mat = (np.arange(n) % 3).astype(np.int32)
+    path = str(tmp_path / "p.vtk")
+    ptr = lambda a: a.ctypes.data
+    assert L.pgmpm_vtk_write_particles(path.encode(), n, ptr(x), ptr(v), ptr(F), ptr(mat), 0.25) == 0
+    r = read_vtk(path)
+    assert "t = 0.25" in r["header"]
+    assert np.array_equal(r["x"], x) and np.array_equal(r["velocity"], v) and np.array_equal(r["material"], mat)
+    assert np.array_equal(r["vertices"], np.stack([np.ones(n, np.int32), np.arange(n, dtype=np.int32)], 1))
+    assert np.allclose(r["J"], np.linalg.det(F.astype(np.float64)), rtol=1e-5, atol=1e-6)
+    # positions only; a bad path is an argument error with a message
+    assert L.pgmpm_vtk_write_particles(path.encode(), n, ptr(x), None, None, None, 0.0) == 0
+    r = read_vtk(path)
+    assert r["velocity"] is None and r["J"] is None and np.array_equal(r["x"], x)
+    assert L.pgmpm_vtk_write_particles(str(tmp_path / "no" / "dir.vtk").encode(), n, ptr(x), None, None, None,
+                                       0.0) == C.PGMPM_ERR_ARG
+    assert b"cannot open" in L.pgmpm_last_error()

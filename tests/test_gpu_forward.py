@@ -422,6 +422,23 @@ def test_plastic_and_viscous_reject_differentiation_and_bad_parameters(gpu):
             gpu.Simulator(scenes, counts, [mat])
 
 
+def test_write_vtk_matches_download(gpu, read_vtk, tmp_path):
+    """Simulator.write_vtk (pgmpm_write_vtk): the file's points, velocity,
+    J = det F and material ids are the downloaded state in upload order."""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.two_material_drop(n_particles=20000, n=32, seed=41)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(7)
+    path = str(tmp_path / "frame.vtk")
+    sim.write_vtk(path, time=7e-4)
+    out = sim.download()
+    r = read_vtk(path)
+    assert np.array_equal(r["x"], out["x"]) and np.array_equal(r["velocity"], out["v"])
+    assert np.array_equal(r["material"], st["mat"])
+    assert np.allclose(r["J"], np.linalg.det(out["F"].reshape(-1, 3, 3).astype(np.float64)), rtol=1e-5, atol=1e-6)
+
+
 def test_graph_and_eager_agree(gpu):
     from physgrad_b200 import workloads as W
 
