@@ -569,13 +569,94 @@ def run_reference(args):
     return line
 
 
+def run_hashgrid(args, device=0):
+    """Spatial hash grid (physgrad_b200.SpatialHashGrid over pgmpm_hashgrid_*):
+    4,194,304 particles uniform in the unit cube, cell 1/160 (4,096,000 cells,
+    not a power of two, so Morton buckets collide as in the reference), radius
+    one cell (27 cells per query), every particle also a query.  Build and query
+    timed with CUDA events over device arrays; the reference's own host class
+    (oracle/_ref) timed on a 1/16 sample for the CPU baseline."""
+    import ctypes
+
+    import torch
+
+    import physgrad_b200 as pg
+    from physgrad_b200 import _capi as C
+
+    torch.cuda.set_device(device)
+    N, cs = 1 << 22, 1.0 / 160
+    r = cs
+    rng = np.random.default_rng(0)
+    p = rng.random((N, 3), dtype=np.float32)
+    grid = pg.SpatialHashGrid(cs, (0, 0, 0), (1, 1, 1), max_particles=N, device=device)
+    L = C.lib()
+    st = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(st.cuda_stream)
+    pd = torch.tensor(p, device=f"cuda:{device}")
+    off = torch.zeros(N + 1, dtype=torch.int64, device=f"cuda:{device}")
+    tot = ctypes.c_int64()
+    C.check(L.pgmpm_hashgrid_build(grid._h, pd.data_ptr(), N, C.PTR_DEVICE, sh))
+    C.check(L.pgmpm_hashgrid_neighbors(grid._h, pd.data_ptr(), N, r, off.data_ptr(), None, 0, ctypes.byref(tot),
+                                       C.PTR_DEVICE, sh))
+    out = torch.empty(tot.value, dtype=torch.int32, device=f"cuda:{device}")
+
+    def build():
+        C.check(L.pgmpm_hashgrid_build(grid._h, pd.data_ptr(), N, C.PTR_DEVICE, sh))
+
+    def query():
+        C.check(L.pgmpm_hashgrid_neighbors(grid._h, pd.data_ptr(), N, r, off.data_ptr(), out.data_ptr(), tot.value,
+                                           ctypes.byref(tot), C.PTR_DEVICE, sh))
+
+    K = max(3, min(args.steps, 20))
+    res = {}
+    for name, fn in (("build", build), ("query", query)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(K):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / K
+    build_rate = N / (res["build"] * 1e-3)
+    line = {"metric": "particles/s (spatial hash grid build)", "value": build_rate, "unit": "particles/s",
+            "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": res["build"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/u32", "data": "synthetic (seeded uniform)",
+            "config": {"workload": "spatial hash grid", "n_particles": N, "cell_size": cs, "cells": grid.total_cells,
+                       "radius": r, "queries": N, "l2": "inputs + table + sort buffers ~ 200 MB > L2"},
+            "query": {"ms": res["query"], "queries_per_s": N / (res["query"] * 1e-3),
+                      "neighbors_per_query": tot.value / N, "neighbors_per_s": tot.value / (res["query"] * 1e-3)},
+            "gpu_launches": {"build": 2 + 3 * 3, "query": 5}}
+    # the reference's host class on a 1/16 sample (same density: a smaller cube)
+    try:
+        from oracle import hashgrid as H
+
+        if not args.no_cpu_baseline and H.reference_available():
+            import time
+
+            n = N // 16
+            side = float(np.float32((1.0 / 16) ** (1.0 / 3)))
+            ps = (p[:n] * side).astype(np.float32)
+            t0 = time.perf_counter()
+            H.reference_build_and_query(ps, ps[: n // 8], r, cs, (0, 0, 0), (side, side, side))
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": n / dt, "unit": "particles/s (build + queries of 1/8 of them)",
+                                    "cores": 1, "kind": "reference",
+                                    "sample": f"{n} particles at the same density, {n // 8} queries, one thread"}
+    except Exception as e:  # the baseline is optional
+        line["cpu_baseline"] = {"unavailable": str(e)[:120]}
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint", "hashgrid"])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="cfg4/cfg5: plain bench line instead of the batched comparison")
@@ -599,6 +680,8 @@ def main():
     try:
         if args.workload == "cfg3_adjoint" and world == 1:
             line = run_adjoint(args, local)
+        elif args.workload == "hashgrid" and world == 1:
+            line = run_hashgrid(args, local)
         elif args.workload in ("cfg4", "cfg5") and world == 1 and not args.plain:
             line = run_batched(args, local, adjoint=args.workload == "cfg5")
         else:

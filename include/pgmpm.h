@@ -250,6 +250,49 @@ PGMPM_API int pgmpm_vtk_write_particles(const char* path, int64_t n, const float
  * material ids when the solver has more than one material. */
 PGMPM_API int pgmpm_write_vtk(pgmpm_solver s, const char* path, double time, void* stream);
 
+/* ---- spatial hash grid (particle neighbourhoods) ------------------------------ */
+/* physgrad::sparse::SpatialHashGrid<float, uint32_t> (src/sparse_data_structures.h:44-296,
+ * used by src/fsi_coupling.h:72) on the GPU.  Cells of size cell_size tile
+ * [domain_min, domain_max); a point's cell id is morton(cell) % total_cells
+ * with the cell clamped to the resolution, as getCellID (:143-151).  The
+ * table (per-cell counts and starts, particle indices sorted by cell, stable
+ * within a cell, and the cell id of each particle) equals buildHashTable's
+ * (:155-190) bit for bit. */
+typedef struct pgmpm_hashgrid_s* pgmpm_hashgrid;
+typedef struct {
+    float average_particles_per_cell; /* over occupied cells (HashTableStats, :243-272) */
+    float load_factor;                /* occupied / total cells */
+    uint32_t max_particles_per_cell;
+    uint32_t occupied_cells;
+    float memory_usage_mb;            /* the host class's accounting */
+    uint32_t total_cells;
+    uint32_t resolution[3];
+} pgmpm_hashgrid_info;
+/* SpatialHashGrid(cell_size, domain_min, domain_max, max_particles) (:76-97). */
+PGMPM_API int pgmpm_hashgrid_create(float cell_size, const float* domain_min, const float* domain_max,
+                                    int64_t max_particles, int32_t device, pgmpm_hashgrid* out);
+PGMPM_API int pgmpm_hashgrid_destroy(pgmpm_hashgrid g);
+/* buildHashTable(positions [n][3], n) (:155-190). */
+PGMPM_API int pgmpm_hashgrid_build(pgmpm_hashgrid g, const float* positions, int64_t n, int32_t ptr_kind,
+                                   void* stream);
+/* getNeighbors(x, y, z, radius) (:206-240) for nq query points [nq][3]:
+ * query i's list is indices[offsets[i] .. offsets[i+1]), offsets has nq + 1
+ * entries and *total = offsets[nq].  As the host class, a list holds every
+ * particle of the (2 ceil(radius / cell_size) + 1)^3 cells around the query's
+ * cell in that method's order, without a distance test.  indices are
+ * written only when capacity >= *total (else call again with room for it). */
+PGMPM_API int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq, float radius,
+                                       int64_t* offsets, uint32_t* indices, int64_t capacity, int64_t* total,
+                                       int32_t ptr_kind, void* stream);
+/* getCellParticleCounts / getCellStartIndices (total_cells entries),
+ * getParticleIndices and the cell ids (n entries) of the last build; NULL
+ * skips an array. */
+PGMPM_API int pgmpm_hashgrid_get_table(pgmpm_hashgrid g, uint32_t* counts, uint32_t* starts,
+                                       uint32_t* particle_indices, uint32_t* cell_ids, int32_t ptr_kind,
+                                       void* stream);
+/* getStats() (:243-272); before a build the particle fields are zero. */
+PGMPM_API int pgmpm_hashgrid_stats(pgmpm_hashgrid g, pgmpm_hashgrid_info* out);
+
 /* ---- inspection ------------------------------------------------------------------ */
 #define PGMPM_ARRAY_USER_INDEX 0   /* physical slot -> upload index */
 #define PGMPM_ARRAY_KEYS 1         /* cell key per physical slot (input of the next sort) */

@@ -17,9 +17,10 @@ from .solver import (  # noqa: F401
     createFluidMaterial,
     radix_sort_pairs,
 )
+from .hashgrid import SpatialHashGrid  # noqa: F401
 
 __all__ = [
     "PGMPMError", "lib", "BoundaryType", "ConstitutiveModel", "MaterialParameters", "MaterialType", "MPMSolver",
     "MPMSolverConfig", "RefCompatSolver", "Scene", "Simulator", "createElasticMaterial", "createFluidMaterial",
-    "radix_sort_pairs",
+    "radix_sort_pairs", "SpatialHashGrid",
 ]

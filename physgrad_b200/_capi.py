@@ -104,6 +104,18 @@ class Metrics(ctypes.Structure):
     ]
 
 
+class HashGridInfo(ctypes.Structure):
+    _fields_ = [
+        ("average_particles_per_cell", ctypes.c_float),
+        ("load_factor", ctypes.c_float),
+        ("max_particles_per_cell", ctypes.c_uint32),
+        ("occupied_cells", ctypes.c_uint32),
+        ("memory_usage_mb", ctypes.c_float),
+        ("total_cells", ctypes.c_uint32),
+        ("resolution", ctypes.c_uint32 * 3),
+    ]
+
+
 # name -> (restype, argtypes)
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -119,6 +131,13 @@ SIGNATURES = {
     "pgmpm_download": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "pgmpm_vtk_write_particles": (ctypes.c_int, [ctypes.c_char_p, _i64, _vp, _vp, _vp, _vp, ctypes.c_double]),
     "pgmpm_write_vtk": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_double, _vp]),
+    "pgmpm_hashgrid_create": (ctypes.c_int, [ctypes.c_float, _vp, _vp, _i64, _i32, ctypes.POINTER(_vp)]),
+    "pgmpm_hashgrid_destroy": (ctypes.c_int, [_vp]),
+    "pgmpm_hashgrid_build": (ctypes.c_int, [_vp, _vp, _i64, _i32, _vp]),
+    "pgmpm_hashgrid_neighbors": (ctypes.c_int, [_vp, _vp, _i64, ctypes.c_float, _vp, _vp, _i64,
+                                                ctypes.POINTER(_i64), _i32, _vp]),
+    "pgmpm_hashgrid_get_table": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "pgmpm_hashgrid_stats": (ctypes.c_int, [_vp, ctypes.POINTER(HashGridInfo)]),
     "pgmpm_download_grid": (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
     "pgmpm_step": (ctypes.c_int, [_vp, _i32, _vp]),
     "pgmpm_advance_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),

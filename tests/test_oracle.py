@@ -161,3 +161,45 @@ def test_oracle_plastic_and_viscous_models(oracle):
     for k in ("x", "v", "C", "F"):
         assert np.array_equal(eos[k], eos0[k]), k
     assert np.abs(visc["v"] - eos["v"]).max() > 1e-6 and np.isfinite(visc["v"]).all()
+
+
+def _hashgrid_case(g, k):
+    prm = g[f"c{k}_param"]
+    return float(prm[0]), prm[1:4], prm[4:7], float(prm[7])
+
+
+def test_hashgrid_oracle_matches_reference_golden():
+    """oracle/hashgrid.py (restated SpatialHashGrid, src/sparse_data_structures.h)
+    reproduces the reference class's table and getNeighbors lists bit for bit
+    on the committed fixture, points and queries outside the domain included."""
+    from oracle import hashgrid as H
+
+    g = np.load(os.path.join(GOLDEN, "hashgrid_small.npz"))
+    for k in range(3):
+        cs, mn, mx, r = _hashgrid_case(g, k)
+        c, s, ix, ids = H.build(g[f"c{k}_p"], cs, mn, mx)
+        assert np.array_equal(c, g[f"c{k}_counts"]) and np.array_equal(s, g[f"c{k}_starts"])
+        assert np.array_equal(ix, g[f"c{k}_indices"])
+        o, l = H.neighbors(g[f"c{k}_q"], r, cs, mn, mx, c, s, ix)
+        assert np.array_equal(o, g[f"c{k}_offsets"]) and np.array_equal(l, g[f"c{k}_lists"])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref",
+                                                    "libref_hashgrid.so")), reason="reference build absent")
+def test_hashgrid_oracle_matches_reference_live():
+    """The same pin on seeded random cases, live against oracle/_ref."""
+    from oracle import hashgrid as H
+
+    rng = np.random.default_rng(7)
+    for _ in range(5):
+        n, cs = int(rng.integers(1, 2000)), float(rng.choice([0.04, 0.07, 0.1]))
+        mn = rng.uniform(-1, 0, 3).astype(np.float32)
+        mx = (mn + rng.uniform(0.4, 1.2, 3)).astype(np.float32)
+        p = (mn + rng.random((n, 3)) * (mx - mn)).astype(np.float32)
+        q = (mn - 0.1 + rng.random((40, 3)) * (mx - mn + 0.2)).astype(np.float32)
+        r = float(rng.choice([0.0, 0.05, 0.15]))
+        c, s, ix, _ = H.build(p, cs, mn, mx)
+        o, l = H.neighbors(q, r, cs, mn, mx, c, s, ix)
+        rc, rs, rix, ro, rl = H.reference_build_and_query(p, q, r, cs, mn, mx)
+        for a, b in ((c, rc), (s, rs), (ix, rix), (o, ro), (l, rl)):
+            assert np.array_equal(a, b)
