@@ -14,8 +14,8 @@
 //              (2 ceil(r / cell) + 1)^3 block around its cell, in the
 //              reference's order (x outer, z inner; a cell's particles by
 //              index), with no distance test -- as getNeighbors (:206-240),
-//              which computes radius^2 but does not use it.  Two passes: a
-//              count per query, a scan into offsets, then the fill.
+//              which computes radius^2 but does not use it.  Two passes (one
+//              warp per query): a count, a scan into offsets, then the fill.
 //
 // Float arithmetic is IEEE single (no contraction), so cell ids match the
 // reference's host code bit for bit.
@@ -99,51 +99,68 @@ __global__ void k_hg_table(const uint32_t* __restrict__ sorted_ids, uint32_t n, 
     counts[c] = e - s;
 }
 
-// Visits the cells of query q's block in the reference's order; for each
-// in-range cell calls f(start, count).
-template <class F>
-__device__ __forceinline__ void hg_visit(const HGDev& G, const float* q, uint32_t src, const uint32_t* counts,
-                                         const uint32_t* starts, F&& f) {
-    uint32_t c[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[a], G.dmin[a], G.cell);
-    for (uint32_t dx = 0; dx <= 2 * src; ++dx) {
-        const uint32_t gx = c[0] + dx - src;  // uint32 wrap: below 0 fails the range test
-        if (gx >= G.res[0]) continue;
-        for (uint32_t dy = 0; dy <= 2 * src; ++dy) {
-            const uint32_t gy = c[1] + dy - src;
-            if (gy >= G.res[1]) continue;
-            for (uint32_t dz = 0; dz <= 2 * src; ++dz) {
-                const uint32_t gz = c[2] + dz - src;
-                if (gz >= G.res[2]) continue;
-                const uint32_t id = hg_morton(gx, gy, gz) % G.total;
-                f(starts[id], counts[id]);
-            }
-        }
-    }
+// One warp per query: lanes take the block's cells in the reference's order
+// (linear index t = (dx (2s+1) + dy) (2s+1) + dz), 32 at a time; the count
+// pass sums them, the fill pass gives each cell its place by a scan over the
+// lanes and copies the cell's particles, so a query's list is written by a
+// whole warp into one contiguous stretch.
+__device__ __forceinline__ bool hg_cell_of(const HGDev& G, const uint32_t c[3], uint32_t src, uint32_t t,
+                                           uint32_t& id) {
+    const uint32_t w = 2 * src + 1;
+    const uint32_t dz = t % w, dy = (t / w) % w, dx = t / (w * w);
+    const uint32_t gx = c[0] + dx - src, gy = c[1] + dy - src, gz = c[2] + dz - src;  // wrap: below 0 fails
+    if (gx >= G.res[0] || gy >= G.res[1] || gz >= G.res[2]) return false;
+    id = hg_morton(gx, gy, gz) % G.total;
+    return true;
 }
 
 __global__ void k_hg_qcount(HGDev G, const float* __restrict__ q, int64_t nq, uint32_t src,
-                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ starts,
-                            uint32_t* __restrict__ qcount) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nq) return;
+                            const uint32_t* __restrict__ counts, uint32_t* __restrict__ qcount) {
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= nq) return;  // whole warps leave together
+    uint32_t c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[3 * i + a], G.dmin[a], G.cell);
+    const uint32_t ncell = (2 * src + 1) * (2 * src + 1) * (2 * src + 1);
     uint32_t k = 0;
-    hg_visit(G, q + 3 * i, src, counts, starts, [&](uint32_t, uint32_t cnt) { k += cnt; });
-    qcount[i] = k;
+    for (uint32_t t = lane; t < ncell; t += 32) {
+        uint32_t id;
+        if (hg_cell_of(G, c, src, t, id)) k += counts[id];
+    }
+    k = __reduce_add_sync(0xFFFFFFFFu, k);
+    if (lane == 0) qcount[i] = k;
 }
 
 __global__ void k_hg_qfill(HGDev G, const float* __restrict__ q, int64_t nq, uint32_t src,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ starts,
                            const uint32_t* __restrict__ sorted_index, const int64_t* __restrict__ offsets,
                            uint32_t* __restrict__ out) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (i >= nq) return;
+    uint32_t c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[3 * i + a], G.dmin[a], G.cell);
+    const uint32_t ncell = (2 * src + 1) * (2 * src + 1) * (2 * src + 1);
     int64_t o = offsets[i];
-    hg_visit(G, q + 3 * i, src, counts, starts, [&](uint32_t s, uint32_t cnt) {
-        for (uint32_t j = 0; j < cnt; ++j) out[o + j] = sorted_index[s + j];
-        o += cnt;
-    });
+    for (uint32_t t0 = 0; t0 < ncell; t0 += 32) {
+        const uint32_t t = t0 + lane;
+        uint32_t id = 0, k = 0, s0 = 0;
+        if (t < ncell && hg_cell_of(G, c, src, t, id)) {
+            k = counts[id];
+            s0 = starts[id];
+        }
+        uint32_t x = k;  // inclusive scan of the counts over the lanes
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+            if (lane >= d) x += y;
+        }
+        const int64_t base = o + (x - k);
+        for (uint32_t j = 0; j < k; ++j) out[base + j] = sorted_index[s0 + j];
+        o += __shfl_sync(0xFFFFFFFFu, x, 31);
+    }
 }
 
 // Exclusive scan of n uint32 counts into int64 offsets[0..n] (offsets[n] =
@@ -370,7 +387,8 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
         return fail(PGMPM_ERR_ARG, "hashgrid: bad query arguments");
     if (ptr_kind != PGMPM_PTR_HOST && ptr_kind != PGMPM_PTR_DEVICE) return fail(PGMPM_ERR_ARG, "bad ptr_kind");
     const float sr = std::ceil(radius / g->cell);  // single precision, as the host class
-    if (!(sr < 1024.f)) return fail(PGMPM_ERR_ARG, "hashgrid: radius spans more than 1023 cells");
+    // (2 src + 1)^3 cells per query must count in uint32
+    if (!(sr < 512.f)) return fail(PGMPM_ERR_ARG, "hashgrid: radius spans more than 511 cells");
     const uint32_t src = (uint32_t)sr;
     DeviceGuard dg(g->device);
     cudaStream_t st = ST(stream);
@@ -386,8 +404,8 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
     int64_t* bsum = g->scan_tmp.as<int64_t>();
     int64_t* doff = ptr_kind == PGMPM_PTR_HOST ? bsum + nb : offsets;
     if (nq > 0) {
-        k_hg_qcount<<<blocks_of(nq, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
-                                                          g->starts.as<uint32_t>(), g->qcount.as<uint32_t>());
+        k_hg_qcount<<<blocks_of(nq * 32, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
+                                                               g->qcount.as<uint32_t>());
         k_scan_sums<<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum);
         k_scan_carry<<<1, SCAN_T, 0, st>>>(bsum, nb);
         k_scan_apply<<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum, doff);
@@ -407,8 +425,9 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
             CK(out_stage.alloc(sizeof(uint32_t) * tot));
             dout = out_stage.as<uint32_t>();
         }
-        k_hg_qfill<<<blocks_of(nq, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
-                                                         g->starts.as<uint32_t>(), g->va.as<uint32_t>(), doff, dout);
+        k_hg_qfill<<<blocks_of(nq * 32, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
+                                                              g->starts.as<uint32_t>(), g->va.as<uint32_t>(), doff,
+                                                              dout);
         CK(cudaGetLastError());
         if (ptr_kind == PGMPM_PTR_HOST)
             CK(cudaMemcpyAsync(indices, dout, sizeof(uint32_t) * tot, cudaMemcpyDeviceToHost, st));
