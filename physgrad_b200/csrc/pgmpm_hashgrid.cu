@@ -6,10 +6,10 @@
 //   cell id    morton(c) % total_cells, c = the cell coordinates of a point,
 //              truncated to uint32 and clamped to the resolution (the
 //              reference's getCellID, :143-151, Morton code :121-131)
-//   build      stable sort of (cell id, particle index) pairs (the existing
-//              LSD radix sort), then per cell its start (a lower bound in
-//              the sorted ids) and count: the reference's count / exclusive
-//              scan / stable fill (:155-190) give the same arrays
+//   build      per-cell counts (a histogram of the cell ids), starts (their
+//              exclusive scan) and a stable sort of (cell id, particle index)
+//              pairs (the existing LSD radix sort): the reference's count /
+//              exclusive scan / stable fill (:155-190) give the same arrays
 //   neighbours for a query point, every particle stored in the cells of the
 //              (2 ceil(r / cell) + 1)^3 block around its cell, in the
 //              reference's order (x outer, z inner; a cell's particles by
@@ -52,7 +52,15 @@ constexpr int HG_T = 256;
 struct HGDev {
     float cell, dmin[3];
     uint32_t res[3], total;
+    unsigned long long total_m;  // 2^64 / total + 1 (mod 2^64), for hg_mod
 };
+
+// a % total by direct computation of the remainder (Lemire, Kaser and Kurz,
+// "Faster remainder by direct computation", 2019): for 32-bit a and d and
+// M = floor(2^64 / d) + 1, a mod d = floor(((M a) mod 2^64) d / 2^64).
+__device__ __forceinline__ uint32_t hg_mod(uint32_t a, const HGDev& G) {
+    return (uint32_t)__umul64hi(G.total_m * (unsigned long long)a, (unsigned long long)G.total);
+}
 
 // src/sparse_data_structures.h:121-128: bit interleave in uint32 arithmetic
 __device__ __forceinline__ uint32_t hg_expand(uint32_t v) {
@@ -71,32 +79,21 @@ __device__ __forceinline__ uint32_t hg_coord(float x, float mn, float cell) {
     return (uint32_t)(unsigned long long)__float2ll_rz(__fdiv_rn(__fsub_rn(x, mn), cell));
 }
 
-__global__ void k_hg_cells(HGDev G, const float* __restrict__ pos, int64_t n, uint32_t* __restrict__ cell_ids) {
+// cell id per particle, and the per-cell counts (warp-aggregated atomics)
+__global__ void k_hg_cells(HGDev G, const float* __restrict__ pos, int64_t n, uint32_t* __restrict__ cell_ids,
+                           uint32_t* __restrict__ counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint32_t c[3];
+    const bool act = i < n;
+    uint32_t id = 0xFFFFFFFFu;
+    if (act) {
+        uint32_t c[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) c[a] = min(hg_coord(pos[3 * i + a], G.dmin[a], G.cell), G.res[a] - 1u);
-    cell_ids[i] = hg_morton(c[0], c[1], c[2]) % G.total;
-}
-
-// start of cell c = number of sorted ids below c; count = start(c + 1) - start(c)
-__device__ __forceinline__ uint32_t hg_lower_bound(const uint32_t* __restrict__ a, uint32_t n, uint32_t v) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
+        for (int a = 0; a < 3; ++a) c[a] = min(hg_coord(pos[3 * i + a], G.dmin[a], G.cell), G.res[a] - 1u);
+        id = hg_mod(hg_morton(c[0], c[1], c[2]), G);
+        cell_ids[i] = id;
     }
-    return lo;
-}
-__global__ void k_hg_table(const uint32_t* __restrict__ sorted_ids, uint32_t n, uint32_t total,
-                           uint32_t* __restrict__ starts, uint32_t* __restrict__ counts) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= total) return;
-    const uint32_t s = hg_lower_bound(sorted_ids, n, c);
-    const uint32_t e = c + 1 == total ? n : hg_lower_bound(sorted_ids, n, c + 1);
-    starts[c] = s;
-    counts[c] = e - s;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, id);
+    if (act && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[id], (uint32_t)__popc(peers));
 }
 
 // One warp per query: lanes take the block's cells in the reference's order
@@ -104,29 +101,42 @@ __global__ void k_hg_table(const uint32_t* __restrict__ sorted_ids, uint32_t n, 
 // pass sums them, the fill pass gives each cell its place by a scan over the
 // lanes and copies the cell's particles, so a query's list is written by a
 // whole warp into one contiguous stretch.
-__device__ __forceinline__ bool hg_cell_of(const HGDev& G, const uint32_t c[3], uint32_t src, uint32_t t,
-                                           uint32_t& id) {
-    const uint32_t w = 2 * src + 1;
-    const uint32_t dz = t % w, dy = (t / w) % w, dx = t / (w * w);
+// (dx, dy, dz) of cell t of the block, packed 10 bits each, for the block's
+// cells in shared memory when there are at most HG_TAB of them
+constexpr int HG_TAB = 1024;
+__device__ __forceinline__ uint32_t hg_offsets(uint32_t t, uint32_t w) {
+    return (t % w) << 20 | ((t / w) % w) << 10 | (t / (w * w));
+}
+__device__ __forceinline__ void hg_fill_table(uint32_t* tab, uint32_t ncell, uint32_t w) {
+    if (ncell <= (uint32_t)HG_TAB)
+        for (uint32_t t = threadIdx.x; t < ncell; t += blockDim.x) tab[t] = hg_offsets(t, w);
+    __syncthreads();
+}
+__device__ __forceinline__ bool hg_cell_of(const HGDev& G, const uint32_t c[3], uint32_t src, uint32_t w,
+                                           uint32_t ncell, const uint32_t* tab, uint32_t t, uint32_t& id) {
+    const uint32_t o = ncell <= (uint32_t)HG_TAB ? tab[t] : hg_offsets(t, w);
+    const uint32_t dx = o & 1023u, dy = (o >> 10) & 1023u, dz = o >> 20;
     const uint32_t gx = c[0] + dx - src, gy = c[1] + dy - src, gz = c[2] + dz - src;  // wrap: below 0 fails
     if (gx >= G.res[0] || gy >= G.res[1] || gz >= G.res[2]) return false;
-    id = hg_morton(gx, gy, gz) % G.total;
+    id = hg_mod(hg_morton(gx, gy, gz), G);
     return true;
 }
 
 __global__ void k_hg_qcount(HGDev G, const float* __restrict__ q, int64_t nq, uint32_t src,
                             const uint32_t* __restrict__ counts, uint32_t* __restrict__ qcount) {
+    __shared__ uint32_t tab[HG_TAB];
+    const uint32_t w = 2 * src + 1, ncell = w * w * w;
+    hg_fill_table(tab, ncell, w);
     const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= nq) return;  // whole warps leave together
     uint32_t c[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[3 * i + a], G.dmin[a], G.cell);
-    const uint32_t ncell = (2 * src + 1) * (2 * src + 1) * (2 * src + 1);
     uint32_t k = 0;
     for (uint32_t t = lane; t < ncell; t += 32) {
         uint32_t id;
-        if (hg_cell_of(G, c, src, t, id)) k += counts[id];
+        if (hg_cell_of(G, c, src, w, ncell, tab, t, id)) k += counts[id];
     }
     k = __reduce_add_sync(0xFFFFFFFFu, k);
     if (lane == 0) qcount[i] = k;
@@ -136,18 +146,20 @@ __global__ void k_hg_qfill(HGDev G, const float* __restrict__ q, int64_t nq, uin
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ starts,
                            const uint32_t* __restrict__ sorted_index, const int64_t* __restrict__ offsets,
                            uint32_t* __restrict__ out) {
+    __shared__ uint32_t tab[HG_TAB];
+    const uint32_t w = 2 * src + 1, ncell = w * w * w;
+    hg_fill_table(tab, ncell, w);
     const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= nq) return;
     uint32_t c[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[3 * i + a], G.dmin[a], G.cell);
-    const uint32_t ncell = (2 * src + 1) * (2 * src + 1) * (2 * src + 1);
     int64_t o = offsets[i];
     for (uint32_t t0 = 0; t0 < ncell; t0 += 32) {
         const uint32_t t = t0 + lane;
         uint32_t id = 0, k = 0, s0 = 0;
-        if (t < ncell && hg_cell_of(G, c, src, t, id)) {
+        if (t < ncell && hg_cell_of(G, c, src, w, ncell, tab, t, id)) {
             k = counts[id];
             s0 = starts[id];
         }
@@ -212,14 +224,16 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_carry(int64_t* __restrict__ bsu
         __syncthreads();
     }
 }
+// OutT: int64 query offsets (with the total in out[n]) or uint32 cell starts
+template <class OutT, bool TOTAL>
 __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const uint32_t* __restrict__ in, int64_t n,
-                                                       const int64_t* __restrict__ bsum, int64_t* __restrict__ out) {
+                                                       const int64_t* __restrict__ bsum, OutT* __restrict__ out) {
     __shared__ int64_t sh[32];
     const int64_t i = (int64_t)blockIdx.x * SCAN_T + threadIdx.x;
     const int64_t v = i < n ? in[i] : 0;
     const int64_t r = block_incl_scan(v, sh);
-    if (i < n) out[i] = bsum[blockIdx.x] + r - v;
-    if (i == n - 1) out[n] = bsum[blockIdx.x] + r;
+    if (i < n) out[i] = (OutT)(bsum[blockIdx.x] + r - v);
+    if (TOTAL && i == n - 1) out[n] = (OutT)(bsum[blockIdx.x] + r);
 }
 
 __global__ void k_hg_stats(const uint32_t* __restrict__ counts, uint32_t total,
@@ -253,6 +267,7 @@ HGDev dev_of(const pgmpm_hashgrid_s* g) {
         d.res[a] = g->res[a];
     }
     d.total = g->total;
+    d.total_m = ~0ull / g->total + 1ull;  // wraps to 0 for total = 1, where every remainder is 0
     return d;
 }
 
@@ -342,20 +357,28 @@ int pgmpm_hashgrid_build(pgmpm_hashgrid g, const float* positions, int64_t n, in
     if (rc) return rc;
     const HGDev G = dev_of(g);
     uint32_t* ids = g->cell_ids.as<uint32_t>();
-    const uint32_t* sorted_ids = ids;
+    uint32_t* counts = g->counts.as<uint32_t>();
     const uint32_t* sorted_index = nullptr;
+    // per-cell counts (histogram of the cell ids), starts = their exclusive scan
+    CK(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * g->total, st));
     if (n > 0) {
-        k_hg_cells<<<blocks_of(n, HG_T), HG_T, 0, st>>>(G, pos, n, ids);
+        k_hg_cells<<<blocks_of(n, HG_T), HG_T, 0, st>>>(G, pos, n, ids, counts);
         CK(cudaGetLastError());
+    }
+    const int64_t nb = ((int64_t)g->total + SCAN_T - 1) / SCAN_T;
+    CK(g->scan_tmp.ensure(sizeof(int64_t) * nb));
+    int64_t* bsum = g->scan_tmp.as<int64_t>();
+    k_scan_sums<<<(int)nb, SCAN_T, 0, st>>>(counts, g->total, bsum);
+    k_scan_carry<<<1, SCAN_T, 0, st>>>(bsum, nb);
+    k_scan_apply<uint32_t, false><<<(int)nb, SCAN_T, 0, st>>>(counts, g->total, bsum, g->starts.as<uint32_t>());
+    CK(cudaGetLastError());
+    // particles ordered by cell, by index within a cell (stable sort)
+    if (n > 0) {
         int which = 0;
         CK(radix_sort_pairs(ids, nullptr, g->ka.as<uint32_t>(), g->va.as<uint32_t>(), g->kb.as<uint32_t>(),
                             g->vb.as<uint32_t>(), g->scratch.as<uint32_t>(), n, g->key_bits, &which, st));
-        sorted_ids = which ? g->kb.as<uint32_t>() : g->ka.as<uint32_t>();
         sorted_index = which ? g->vb.as<uint32_t>() : g->va.as<uint32_t>();
     }
-    k_hg_table<<<blocks_of(g->total, HG_T), HG_T, 0, st>>>(sorted_ids, (uint32_t)n, g->total,
-                                                            g->starts.as<uint32_t>(), g->counts.as<uint32_t>());
-    CK(cudaGetLastError());
     // keep the sorted indices where queries read them
     if (n > 0 && sorted_index != g->va.as<uint32_t>())
         CK(cudaMemcpyAsync(g->va.p, sorted_index, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
@@ -408,7 +431,7 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
                                                                g->qcount.as<uint32_t>());
         k_scan_sums<<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum);
         k_scan_carry<<<1, SCAN_T, 0, st>>>(bsum, nb);
-        k_scan_apply<<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum, doff);
+        k_scan_apply<int64_t, true><<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum, doff);
         CK(cudaGetLastError());
     } else {
         CK(cudaMemsetAsync(doff, 0, sizeof(int64_t), st));
