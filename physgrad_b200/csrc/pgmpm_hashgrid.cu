@@ -79,21 +79,19 @@ __device__ __forceinline__ uint32_t hg_coord(float x, float mn, float cell) {
     return (uint32_t)(unsigned long long)__float2ll_rz(__fdiv_rn(__fsub_rn(x, mn), cell));
 }
 
-// cell id per particle, and the per-cell counts (warp-aggregated atomics)
+// cell id per particle, and the per-cell counts (one atomic per particle:
+// input order is arbitrary, so a warp's particles rarely share a cell and
+// aggregating them over the warp cost more than it saved)
 __global__ void k_hg_cells(HGDev G, const float* __restrict__ pos, int64_t n, uint32_t* __restrict__ cell_ids,
                            uint32_t* __restrict__ counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = i < n;
-    uint32_t id = 0xFFFFFFFFu;
-    if (act) {
-        uint32_t c[3];
+    if (i >= n) return;
+    uint32_t c[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) c[a] = min(hg_coord(pos[3 * i + a], G.dmin[a], G.cell), G.res[a] - 1u);
-        id = hg_mod(hg_morton(c[0], c[1], c[2]), G);
-        cell_ids[i] = id;
-    }
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, id);
-    if (act && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[id], (uint32_t)__popc(peers));
+    for (int a = 0; a < 3; ++a) c[a] = min(hg_coord(pos[3 * i + a], G.dmin[a], G.cell), G.res[a] - 1u);
+    const uint32_t id = hg_mod(hg_morton(c[0], c[1], c[2]), G);
+    cell_ids[i] = id;
+    atomicAdd(&counts[id], 1u);
 }
 
 // One warp per query: lanes take the block's cells in the reference's order
