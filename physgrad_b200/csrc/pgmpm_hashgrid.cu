@@ -14,8 +14,9 @@
 //              (2 ceil(r / cell) + 1)^3 block around its cell, in the
 //              reference's order (x outer, z inner; a cell's particles by
 //              index), with no distance test -- as getNeighbors (:206-240),
-//              which computes radius^2 but does not use it.  Two passes (one
-//              warp per query): a count, a scan into offsets, then the fill.
+//              which computes radius^2 but does not use it.  Two passes: a
+//              count (thread per query), a scan into offsets, then the fill
+//              (8 lanes per query, so each list is written contiguously).
 //
 // Float arithmetic is IEEE single (no contraction), so cell ids match the
 // reference's host code bit for bit.
@@ -94,11 +95,11 @@ __global__ void k_hg_cells(HGDev G, const float* __restrict__ pos, int64_t n, ui
     atomicAdd(&counts[id], 1u);
 }
 
-// One warp per query: lanes take the block's cells in the reference's order
-// (linear index t = (dx (2s+1) + dy) (2s+1) + dz), 32 at a time; the count
-// pass sums them, the fill pass gives each cell its place by a scan over the
-// lanes and copies the cell's particles, so a query's list is written by a
-// whole warp into one contiguous stretch.
+// Fill pass, HG_FG lanes per query: they take the block's cells in the
+// reference's order (linear index t = (dx (2s+1) + dy) (2s+1) + dz), HG_FG at
+// a time, give each cell its place by a scan over the lanes and copy the
+// cell's particles, so a query's list is written into one contiguous stretch
+// by its lanes together.
 // (dx, dy, dz) of cell t of the block, packed 10 bits each, for the block's
 // cells in shared memory when there are at most HG_TAB of them
 constexpr int HG_TAB = 1024;
@@ -120,26 +121,33 @@ __device__ __forceinline__ bool hg_cell_of(const HGDev& G, const uint32_t c[3], 
     return true;
 }
 
+// Count pass, one thread per query: the block's cells in nested loops (the
+// reference's order does not matter for a sum)
 __global__ void k_hg_qcount(HGDev G, const float* __restrict__ q, int64_t nq, uint32_t src,
                             const uint32_t* __restrict__ counts, uint32_t* __restrict__ qcount) {
-    __shared__ uint32_t tab[HG_TAB];
-    const uint32_t w = 2 * src + 1, ncell = w * w * w;
-    hg_fill_table(tab, ncell, w);
-    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= nq) return;  // whole warps leave together
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
     uint32_t c[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[3 * i + a], G.dmin[a], G.cell);
     uint32_t k = 0;
-    for (uint32_t t = lane; t < ncell; t += 32) {
-        uint32_t id;
-        if (hg_cell_of(G, c, src, w, ncell, tab, t, id)) k += counts[id];
+    for (uint32_t dx = 0; dx <= 2 * src; ++dx) {
+        const uint32_t gx = c[0] + dx - src;  // uint32 wrap: below 0 fails the range test
+        if (gx >= G.res[0]) continue;
+        for (uint32_t dy = 0; dy <= 2 * src; ++dy) {
+            const uint32_t gy = c[1] + dy - src;
+            if (gy >= G.res[1]) continue;
+            for (uint32_t dz = 0; dz <= 2 * src; ++dz) {
+                const uint32_t gz = c[2] + dz - src;
+                if (gz >= G.res[2]) continue;
+                k += counts[hg_mod(hg_morton(gx, gy, gz), G)];
+            }
+        }
     }
-    k = __reduce_add_sync(0xFFFFFFFFu, k);
-    if (lane == 0) qcount[i] = k;
+    qcount[i] = k;
 }
 
+constexpr int HG_FG = 8;  // lanes per query in the fill (4 queries per warp; 4 lanes and 32 were slower)
 __global__ void k_hg_qfill(HGDev G, const float* __restrict__ q, int64_t nq, uint32_t src,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ starts,
                            const uint32_t* __restrict__ sorted_index, const int64_t* __restrict__ offsets,
@@ -147,29 +155,30 @@ __global__ void k_hg_qfill(HGDev G, const float* __restrict__ q, int64_t nq, uin
     __shared__ uint32_t tab[HG_TAB];
     const uint32_t w = 2 * src + 1, ncell = w * w * w;
     hg_fill_table(tab, ncell, w);
-    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= nq) return;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / HG_FG;
+    const int lane = threadIdx.x & 31, sub = lane % HG_FG;
+    const uint32_t gmask = ((1u << HG_FG) - 1u) << (lane - sub);  // this query's lanes
+    if (i >= nq) return;  // a query's lanes leave together
     uint32_t c[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) c[a] = hg_coord(q[3 * i + a], G.dmin[a], G.cell);
     int64_t o = offsets[i];
-    for (uint32_t t0 = 0; t0 < ncell; t0 += 32) {
-        const uint32_t t = t0 + lane;
+    for (uint32_t t0 = 0; t0 < ncell; t0 += HG_FG) {
+        const uint32_t t = t0 + sub;
         uint32_t id = 0, k = 0, s0 = 0;
         if (t < ncell && hg_cell_of(G, c, src, w, ncell, tab, t, id)) {
             k = counts[id];
             s0 = starts[id];
         }
-        uint32_t x = k;  // inclusive scan of the counts over the lanes
+        uint32_t x = k;  // inclusive scan of the counts over the query's lanes
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
-            if (lane >= d) x += y;
+        for (int d = 1; d < HG_FG; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(gmask, x, d, HG_FG);
+            if (sub >= d) x += y;
         }
         const int64_t base = o + (x - k);
         for (uint32_t j = 0; j < k; ++j) out[base + j] = sorted_index[s0 + j];
-        o += __shfl_sync(0xFFFFFFFFu, x, 31);
+        o += __shfl_sync(gmask, x, HG_FG - 1, HG_FG);
     }
 }
 
@@ -425,8 +434,8 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
     int64_t* bsum = g->scan_tmp.as<int64_t>();
     int64_t* doff = ptr_kind == PGMPM_PTR_HOST ? bsum + nb : offsets;
     if (nq > 0) {
-        k_hg_qcount<<<blocks_of(nq * 32, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
-                                                               g->qcount.as<uint32_t>());
+        k_hg_qcount<<<blocks_of(nq, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
+                                                          g->qcount.as<uint32_t>());
         k_scan_sums<<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum);
         k_scan_carry<<<1, SCAN_T, 0, st>>>(bsum, nb);
         k_scan_apply<int64_t, true><<<(int)nb, SCAN_T, 0, st>>>(g->qcount.as<uint32_t>(), nq, bsum, doff);
@@ -446,7 +455,7 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
             CK(out_stage.alloc(sizeof(uint32_t) * tot));
             dout = out_stage.as<uint32_t>();
         }
-        k_hg_qfill<<<blocks_of(nq * 32, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
+        k_hg_qfill<<<blocks_of(nq * HG_FG, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
                                                               g->starts.as<uint32_t>(), g->va.as<uint32_t>(), doff,
                                                               dout);
         CK(cudaGetLastError());
