@@ -84,3 +84,22 @@ def test_hashgrid_device_pointers_capacity_and_errors(gpu):
     assert lists.size == 0 and np.array_equal(o, np.zeros(5, np.int64))
     with pytest.raises(Exception, match="max_particles"):
         grid.buildHashTable(np.zeros((len(p) + 1, 3), np.float32))
+
+
+def test_hashgrid_wide_radius_matches_oracle(gpu):
+    """A radius of 5.5 cells visits 13^3 = 2197 cells per query, more than the
+    fill's shared offset table holds (the offsets are then computed per
+    cell): lists equal the restated reference's (oracle/hashgrid.py)."""
+    from oracle import hashgrid as H
+
+    rng = np.random.default_rng(11)
+    cs, mn, mx = 0.05, np.zeros(3, np.float32), np.ones(3, np.float32)
+    p = rng.random((4000, 3), dtype=np.float32)
+    q = rng.random((24, 3), dtype=np.float32)
+    r = 5.5 * cs
+    grid = gpu.SpatialHashGrid(cs, mn, mx, max_particles=len(p))
+    grid.buildHashTable(p)
+    c, s, ix, _ = H.build(p, cs, mn, mx)
+    o_ref, l_ref = H.neighbors(q, r, cs, mn, mx, c, s, ix)
+    off, lists = grid.neighbors(q, r)
+    assert np.array_equal(off, o_ref) and np.array_equal(lists, l_ref)
