@@ -43,7 +43,7 @@ struct pgmpm_hashgrid_s {
     DevBuf counts, starts;          // per cell
     DevBuf cell_ids;                // per particle: cell id (particle order)
     DevBuf ka, va, kb, vb, scratch, pos_stage;  // sort buffers; va keeps the sorted particle indices
-    DevBuf qcount, qstage, scan_tmp, stats;
+    DevBuf qcount, qstage, qout_stage, scan_tmp, stats;  // query scratch, kept between calls
 };
 
 namespace {
@@ -450,10 +450,9 @@ int pgmpm_hashgrid_neighbors(pgmpm_hashgrid g, const float* queries, int64_t nq,
     if (ptr_kind == PGMPM_PTR_HOST) CK(cudaMemcpyAsync(offsets, doff, off_bytes, cudaMemcpyDeviceToHost, st));
     if (indices && tot <= capacity && tot > 0) {
         uint32_t* dout = indices;
-        DevBuf out_stage;
         if (ptr_kind == PGMPM_PTR_HOST) {
-            CK(out_stage.alloc(sizeof(uint32_t) * tot));
-            dout = out_stage.as<uint32_t>();
+            CK(g->qout_stage.ensure(sizeof(uint32_t) * tot));
+            dout = g->qout_stage.as<uint32_t>();
         }
         k_hg_qfill<<<blocks_of(nq * HG_FG, HG_T), HG_T, 0, st>>>(G, q, nq, src, g->counts.as<uint32_t>(),
                                                               g->starts.as<uint32_t>(), g->va.as<uint32_t>(), doff,
