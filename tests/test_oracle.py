@@ -124,6 +124,84 @@ def test_oracle_adjoint_matches_central_differences(oracle, bc):
     assert np.abs(num - ana).max() <= 1e-4 * np.abs(num).max() + 1e-10
 
 
+@pytest.mark.parametrize("bc", [1, 2, 3])
+def test_oracle_adjoint_at_walls_on_ragged_grid(oracle, bc):
+    """FP64 oracle adjoint vs central FD on a 14 x 9 x 17 grid with an
+    origin and off-axis gravity, particles spread through the wall layers
+    (most stencils touch a wall node), each wall type."""
+    rng = np.random.default_rng(70 + bc)
+    n, dx, org, steps = (14, 9, 17), 1 / 16, (0.2, -0.1, 0.05), 3
+    N = 200
+    o_ = np.asarray(org)
+    st = dict(x=rng.uniform(o_ + dx, o_ + (np.asarray(n) - 2.0) * dx, (N, 3)), v=rng.normal(0, 0.3, (N, 3)),
+              C=rng.normal(0, 0.5, (N, 9)), F=np.tile(np.eye(3).ravel(), (N, 1)) + rng.normal(0, 0.05, (N, 9)),
+              m=np.full(N, 1000 * (dx / 2) ** 3), V0=np.full(N, (dx / 2) ** 3), mat=(np.arange(N) % 3).astype(np.int32))
+    s = np.floor((st["x"] - o_) / dx - 0.5).astype(int)
+    assert ((s < 3) | (s + 2 >= np.asarray(n) - 3)).any(1).sum() > N // 2
+    sc = oracle.make_scene(n, dx, 2e-3, gravity=(0.4, -9.8, 0.0), origin=org, physics=oracle.MLS, boundary=bc,
+                           bthick=3)
+    mlist = [(oracle.FIXED_COROTATED, 1e4, 0.3), (oracle.NEO_HOOKEAN, 3e4, 0.25), (oracle.EOS_FLUID, 1e4, 0.0)]
+    mats = oracle.make_materials(mlist)
+    tgt = np.array([0.5, 0.3, 0.5])
+
+    def loss(s_, mt=mats):
+        o = oracle.run(sc, mt, s_, steps, prec=64)
+        return ((o["x"].mean(0) - tgt) ** 2).sum() + 0.1 * (o["v"] ** 2).sum() + 0.01 * (o["F"] ** 2).sum()
+
+    o = oracle.run(sc, mats, st, steps, prec=64)
+    g = oracle.adjoint(sc, mats, st, steps, dict(x=np.tile(2 * (o["x"].mean(0) - tgt) / N, (N, 1)), v=0.2 * o["v"],
+                                                 F=0.02 * o["F"].reshape(N, 9)))
+    eps = 1e-6
+    num, ana = [], []
+    for key, cols in (("x", 3), ("v", 3), ("C", 9), ("F", 9)):
+        for _ in range(6):
+            i, j = rng.integers(N), rng.integers(cols)
+            sp = {k: (a.copy() if isinstance(a, np.ndarray) else a) for k, a in st.items()}
+            sm = {k: (a.copy() if isinstance(a, np.ndarray) else a) for k, a in st.items()}
+            sp[key] = sp[key].reshape(N, cols)
+            sm[key] = sm[key].reshape(N, cols)
+            sp[key][i, j] += eps
+            sm[key][i, j] -= eps
+            num.append((loss(sp) - loss(sm)) / (2 * eps))
+            ana.append(g[key].reshape(N, -1)[i, j])
+    for mi in range(3):
+        hi = [(a, b + (1e-2 if k == mi else 0), c) for k, (a, b, c) in enumerate(mlist)]
+        lo = [(a, b - (1e-2 if k == mi else 0), c) for k, (a, b, c) in enumerate(mlist)]
+        num.append((loss(st, oracle.make_materials(hi)) - loss(st, oracle.make_materials(lo))) / 2e-2)
+        ana.append(g["E"][mi])
+    num, ana = np.array(num), np.array(ana)
+    assert np.abs(num - ana).max() <= 1e-4 * np.abs(num).max() + 1e-10
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref",
+                                                    "libref_mpm.so")), reason="reference build absent")
+def test_ref_compat_matches_reference_on_ragged_grid(oracle):
+    """The REF_COMPAT pin on a grid that is not whole 4^3 tiles: 30 x 21 x 37
+    nodes, a non-zero origin and off-axis gravity, particles up to the
+    outermost nodes (30 steps, particles and both grid arrays)."""
+    rng = np.random.default_rng(11)
+    n, dx = (30, 21, 37), np.float32(1 / 32)
+    org = (np.float32(-0.25), np.float32(0.125), np.float32(0.3))
+    grav = (np.float32(0.5), np.float32(-9.8), np.float32(1.5))
+    N = 6000
+    x = rng.uniform(np.array(org, np.float32) + 2 * dx, np.array(org, np.float32) + (np.array(n) - 3) * dx,
+                    (N, 3)).astype(np.float32)
+    v = rng.normal(0, 0.5, (N, 3)).astype(np.float32)
+    vol = np.full(N, dx ** 3 / 8, np.float32)
+    m = (1000 * vol).astype(np.float32)
+    r = oracle.ref_run(x, v, m, vol, n, dx, np.float32(1e-3), grav, 30, origin=org, want_grid=True)
+    sc = oracle.make_scene(n, dx, np.float32(1e-3), gravity=grav, origin=org, physics=oracle.REF_COMPAT,
+                           boundary=oracle.BC_NONE)
+    st = dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)),
+              F=np.tile(np.eye(3).ravel(), (N, 1)), m=m.astype(np.float64), V0=vol.astype(np.float64))
+    o = oracle.run(sc, oracle.make_materials([(0, 1e4, 0.3)]), st, 30, prec=32, want_grid=True)
+    assert np.abs(r["x"] - x).max() > dx / 4  # the particles moved
+    assert np.array_equal(o["x"].astype(np.float32), r["x"])
+    assert np.array_equal(o["v"].astype(np.float32), r["v"])
+    assert np.array_equal(o["grid_m"].astype(np.float32), r["grid_m"])
+    assert np.array_equal(o["grid_v"].astype(np.float32), r["grid_v"])
+
+
 def test_oracle_fp32_mirror_close_to_fp64(oracle):
     rng = np.random.default_rng(5)
     N, dx = 1000, 1 / 32
