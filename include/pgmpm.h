@@ -26,6 +26,11 @@
  *   pgmpm_download / pgmpm_download_grid
  *       getParticles() / getGrid()        src/mpm_solver.h:322-324,
  *                                         src/material_point_method.h:503-504
+ *   pgmpm_set_scene_params
+ *       the per-call dt and gravity of
+ *       DifferentiableMPMSystem::simulationStep(dt, gravity)
+ *                                         src/differentiable_mpm.h:748
+ *       and of launch_mpm_timestep_forward src/pytorch_autograd.cu:371-382
  *   pgmpm_get_metrics
  *       MPMSolver<T>::getMetrics          src/mpm_solver.h:324 (struct :72-101)
  *   pgmpm_forward_checkpointed / pgmpm_backward
@@ -51,7 +56,7 @@
 extern "C" {
 #endif
 
-#define PGMPM_ABI_VERSION 2
+#define PGMPM_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define PGMPM_API __attribute__((visibility("default")))
@@ -160,6 +165,14 @@ PGMPM_API int pgmpm_destroy(pgmpm_solver s);
 /* Replace the material table (same count), e.g. a new Young's modulus
  * between optimisation iterations.  Host pointer. */
 PGMPM_API int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t n_materials);
+
+/* Change the time step and gravity of one scene between steps (gravity NULL
+ * keeps it).  The next step's P2G payload is recomputed with the new dt.  A
+ * recording of pgmpm_forward_checkpointed made before a change can no longer
+ * be differentiated (pgmpm_backward then fails with PGMPM_ERR_STATE); so
+ * does one made before pgmpm_set_materials.  Ordered after prior work on the
+ * legacy default stream; returns when the change is in place. */
+PGMPM_API int pgmpm_set_scene_params(pgmpm_solver s, int32_t scene, float dt, const float* gravity);
 
 /* Upload particle state, scenes back to back in scene order.
  * x,v [N][3]; C,F [N][9] row-major (NULL C = 0, NULL F = I); m,V0 [N];

@@ -127,6 +127,7 @@ SIGNATURES = {
                                     _i32, _i32, ctypes.POINTER(_vp)]),
     "pgmpm_destroy": (ctypes.c_int, [_vp]),
     "pgmpm_set_materials": (ctypes.c_int, [_vp, ctypes.POINTER(Material), _i32]),
+    "pgmpm_set_scene_params": (ctypes.c_int, [_vp, _i32, ctypes.c_float, _vp]),
     "pgmpm_upload": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "pgmpm_download": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "pgmpm_vtk_write_particles": (ctypes.c_int, [ctypes.c_char_p, _i64, _vp, _vp, _vp, _vp, ctypes.c_double]),

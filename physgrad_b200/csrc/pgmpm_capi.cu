@@ -407,8 +407,39 @@ int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t
     // ordered with prior work on the legacy stream; graphs read the table at run time
     CK(cudaMemcpy(s->d_mats.p, md.data(), sizeof(MatDev) * n_materials, cudaMemcpyHostToDevice));
     s->mats_h.assign(materials, materials + n_materials);
+    s->ck_valid = false;  // a replay would run with the new table
     if (s->uploaded) {
         // the payload holds the stress of the old material table
+        CK(cudaDeviceSynchronize());
+        int rc = refresh_payload(s, s->cap_stream);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(s->cap_stream));
+    }
+    return PGMPM_OK;
+}
+
+int pgmpm_set_scene_params(pgmpm_solver s, int32_t scene, float dt, const float* gravity) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (scene < 0 || scene >= s->S) return fail(PGMPM_ERR_ARG, "scene %d out of range [0, %d)", scene, s->S);
+    if (!(dt > 0.f) || !std::isfinite(dt)) return fail(PGMPM_ERR_ARG, "dt must be positive and finite");
+    if (gravity)
+        for (int a = 0; a < 3; ++a)
+            if (!std::isfinite(gravity[a])) return fail(PGMPM_ERR_ARG, "gravity must be finite");
+    SceneDev& sd = s->scenes[scene];
+    bool same = sd.dt == dt;
+    if (gravity)
+        for (int a = 0; a < 3; ++a) same = same && sd.gravity[a] == gravity[a];
+    if (same) return PGMPM_OK;
+    DeviceGuard dg(s->device);
+    sd.dt = dt;
+    s->desc[scene].dt = dt;
+    if (gravity)
+        for (int a = 0; a < 3; ++a) sd.gravity[a] = s->desc[scene].gravity[a] = gravity[a];
+    // kernels and captured graphs read the scene table from device memory
+    CK(cudaMemcpy(s->d_scenes.as<SceneDev>() + scene, &sd, sizeof(SceneDev), cudaMemcpyHostToDevice));
+    s->ck_valid = false;  // a replay would run with the new dt / gravity
+    if (s->uploaded && s->pf.physics == PHYS_MLS) {
+        // the payload holds -dt V0 D tau of the old dt
         CK(cudaDeviceSynchronize());
         int rc = refresh_payload(s, s->cap_stream);
         if (rc) return rc;

@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes
 import os
 import enum
+import dataclasses
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -259,6 +260,20 @@ class Simulator:
         md = (C.Material * len(materials))(*[m.to_c() for m in materials])
         check(lib().pgmpm_set_materials(self._h, md, len(materials)))
         self.materials = list(materials)
+
+    def set_scene_params(self, scene: int = 0, dt: float | None = None, gravity: Sequence[float] | None = None):
+        """New time step and/or gravity for one scene between steps (the
+        per-call dt, gravity of DifferentiableMPMSystem::simulationStep,
+        src/differentiable_mpm.h:748).  Invalidates a recording made by
+        forward_checkpointed before the change."""
+        s = self.scenes[scene] if 0 <= scene < len(self.scenes) else None  # the C-ABI rejects the index
+        new_dt = float(dt) if dt is not None else (float(s.dt) if s is not None else 0.0)
+        g = None
+        if gravity is not None:
+            g = (ctypes.c_float * 3)(*[float(a) for a in gravity])
+        check(lib().pgmpm_set_scene_params(self._h, int(scene), new_dt, g))
+        self.scenes[scene] = dataclasses.replace(s, dt=new_dt,
+                                                 gravity=tuple(s.gravity) if gravity is None else tuple(gravity))
 
     def set_tuning(self, p2g_block=0, ppt=0, g2p_block=0, use_graph=-1):
         check(lib().pgmpm_set_tuning(self._h, int(p2g_block), int(ppt), int(g2p_block), int(use_graph)))

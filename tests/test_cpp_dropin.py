@@ -44,3 +44,123 @@ def test_dropin_run_writes_vtk_frames(gpu, built_lib, read_vtk, tmp_path):
     assert 3 <= len(frames) <= 4 and frames[0] == "frame_00000.vtk", frames
     v = read_vtk(str(out / frames[-1]))
     assert v["x"].shape == (512, 3) and v["velocity"] is not None
+
+
+# ------------------------------------------- material_point_method.h / differentiable_mpm.h
+SRC_RD = os.path.join(ROOT, "tests", "cpp", "drop_in_ref_diff.cpp")
+
+
+def _build_rd(built_lib, out):
+    libdir = os.path.dirname(built_lib)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    SRC_RD, "-o", out, "-L", libdir, "-lpgmpm", f"-Wl,-rpath,{libdir}"], check=True)
+
+
+def _write(path, ints, floats):
+    import numpy as np
+
+    with open(path, "wb") as f:
+        np.asarray(ints, np.int32).tofile(f)
+        for a in floats:
+            np.asarray(a, np.float32).ravel().tofile(f)
+
+
+def test_ref_and_differentiable_dropin_headers_compile_and_link(built_lib, tmp_path):
+    """The drop-ins for src/material_point_method.h (MPMSolver<T,64>) and
+    src/differentiable_mpm.h (DifferentiableMPMSystem<T>) compile with
+    -Wall -Wextra -Werror and link against libpgmpm.so."""
+    _build_rd(built_lib, str(tmp_path / "rd"))
+
+
+@pytest.mark.gpu
+def test_ref_dropin_matches_reference_path(gpu, oracle, built_lib, tmp_path):
+    """MPMSolver<float, 64> of the drop-in header (two addParticles batches,
+    25 steps) on a 24 x 20 x 28 grid with an origin against the float oracle
+    of the reference's PIC step (bit-identical to the reference's own solver):
+    positions <= 2e-6, velocities <= 1e-4 * max|v|, grid mass <= 1e-5 * max m,
+    grid momentum <= 1e-4 * max |p| (GPU atomics sum in another order)."""
+    import numpy as np
+
+    exe = str(tmp_path / "rd")
+    _build_rd(built_lib, exe)
+    rng = np.random.default_rng(5)
+    n, dx, org, dt, g, steps = (24, 20, 28), np.float32(1 / 24), (0.1, -0.2, 0.05), 1e-3, (0.3, -9.8, 0.5), 25
+    N = 5000
+    o = np.asarray(org, np.float32)
+    x = rng.uniform(o + 0.2 * dx, o + (np.asarray(n) - 1.2) * dx, (N, 3)).astype(np.float32)
+    v = rng.normal(0, 0.5, (N, 3)).astype(np.float32)
+    vol = np.full(N, dx ** 3 / 8, np.float32)
+    m = (1000 * vol).astype(np.float32)
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    _write(fin, [N, *n, steps], [dx, o, np.float32(dt), np.asarray(g, np.float32), x, v, m, vol])
+    r = subprocess.run([exe, "ref", fin, fout], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert '"ref_steps": 25' in r.stdout
+    nodes = int(np.prod(n))
+    out = np.fromfile(fout, np.float32)
+    sizes = [3 * N, 3 * N, nodes, 3 * nodes, 3 * nodes]
+    assert out.size == sum(sizes)
+    ox, ov, gm, gv, gp = np.split(out, np.cumsum(sizes)[:-1])
+    sc = oracle.make_scene(n, dx, np.float32(dt), gravity=tuple(np.float32(a) for a in g),
+                           origin=tuple(np.float32(a) for a in org), physics=oracle.REF_COMPAT,
+                           boundary=oracle.BC_NONE)
+    st = dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)), F=np.tile(np.eye(3).ravel(), (N, 1)),
+              m=m.astype(np.float64), V0=vol.astype(np.float64))
+    ref = oracle.run(sc, oracle.make_materials([(0, 1e4, 0.3)]), st, steps, prec=32, want_grid=True)
+    assert np.abs(ox.reshape(N, 3) - ref["x"]).max() <= 2e-6
+    assert np.abs(ov.reshape(N, 3) - ref["v"]).max() <= 1e-4 * np.abs(ref["v"]).max()
+    assert np.abs(gm - ref["grid_m"]).max() <= 1e-5 * ref["grid_m"].max()
+    p_ref = ref["grid_m"][:, None] * ref["grid_v"]
+    assert np.abs(gp.reshape(nodes, 3) - p_ref).max() <= 1e-4 * np.abs(p_ref).max()
+    assert np.abs(gv.reshape(nodes, 3) * gm[:, None] - gp.reshape(nodes, 3)).max() <= 1e-6 * np.abs(p_ref).max()
+
+
+@pytest.mark.gpu
+def test_differentiable_dropin_matches_oracle_adjoint(gpu, oracle, built_lib, tmp_path):
+    """DifferentiableMPMSystem<float> of the drop-in header: 6 recorded steps
+    (checkpoints every 2) on an 20 x 16 x 24 grid with an origin and three
+    Young's moduli, then computeGradients() from seeded dL/dx, dL/dv of the
+    final state.  Final state vs the FP64 oracle (MLS bounds); dL/d(x0, v0, C0,
+    F0) and dL/dE per material vs the FP64 oracle adjoint, <= 2e-3 * max|oracle|
+    per field.  The program also checks the reference's error paths."""
+    import numpy as np
+
+    exe = str(tmp_path / "rd")
+    _build_rd(built_lib, exe)
+    rng = np.random.default_rng(9)
+    n, dx, org, dt, g, steps, k = (20, 16, 24), 1 / 16, (0.2, -0.1, 0.05), 1e-3, (0.4, -9.8, 0.0), 6, 2
+    N = 1500
+    Es = np.array([8e3, 1.2e4, 2e4], np.float32)
+    o = np.asarray(org)
+    x = rng.uniform(o + 3.5 * dx, o + (np.asarray(n) - 4.5) * dx, (N, 3)).astype(np.float32)
+    v = rng.normal(0, 0.3, (N, 3)).astype(np.float32)
+    E = Es[np.arange(N) % 3]
+    sx = (rng.normal(0, 1, (N, 3)) / N).astype(np.float32)
+    sv = (rng.normal(0, 1, (N, 3)) / N).astype(np.float32)
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    _write(fin, [N, *n, steps, k, 1, 3], [np.float32(dx), o, np.float32(dt), np.asarray(g, np.float32), x, v, E, sx, sv])
+    r = subprocess.run([exe, "diff", fin, fout], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert '"diff_steps": 6, "materials": 3' in r.stdout
+    out = np.fromfile(fout, np.float32)
+    sizes = [3 * N, 3 * N, 3 * N, 3 * N, 9 * N, 9 * N]
+    parts = np.split(out[:sum(sizes)], np.cumsum(sizes)[:-1])
+    ox, ov, gx, gv, gC, gF = [p.reshape(N, -1) for p in parts]
+    tab = out[sum(sizes):]
+    assert int(tab[0]) == 3 and np.array_equal(tab[1::2], Es)
+    gE = tab[2::2]
+    V0 = np.full(N, (dx / 2) ** 3)
+    st = dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)), F=np.tile(np.eye(3).ravel(), (N, 1)),
+              m=np.float32(1000) * V0.astype(np.float32), V0=V0, mat=(np.arange(N) % 3).astype(np.int32))
+    st["m"] = st["m"].astype(np.float64)
+    sc = oracle.make_scene(n, dx, dt, gravity=g, origin=org, physics=oracle.MLS, boundary=oracle.BC_STICKY, bthick=3)
+    mats = oracle.make_materials([(oracle.FIXED_COROTATED, float(e), 0.3) for e in Es])
+    fwd = oracle.run(sc, mats, st, steps, prec=64)
+    assert np.abs(ox - fwd["x"]).max() <= 2e-5
+    assert np.abs(ov - fwd["v"]).max() <= 1e-3 * np.abs(fwd["v"]).max() + 1e-5
+    ref = oracle.adjoint(sc, mats, st, steps, {"x": sx.astype(np.float64), "v": sv.astype(np.float64)})
+    for key, a in (("x", gx), ("v", gv), ("C", gC), ("F", gF), ("E", gE)):
+        b = np.asarray(ref[key]).reshape(a.shape)
+        err = np.abs(a - b).max() / np.abs(b).max()
+        print(f"drop-in d/d{key}: rel err {err:.2e}")
+        assert err <= 2e-3, (key, err)

@@ -246,6 +246,38 @@ def test_checkpointed_forward_leaves_the_stepped_state(gpu):
     assert np.abs(gv0 - gv1).max() <= 1e-3 * (np.abs(gv0).max() + 1e-6)
 
 
+def test_recording_invalidated_by_scene_or_material_change(gpu):
+    """pgmpm_backward differentiates the recording of the last
+    pgmpm_forward_checkpointed; after pgmpm_set_scene_params or
+    pgmpm_set_materials its replay would run other physics, so it fails with
+    PGMPM_ERR_STATE until the forward is run again."""
+    from physgrad_b200 import _capi as C
+
+    rng = np.random.default_rng(61)
+    N, n = 400, 16
+    st = _case(rng, N, n)
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3), gpu.createElasticMaterial(1000, 3e4, 0.25, 1),
+            gpu.createFluidMaterial(1000, 0.0, 1e4)]
+    sim = gpu.Simulator([gpu.Scene((n, n, n), 1.0 / n, 1e-3, (0, -9.8, 0), (0, 0, 0), 0, 1, 3)], [N], mats)
+    sim.upload(st["x"], st["v"], st["C"], st["F"], st["m"], st["V0"], st["mat"])
+    go = {"x": np.full((N, 3), 1.0 / N, np.float32)}
+    sim.forward_checkpointed(4, 2)
+    g0 = sim.backward(go)
+    sim.set_scene_params(0, dt=5e-4)
+    with pytest.raises(C.PGMPMError) as ei:
+        sim.backward(go)
+    assert ei.value.code == C.PGMPM_ERR_STATE
+    sim.set_scene_params(0, dt=1e-3)
+    sim.upload(st["x"], st["v"], st["C"], st["F"], st["m"], st["V0"], st["mat"])
+    sim.forward_checkpointed(4, 2)
+    g1 = sim.backward(go)
+    assert np.abs(g1["v"] - g0["v"]).max() <= 1e-5 * np.abs(g0["v"]).max()
+    sim.set_materials(mats)
+    with pytest.raises(C.PGMPMError) as ei:
+        sim.backward(go)
+    assert ei.value.code == C.PGMPM_ERR_STATE
+
+
 def test_tape_steps_report_error_flags(gpu):
     """A particle leaving the grid inside the segment the forward runs in the
     tape still raises PGMPM_FLAG_ESCAPE on the solver."""

@@ -511,6 +511,41 @@ def test_escape_and_nonfinite_flags(gpu):
     assert nan.status() & C.FLAG_NONFINITE
 
 
+@pytest.mark.parametrize("physics", [0, 1])
+def test_scene_params_change_between_steps(gpu, oracle, physics):
+    """pgmpm_set_scene_params: 6 steps at one dt and gravity, then 6 at
+    another, against the oracle run the same way.  MLS rebuilds the next
+    step's P2G payload (it holds -dt V0 D tau) with the new dt."""
+    from physgrad_b200 import _capi as C
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=8000, n=32, v_sigma=0.5, seed=14, physics=physics,
+                                                 boundary=C.BC_STICKY if physics == 0 else C.BC_NONE)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(6)
+    with pytest.raises(C.PGMPMError):
+        sim.set_scene_params(0, dt=-1.0)
+    with pytest.raises(C.PGMPMError):
+        sim.set_scene_params(1, dt=1e-4)
+    sim.set_scene_params(0, dt=2.5e-4, gravity=(1.5, -4.0, 0.5))
+    sim.step(6)
+    out = sim.download()
+    omats = oracle.make_materials([(0, 1e4, 0.3)])
+    prec = 64 if physics == 0 else 32
+    mid = oracle.run(_oracle_scene(oracle, scenes[0]), omats, _oracle_state(st), 6, prec=prec)
+    s2 = oracle.make_scene(tuple(scenes[0].n), np.float32(scenes[0].dx), np.float32(2.5e-4),
+                           gravity=(np.float32(1.5), np.float32(-4.0), np.float32(0.5)), physics=physics,
+                           boundary=scenes[0].boundary, bthick=scenes[0].boundary_thickness)
+    st2 = dict(_oracle_state(st), x=mid["x"], v=mid["v"], C=mid["C"].reshape(-1, 9), F=mid["F"].reshape(-1, 9))
+    ref = oracle.run(s2, omats, st2, 6, prec=prec)
+    if physics == 0:
+        _assert_mls(out, ref, "scene params")
+    else:
+        assert np.abs(out["x"] - ref["x"]).max() <= 1e-6
+        assert np.abs(out["v"] - ref["v"]).max() <= 1e-4 * np.abs(ref["v"]).max()
+    assert abs(sim.scenes[0].dt - 2.5e-4) < 1e-12 and tuple(sim.scenes[0].gravity) == (1.5, -4.0, 0.5)
+
+
 def test_invalid_material_rejected(gpu):
     from physgrad_b200 import _capi as C
 
