@@ -40,8 +40,8 @@
  *   pgmpm_set_tuning / pgmpm_autotune
  *       MPMSolverConfig::cuda_block_size  src/mpm_solver.h:51 and
  *       kernels::KernelConfig             src/mpm_g2p2g_kernels.h:68-75
- *   launch_mpm_timestep_forward
- *       same name and arguments as        src/pytorch_autograd.cu:371-382
+ *   launch_mpm_timestep_forward / launch_mpm_timestep_backward
+ *       same names and arguments as       src/pytorch_autograd.cu:371-402
  *   pgmpm_radix_sort_pairs
  *       no reference counterpart (the reference does not sort); exported so
  *       the integer sort can be checked bit for bit on its own.
@@ -153,6 +153,9 @@ typedef struct {
 
 /* ---- lifecycle ---------------------------------------------------------- */
 PGMPM_API const char* pgmpm_last_error(void);
+/* Empties the calling thread's last error message, so that a caller of the
+ * void launch_* entry points can tell whether one of them failed. */
+PGMPM_API void pgmpm_clear_error(void);
 PGMPM_API int pgmpm_abi_version(void);
 
 /* Create a solver over n_scenes scenes (n_scenes = 1 for a plain solver).
@@ -344,6 +347,20 @@ PGMPM_API int pgmpm_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint
  * cudaStream_t.  Errors are reported through pgmpm_last_error(). */
 PGMPM_API void launch_mpm_timestep_forward(float* positions, float* velocities, const float* masses, int num_particles,
                                  int grid_resolution, float dt, const float* gravity, void* stream);
+
+/* Reference-shaped launcher (src/pytorch_autograd.cu:384-402): the reverse of
+ * the step launch_mpm_timestep_forward ran from saved_positions,
+ * saved_velocities (that step's inputs).  grad_positions, grad_velocities:
+ * dL/d of the step's outputs; writes dL/d of its inputs to
+ * grad_input_positions, grad_input_velocities [n][3] and grad_masses [n]
+ * (may be NULL), and adds dL/dgravity to grad_gravity [3] (may be NULL), as
+ * the reference's kernel does.  Masses and gravity are those of the last
+ * forward call with the same device, particle count and resolution (an
+ * error if there was none).  Device pointers; asynchronous on stream. */
+PGMPM_API void launch_mpm_timestep_backward(const float* grad_positions, const float* grad_velocities,
+                                  float* grad_input_positions, float* grad_input_velocities, float* grad_masses,
+                                  float* grad_gravity, const float* saved_positions, const float* saved_velocities,
+                                  int num_particles, int grid_resolution, float dt, void* stream);
 
 #ifdef __cplusplus
 }

@@ -123,6 +123,7 @@ _i64 = ctypes.c_int64
 SIGNATURES = {
     "pgmpm_last_error": (ctypes.c_char_p, []),
     "pgmpm_abi_version": (ctypes.c_int, []),
+    "pgmpm_clear_error": (None, []),
     "pgmpm_create": (ctypes.c_int, [ctypes.POINTER(SceneDesc), _i32, ctypes.POINTER(_i64), ctypes.POINTER(Material),
                                     _i32, _i32, ctypes.POINTER(_vp)]),
     "pgmpm_destroy": (ctypes.c_int, [_vp]),
@@ -155,6 +156,8 @@ SIGNATURES = {
     "pgmpm_radix_sort_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp]),
     "pgmpm_radix_sort_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp]),
     "launch_mpm_timestep_forward": (None, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp]),
+    "launch_mpm_timestep_backward": (None, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_float, _vp]),
 }
 
 _lib = None

@@ -1,18 +1,26 @@
-"""torch.autograd.Function over the checkpointed MLS-MPM forward/backward.
+"""torch.autograd.Functions over the MPM step.
 
-Replaces the reference's PhysicsSimulationFunction pattern
-(src/pytorch_autograd.h:146-226: save inputs, run forward, backward by the
-adjoint) for the MPM path, whose reference adjoint records an empty backward
-(src/differentiable_mpm.h:871-876).  Device tensors cross the C-ABI by
-pointer (no copies); work runs on torch's current stream.
+* MPMSimulate: the checkpointed MLS-MPM forward / backward over many steps.
+  It replaces the reference's PhysicsSimulationFunction pattern
+  (src/pytorch_autograd.h:146-226: save inputs, run forward, backward by the
+  adjoint) for the MPM path, whose reference adjoint records an empty backward
+  (src/differentiable_mpm.h:871-876).
+* MPMTimestep: one step of the reference's PIC step through the extern-C
+  launchers launch_mpm_timestep_forward / _backward
+  (src/pytorch_autograd.cu:371-402).
+
+Device tensors cross the C-ABI by pointer (no copies); work runs on torch's
+current stream.
 """
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 from typing import Optional
 
 import torch
 
+from ._capi import PGMPMError, lib
 from .solver import Simulator
 
 
@@ -64,3 +72,54 @@ def simulate(sim: Simulator, x0, v0, E, m, V0, n_steps: int, checkpoint_every: i
     if F0 is None:
         F0 = torch.eye(3, device=x0.device).expand(N, 3, 3).contiguous()
     return MPMSimulate.apply(sim, n_steps, checkpoint_every, x0, v0, C0, F0, E, m, V0, mat)
+
+
+def _launch(name: str, *args):
+    """Calls a void launch_* entry point; raises if it reported an error."""
+    L = lib()
+    L.pgmpm_clear_error()
+    getattr(L, name)(*args)
+    msg = L.pgmpm_last_error()
+    if msg:
+        raise PGMPMError(-1, msg.decode())
+
+
+class MPMTimestep(torch.autograd.Function):
+    """One step of the reference's PIC MPM step (REF_COMPAT physics) on the
+    unit cube with a grid_resolution^3 grid, through the extern-C launchers
+    launch_mpm_timestep_forward / launch_mpm_timestep_backward
+    (src/pytorch_autograd.cu:371-402): (positions [N,3], velocities [N,3],
+    masses [N], gravity [3]) -> (positions, velocities); gradients flow to
+    all four.  Chains into rollouts like any torch op."""
+
+    @staticmethod
+    def forward(ctx, positions, velocities, masses, gravity, grid_resolution: int, dt: float):
+        if not positions.is_cuda:
+            raise ValueError("MPMTimestep expects CUDA tensors")
+        f32 = lambda t: t.detach().to(torch.float32).contiguous()
+        x0, v0, m, g = f32(positions), f32(velocities), f32(masses), f32(gravity)
+        x, v = x0.clone(), v0.clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _launch("launch_mpm_timestep_forward", x.data_ptr(), v.data_ptr(), m.data_ptr(), x.shape[0],
+                int(grid_resolution), float(dt), g.data_ptr(), stream)
+        ctx.save_for_backward(x0, v0, m, g)
+        ctx.res, ctx.dt = int(grid_resolution), float(dt)
+        return x, v
+
+    @staticmethod
+    def backward(ctx, gx, gv):
+        x0, v0, m, g = ctx.saved_tensors
+        N = x0.shape[0]
+        z = lambda t: torch.zeros_like(x0) if t is None else t.detach().to(torch.float32).contiguous()
+        gx, gv = z(gx), z(gv)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        # the backward launcher uses the masses and gravity of the last forward
+        # call with this particle count and resolution: make that this step's
+        xs, vs = x0.clone(), v0.clone()
+        _launch("launch_mpm_timestep_forward", xs.data_ptr(), vs.data_ptr(), m.data_ptr(), N, ctx.res, ctx.dt,
+                g.data_ptr(), stream)
+        gix, giv = torch.empty_like(x0), torch.empty_like(v0)
+        gim, gg = torch.empty_like(m), torch.zeros_like(g)
+        _launch("launch_mpm_timestep_backward", gx.data_ptr(), gv.data_ptr(), gix.data_ptr(), giv.data_ptr(),
+                gim.data_ptr(), gg.data_ptr(), x0.data_ptr(), v0.data_ptr(), N, ctx.res, ctx.dt, stream)
+        return gix, giv, gim, gg, None, None

@@ -223,6 +223,7 @@ int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
 extern "C" {
 
 const char* pgmpm_last_error(void) { return g_err.c_str(); }
+void pgmpm_clear_error(void) { g_err.clear(); }
 int pgmpm_abi_version(void) { return PGMPM_ABI_VERSION; }
 
 int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,

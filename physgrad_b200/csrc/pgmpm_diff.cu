@@ -386,8 +386,26 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
 // solver per (device, particle count, resolution) is kept for the process so
 // repeated calls reuse their device buffers.
 namespace {
+struct LaunchEntry {
+    pgmpm_solver s = nullptr;
+    pgmpm::DevBuf masses;  // the last forward's masses: the backward's signature carries none
+};
 std::mutex g_launch_mu;
-std::map<std::tuple<int, int, int>, pgmpm_solver> g_launch_solvers;
+std::map<std::tuple<int, int, int>, LaunchEntry> g_launch_solvers;
+
+// per-call dt into the scene table (the dt word only: gravity arrives as a
+// device pointer and is copied there by the forward)
+bool launch_set_dt(pgmpm_solver s, float dt, cudaStream_t st, const char* who) {
+    if (s->scenes[0].dt == dt) return true;
+    s->scenes[0].dt = dt;
+    if (cudaMemcpyAsync(&s->d_scenes.as<SceneDev>()[0].dt, &s->scenes[0].dt, sizeof(float), cudaMemcpyHostToDevice,
+                        st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        fail(PGMPM_ERR_CUDA, "%s: dt update failed", who);
+        return false;
+    }
+    return true;
+}
 }  // namespace
 
 extern "C" void launch_mpm_timestep_forward(float* positions, float* velocities, const float* masses,
@@ -402,6 +420,7 @@ extern "C" void launch_mpm_timestep_forward(float* positions, float* velocities,
     cudaGetDevice(&dev);
     cudaStream_t st = ST(stream);
     pgmpm_solver s = nullptr;
+    LaunchEntry* entry = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_launch_mu);
         auto key = std::make_tuple(dev, num_particles, grid_resolution);
@@ -416,21 +435,15 @@ extern "C" void launch_mpm_timestep_forward(float* positions, float* velocities,
             const int64_t cnt = num_particles;
             pgmpm_material mat{PGMPM_MAT_ELASTIC, PGMPM_MODEL_FIXED_COROTATED, 1e6f, 0.3f, 1000.f};
             if (pgmpm_create(&d, 1, &cnt, &mat, 1, dev, &s) != PGMPM_OK) return;
-            g_launch_solvers[key] = s;
+            entry = &g_launch_solvers[key];
+            entry->s = s;
         } else {
-            s = it->second;
+            entry = &it->second;
+            s = entry->s;
         }
     }
     // per-call dt and gravity (device pointer) into the scene table
-    if (s->scenes[0].dt != dt) {
-        s->scenes[0].dt = dt;
-        if (cudaMemcpyAsync(&s->d_scenes.as<SceneDev>()[0].dt, &s->scenes[0].dt, sizeof(float),
-                            cudaMemcpyHostToDevice, st) != cudaSuccess) {
-            fail(PGMPM_ERR_CUDA, "launch_mpm_timestep_forward: dt update failed");
-            return;
-        }
-        cudaStreamSynchronize(st);
-    }
+    if (!launch_set_dt(s, dt, st, "launch_mpm_timestep_forward")) return;
     if (gravity) {
         if (cudaMemcpyAsync(&s->d_scenes.as<SceneDev>()[0].gravity[0], gravity, 3 * sizeof(float),
                             cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
@@ -442,5 +455,63 @@ extern "C" void launch_mpm_timestep_forward(float* positions, float* velocities,
     if (pgmpm_upload(s, positions, velocities, nullptr, nullptr, masses, nullptr, nullptr, PGMPM_PTR_DEVICE, stream))
         return;
     if (pgmpm_step(s, 1, stream)) return;
-    pgmpm_download(s, positions, velocities, nullptr, nullptr, PGMPM_PTR_DEVICE, stream);
+    if (pgmpm_download(s, positions, velocities, nullptr, nullptr, PGMPM_PTR_DEVICE, stream)) return;
+    // kept for launch_mpm_timestep_backward
+    if (entry->masses.ensure(sizeof(float) * (size_t)num_particles) != cudaSuccess ||
+        cudaMemcpyAsync(entry->masses.p, masses, sizeof(float) * (size_t)num_particles, cudaMemcpyDeviceToDevice,
+                        st) != cudaSuccess)
+        fail(PGMPM_ERR_CUDA, "launch_mpm_timestep_forward: keeping the masses failed");
+}
+
+// launch_mpm_timestep_backward: src/pytorch_autograd.cu:384-402 shape.  The
+// reverse of the step launch_mpm_timestep_forward runs, from that step's
+// inputs (saved_positions, saved_velocities); masses and gravity are those of
+// the last forward call with the same device, particle count and resolution.
+// The forward step is recomputed (its grid is the linearisation point), then
+// the three reverse kernels of pgmpm_ref_adjoint.cu run.  grad_gravity is
+// added to, as the reference's kernel does (zero it first); grad_masses may
+// be NULL.
+extern "C" void launch_mpm_timestep_backward(const float* grad_positions, const float* grad_velocities,
+                                             float* grad_input_positions, float* grad_input_velocities,
+                                             float* grad_masses, float* grad_gravity, const float* saved_positions,
+                                             const float* saved_velocities, int num_particles, int grid_resolution,
+                                             float dt, void* stream) {
+    if (num_particles < 0 || grid_resolution < 4 || !(dt > 0.f) ||
+        (num_particles > 0 && (!grad_positions || !grad_velocities || !grad_input_positions ||
+                               !grad_input_velocities || !saved_positions || !saved_velocities))) {
+        fail(PGMPM_ERR_ARG, "launch_mpm_timestep_backward: invalid arguments");
+        return;
+    }
+    if (num_particles == 0) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaStream_t st = ST(stream);
+    pgmpm_solver s = nullptr;
+    const float* masses = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_launch_mu);
+        auto it = g_launch_solvers.find(std::make_tuple(dev, num_particles, grid_resolution));
+        if (it == g_launch_solvers.end() || !it->second.masses.p) {
+            fail(PGMPM_ERR_STATE,
+                 "launch_mpm_timestep_backward: no launch_mpm_timestep_forward call with this device, particle "
+                 "count and resolution");
+            return;
+        }
+        s = it->second.s;
+        masses = it->second.masses.as<float>();
+    }
+    if (!launch_set_dt(s, dt, st, "launch_mpm_timestep_backward")) return;
+    if (pgmpm_upload(s, saved_positions, saved_velocities, nullptr, nullptr, masses, nullptr, nullptr,
+                     PGMPM_PTR_DEVICE, stream))
+        return;
+    if (pgmpm_step(s, 1, stream)) return;
+    const size_t gbytes = sizeof(float4) * nodes_of(s);
+    if (s->adj_grid_gv.ensure(gbytes) != cudaSuccess || cudaMemsetAsync(s->adj_grid_gv.p, 0, gbytes, st) != cudaSuccess) {
+        fail(PGMPM_ERR_CUDA, "launch_mpm_timestep_backward: grid adjoint buffer");
+        return;
+    }
+    if (launch_ref_adjoint(s->view(), saved_positions, saved_velocities, masses, grad_positions, grad_velocities,
+                           s->adj_grid_gv.as<float4>(), grad_input_positions, grad_input_velocities, grad_masses,
+                           grad_gravity, s->num_sms, st) != cudaSuccess)
+        fail(PGMPM_ERR_CUDA, "launch_mpm_timestep_backward: %s", cudaGetErrorString(cudaGetLastError()));
 }

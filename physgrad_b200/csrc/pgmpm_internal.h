@@ -158,6 +158,11 @@ cudaError_t launch_adj_gather(const View& V, const AdjView& A, const PhysFlags& 
                               cudaStream_t st);
 cudaError_t launch_state_to_planes(const float* x, const float* v, const float* C, const float* F,
                                    const uint32_t* user_of_phys, float4* g, int64_t N, cudaStream_t st);
+// reverse of one REF_COMPAT step (pgmpm_ref_adjoint.cu); particle arrays in
+// the caller's order, G: one float4 per grid node, zeroed by the caller
+cudaError_t launch_ref_adjoint(const View& V, const float* x, const float* v, const float* m, const float* gx,
+                               const float* gv, float4* G, float* gx_in, float* gv_in, float* gm_in, float* ggrav,
+                               int num_sms, cudaStream_t st);
 cudaError_t launch_planes_to_state(const float4* g, const uint32_t* phys_of_user, float* x, float* v, float* C,
                                    float* F, int64_t N, cudaStream_t st);
 

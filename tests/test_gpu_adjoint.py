@@ -291,3 +291,123 @@ def test_tape_steps_report_error_flags(gpu):
     sim.upload(x, v, None, None, np.full(2, 1e-3, np.float32), np.full(2, 1e-6, np.float32))
     sim.forward_checkpointed(30, 30)  # one segment: every step runs in the tape
     assert sim.status() & C.FLAG_ESCAPE
+
+
+# ------------------------------------------- launch_mpm_timestep_backward
+def _ref_step_case(rng, N, res):
+    """Particles whose fractional cell coordinate is in [0.1, 0.9]: the
+    reference's floor-based 3-node stencil jumps where a coordinate crosses a
+    cell boundary, so central differences need room on both sides."""
+    cells = rng.integers(6, res - 6, (N, 3))
+    x = ((cells + rng.uniform(0.1, 0.9, (N, 3))) / res).astype(np.float32)
+    v = rng.normal(0, 0.5, (N, 3)).astype(np.float32)
+    m = (rng.uniform(0.5, 1.5, N) * 1e-3).astype(np.float32)
+    return x, v, m
+
+
+def _ref_loss(oracle, x, v, m, g, res, dt, steps, sx, sv):
+    """sum(sx . x') + sum(sv . v') after `steps` REF steps, FP64 oracle."""
+    N = x.shape[0]
+    sc = oracle.make_scene((res, res, res), 1.0 / res, dt, gravity=tuple(g), physics=oracle.REF_COMPAT,
+                           boundary=oracle.BC_NONE)
+    st = dict(x=x, v=v, C=np.zeros((N, 9)), F=np.tile(np.eye(3).ravel(), (N, 1)), m=m, V0=np.full(N, 1e-6))
+    o = oracle.run(sc, oracle.make_materials([(0, 1e4, 0.3)]), st, steps, prec=64)
+    return float((sx * o["x"]).sum() + (sv * o["v"]).sum())
+
+
+def _fd_check(oracle, rng, x, v, m, g, res, dt, steps, sx, sv, grads, n_samples=6):
+    """Central differences (FP64, eps 1e-6) of _ref_loss at sampled entries
+    of x, v, m and every entry of g against the given gradients; per input,
+    max error <= 1e-3 * max |difference quotient|."""
+    base = dict(x=x.astype(np.float64), v=v.astype(np.float64), m=m.astype(np.float64), g=g.astype(np.float64))
+    eps = 1e-6
+    for key in ("x", "v", "m", "g"):
+        arr = base[key]
+        idx = [tuple(rng.integers(0, s) for s in arr.shape) for _ in range(n_samples)] if key != "g" else \
+            [(0,), (1,), (2,)]
+        num, ana = [], []
+        for i in idx:
+            hi = {k: a.copy() for k, a in base.items()}
+            lo = {k: a.copy() for k, a in base.items()}
+            hi[key][i] += eps
+            lo[key][i] -= eps
+            f = lambda d: _ref_loss(oracle, d["x"], d["v"], d["m"], d["g"], res, dt, steps, sx, sv)
+            num.append((f(hi) - f(lo)) / (2 * eps))
+            ana.append(float(grads[key][i]))
+        num, ana = np.array(num), np.array(ana)
+        print(f"d/d{key}: max |fd - adjoint| {np.abs(num - ana).max():.2e} of max |fd| {np.abs(num).max():.2e}")
+        assert np.abs(num - ana).max() <= 1e-3 * np.abs(num).max() + 1e-12, (key, num, ana)
+
+
+def test_launch_mpm_timestep_backward_vs_central_differences(gpu, oracle):
+    """launch_mpm_timestep_backward (src/pytorch_autograd.cu:384-402 shape):
+    the reverse of the REF_COMPAT step launch_mpm_timestep_forward runs,
+    against central differences of the FP64 oracle's REF step for positions,
+    velocities, masses and gravity.  Also: the forward output matches the
+    float oracle, and a backward without a matching forward is an error."""
+    import torch
+    from physgrad_b200 import _capi as C
+
+    L = C.lib()
+    rng = np.random.default_rng(71)
+    N, res, dt = 3000, 32, 2e-3
+    x, v, m = _ref_step_case(rng, N, res)
+    g = np.array([0.3, -9.8, 0.5], np.float32)
+    sx = rng.normal(0, 1, (N, 3))
+    sv = rng.normal(0, 1, (N, 3))
+    dev = torch.device("cuda:0")
+    t = lambda a: torch.tensor(a, dtype=torch.float32, device=dev)
+    tx, tv, tm, tg = t(x), t(v), t(m), t(g)
+    L.pgmpm_clear_error()
+    L.launch_mpm_timestep_forward(tx.data_ptr(), tv.data_ptr(), tm.data_ptr(), N, res, dt, tg.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert L.pgmpm_last_error() == b""
+    sc = oracle.make_scene((res, res, res), np.float32(1.0 / res), np.float32(dt), gravity=tuple(g),
+                           physics=oracle.REF_COMPAT, boundary=oracle.BC_NONE)
+    st = dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)),
+              F=np.tile(np.eye(3).ravel(), (N, 1)), m=m.astype(np.float64), V0=np.full(N, 1e-6))
+    fwd = oracle.run(sc, oracle.make_materials([(0, 1e4, 0.3)]), st, 1, prec=32)
+    assert np.abs(tx.cpu().numpy() - fwd["x"]).max() <= 1e-6
+    assert np.abs(tv.cpu().numpy() - fwd["v"]).max() <= 1e-4 * np.abs(fwd["v"]).max()
+    gix, giv, gim, gg = torch.empty_like(tx), torch.empty_like(tv), torch.empty_like(tm), torch.zeros_like(tg)
+    # every tensor whose pointer crosses the C-ABI stays referenced until the
+    # kernels are done (a temporary's block would be handed to the next one)
+    tsx, tsv, tx0, tv0 = t(sx), t(sv), t(x), t(v)
+    L.launch_mpm_timestep_backward(tsx.data_ptr(), tsv.data_ptr(), gix.data_ptr(), giv.data_ptr(), gim.data_ptr(),
+                                   gg.data_ptr(), tx0.data_ptr(), tv0.data_ptr(), N, res, dt, None)
+    torch.cuda.synchronize()
+    assert L.pgmpm_last_error() == b""
+    grads = {"x": gix.cpu().numpy(), "v": giv.cpu().numpy(), "m": gim.cpu().numpy(), "g": gg.cpu().numpy()}
+    _fd_check(oracle, rng, x, v, m, g, res, dt, 1, sx, sv, grads)
+    L.launch_mpm_timestep_backward(tsx.data_ptr(), tsv.data_ptr(), gix.data_ptr(), giv.data_ptr(), gim.data_ptr(),
+                                   gg.data_ptr(), tx0.data_ptr(), tv0.data_ptr(), N, res + 4, dt, None)
+    torch.cuda.synchronize()
+    assert b"no launch_mpm_timestep_forward call" in L.pgmpm_last_error()
+
+
+def test_mpm_timestep_function_rollout_vs_central_differences(gpu, oracle):
+    """physgrad_b200.autograd.MPMTimestep chained over 3 steps by torch
+    autograd: gradients of sum(sx . x3) + sum(sv . v3) with respect to the
+    initial positions, velocities, masses and gravity against central
+    differences of the FP64 oracle's 3-step REF run."""
+    import torch
+    from physgrad_b200.autograd import MPMTimestep
+
+    rng = np.random.default_rng(72)
+    N, res, dt, steps = 2000, 32, 2e-3, 3
+    x, v, m = _ref_step_case(rng, N, res)
+    g = np.array([0.0, -9.8, 1.0], np.float32)
+    sx = rng.normal(0, 1, (N, 3))
+    sv = rng.normal(0, 1, (N, 3))
+    dev = torch.device("cuda:0")
+    leaf = lambda a: torch.tensor(a, dtype=torch.float32, device=dev, requires_grad=True)
+    tx, tv, tm, tg = leaf(x), leaf(v), leaf(m), leaf(g)
+    xs, vs = tx, tv
+    for _ in range(steps):
+        xs, vs = MPMTimestep.apply(xs, vs, tm, tg, res, dt)
+    loss = (torch.tensor(sx, dtype=torch.float32, device=dev) * xs).sum() + \
+        (torch.tensor(sv, dtype=torch.float32, device=dev) * vs).sum()
+    loss.backward()
+    grads = {"x": tx.grad.cpu().numpy(), "v": tv.grad.cpu().numpy(), "m": tm.grad.cpu().numpy(),
+             "g": tg.grad.cpu().numpy()}
+    _fd_check(oracle, rng, x, v, m, g, res, dt, steps, sx, sv, grads)
