@@ -993,7 +993,13 @@ __global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
             c = l;
             cend = wend[c];
         }
+        // the next particle's index is loaded one iteration ahead, so an
+        // iteration's payload loads do not wait on its index load (P2G of the
+        // two-material drop: 110.5 -> 107.4 us)
+        uint32_t pn = i0 < i1 ? V.order[i0] : 0u;
         for (uint32_t i = i0; i < i1; ++i) {
+            const uint32_t p = pn;
+            if (i + 1 < i1) pn = V.order[i + 1];
             if (i == cend) {
                 // the run passed the last particle of cell c: its sums are final
                 runs_store(T4, c, h, accA, accB);
@@ -1005,7 +1011,6 @@ __global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
                 }
                 cend = wend[c];
             }
-            const uint32_t p = V.order[i];
             if (p >= (uint32_t)N) {
                 flags |= FLAG_TILE_RANGE;
                 continue;
