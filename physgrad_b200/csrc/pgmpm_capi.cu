@@ -115,9 +115,13 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, 
     // P2G variant 1 builds its payload from the state's v and C
     V.write_vc = write_vc || s->pf.physics != PHYS_MLS || s->tune.p2g_variant == 1 ? 1 : 0;
     // per-step resets: tile counts, active node count, work cursors, and the
-    // active node tile flags (the bin sort writes every flag itself)
-    if (s->tune.step_sort != 0) CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
-    CK(cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * CNT_RESET, st));
+    // active node tile flags.  The bin sort's first kernel clears the
+    // counters and the sort writes every flag itself, so a bin-sorted step
+    // has no memset node.
+    if (s->tune.step_sort != 0) {
+        CK(cudaMemsetAsync(b.tile_flags, 0, sizeof(uint32_t) * (size_t)s->total_nt, st));
+        CK(cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * CNT_RESET, st));
+    }
     if (timed) CK(cudaEventRecord(s->ev[0], st));
     if (s->tune.step_sort == 0) {
         BinSortBufs B;

@@ -147,7 +147,8 @@ int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t
         View V = s->view_for(b);
         V.grid_mp = A.grid_gv;  // scatter target of the G2P reverse
         A.q_next = b.q_out;
-        CK(cudaMemsetAsync(b.counters + CNT_P2G_CURSOR, 0, sizeof(uint32_t), st));
+        // the slot's P2G work cursor is zero: the grid update of the slot's
+        // forward step cleared it after P2G
         CK(launch_adj_scatter(V, A, s->pf, s->tune, s->num_sms, st));
         CK(launch_adj_grid(V, A, s->tune, s->num_sms, st));
         CK(launch_adj_gather(V, A, s->pf, s->tune, st));

@@ -1277,6 +1277,9 @@ __global__ void __launch_bounds__(ADJR_T, 6) k_adj_runs(View V, AdjView AV) {
 // ------------------------------------------------------------ grid update
 template <int PHYS>
 __global__ void k_grid(View V) {
+    // P2G has finished with its work cursor: leave it at zero for the reverse
+    // of this step, whose scatter takes work from the same cursor
+    if (blockIdx.x == 0 && threadIdx.x == 0) V.counters[CNT_P2G_CURSOR] = 0u;
     const uint32_t count = V.counters[CNT_TILES];
     const int tiles_per_block = blockDim.x >> 6;
     const int l = threadIdx.x & 63;

@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
 // --------------------------------------------------- per-step bin sort
 // The MPM step groups particles by cell with a counting sort over the cells
 // (key = cell tile << 6 | cell in tile) instead of a full radix sort:
-//   bs_count     particles per cell and per cell tile, and each particle's
+//   bs_count     clears the step's counters (words [0, CNT_RESET));
+//                particles per cell and per cell tile, and each particle's
 //                slot in its cell.  Lanes holding equal keys in a run (the
 //                physical order stays close to cell order) share one atomic:
 //                the run's first lane adds the run length.  8 keys per thread
@@ -248,6 +249,9 @@ __global__ void __launch_bounds__(BS_T) bs_count(const uint32_t* __restrict__ ke
                                                  uint32_t* __restrict__ ccount, uint32_t* __restrict__ tcount,
                                                  uint32_t* __restrict__ slot, uint32_t* __restrict__ counters) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the step's per-step counters start at zero: this is the step's first
+    // kernel and it reads none of them (the step recording issues no memset)
+    if (blockIdx.x == 0 && threadIdx.x < CNT_RESET) counters[threadIdx.x] = 0u;
     const int64_t base = (int64_t)blockIdx.x * BS_TILE + warp * (32 * BS_ITEMS);
     uint32_t k[BS_ITEMS], cb[BS_ITEMS];
     int st[BS_ITEMS];
