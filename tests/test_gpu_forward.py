@@ -217,6 +217,35 @@ def test_mls_vs_fp64_oracle(gpu, oracle, case):
     assert sim.status() & 2 == 0
 
 
+@pytest.mark.parametrize("case", ["cfg4_small", "cfg5_small"])
+def test_batched_vs_fp64_oracle(gpu, oracle, case):
+    """Batched scenes of uneven counts and grids, each scene against the FP64
+    oracle run on that scene alone (its own material)."""
+    from physgrad_b200 import workloads as W
+
+    if case == "cfg4_small":
+        scenes, counts, mats, st, meta = W.batched_scenes(n_scenes=6, lo=2048, hi=40000, seed=11)
+        steps = 60
+    else:
+        scenes, counts, mats, st, meta = W.batched_scenes(n_scenes=4, lo=4096, hi=160000, seed=12, grids="large",
+                                                          v_sigma=0.1)
+        steps = 40
+    assert len(set(meta["grids"])) > 1
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(steps)
+    out = sim.download()
+    assert sim.status() & 2 == 0
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for s, sc in enumerate(scenes):
+        a, b = int(off[s]), int(off[s + 1])
+        sub = {k: v[a:b] for k, v in st.items() if k != "mat"}
+        omats = oracle.make_materials([(int(mats[s].model), float(mats[s].youngs_modulus),
+                                        float(mats[s].poisson_ratio))])
+        ref = oracle.run(_oracle_scene(oracle, sc), omats, _oracle_state(sub), steps, prec=64)
+        _assert_mls({k: v[a:b] for k, v in out.items() if k in ("x", "v", "F", "C")}, ref,
+                    f"{case} scene {s} ({b - a} particles, {sc.n[0]}^3)")
+
+
 def test_mls_grid_download_matches_oracle(gpu, oracle):
     from physgrad_b200 import workloads as W
 
