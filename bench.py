@@ -471,9 +471,11 @@ def run_adjoint(args, device=0):
     return line
 
 
-def run_batched(args, device=0, adjoint=False):
+def run_batched(args, device=0, adjoint=False, steps=None):
     """Config 4 (or 5 with adjoint): all scenes in one solver vs a loop of
-    single-scene solvers (one launch sequence per scene per step)."""
+    single-scene solvers (one launch sequence per scene per step).  steps:
+    the configuration's own step count when None and --workload names it,
+    else min(--steps, the configuration's)."""
     import torch
 
     import physgrad_b200 as pg
@@ -481,7 +483,7 @@ def run_batched(args, device=0, adjoint=False):
     torch.cuda.set_device(device)
     scenes, counts, mats, st, meta = make_workload("cfg5" if adjoint else "cfg4")
     N = int(sum(counts))
-    steps = min(args.steps, meta["steps"])
+    steps = min(args.steps, meta["steps"]) if steps is None else int(steps)
     off = np.concatenate([[0], np.cumsum(counts)])
     sl = lambda a, s: None if a is None else a[off[s]:off[s + 1]]
     big = pg.Simulator(scenes, counts, mats, device=device)
@@ -546,6 +548,53 @@ def run_batched(args, device=0, adjoint=False):
     for one in singles:
         one.close()
     return line
+
+
+def run_targets(args, device=0):
+    """The task's other targets, measured in the same run as the headline
+    line: forward + adjoint of the differentiable elastic cube (262,144
+    particles, 256 steps, checkpoints every 16) against its plain forward,
+    with the gradient checked against a full-size central difference; the
+    64-scene batched forward (500 steps) against a loop of single-scene
+    solvers; the 32-scene batched forward + adjoint (128 steps, checkpoints
+    every 8) against 32 sequential single-scene forward + adjoint solves.
+    Every figure is a device time (CUDA events) at the configuration's own
+    step count."""
+    import torch
+
+    adj = run_adjoint(args, device)
+    torch.cuda.empty_cache()
+    b4 = run_batched(args, device, adjoint=False, steps=500)
+    torch.cuda.empty_cache()
+    b5 = run_batched(args, device, adjoint=True, steps=128)
+    torch.cuda.empty_cache()
+    return {
+        "adjoint_ratio_vs_plain": round(adj["ratio_vs_plain_forward"], 4),
+        "grad_fd_rel_err": adj["grad_check"]["rel_err"],
+        "batched_speedup_vs_loop": round(b4["speedup_vs_loop"], 3),
+        "batched_adjoint_speedup_vs_loop": round(b5["speedup_vs_loop"], 3),
+        "targets": {
+            "differentiable_elastic_cube": {
+                "n_particles": adj["config"]["n_particles"], "steps": adj["steps"], "checkpoint_every": 16,
+                "plain_forward_ms": round(adj["plain_forward_ms"], 3),
+                "forward_adjoint_ms": round(adj["forward_adjoint_ms"], 3),
+                "ratio_vs_plain_forward": round(adj["ratio_vs_plain_forward"], 4), "target_ratio": 3.0,
+                "grad_check": adj["grad_check"],
+                "forward_adjoint_particle_steps_per_s": adj["value"]},
+            "batched_forward_64_scenes": {
+                "n_particles": b4["config"]["n_particles"], "steps": b4["steps"],
+                "batched_ms": round(b4["batched_ms"], 3), "loop_ms": round(b4["loop_ms"], 3),
+                "batched_particle_steps_per_s": b4["value"],
+                "loop_particle_steps_per_s": b4["loop_of_single_scene_value"],
+                "speedup_vs_loop": round(b4["speedup_vs_loop"], 3), "target_speedup": 1.5},
+            "batched_forward_adjoint_32_scenes": {
+                "n_particles": b5["config"]["n_particles"], "steps": b5["steps"], "checkpoint_every": 8,
+                "batched_ms": round(b5["batched_ms"], 3), "loop_ms": round(b5["loop_ms"], 3),
+                "batched_particle_steps_per_s": b5["value"],
+                "loop_particle_steps_per_s": b5["loop_of_single_scene_value"],
+                "speedup_vs_loop": round(b5["speedup_vs_loop"], 3)},
+        },
+    }
 
 
 def run_reference(args):
@@ -660,6 +709,8 @@ def main():
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="cfg4/cfg5: plain bench line instead of the batched comparison")
+    ap.add_argument("--no-targets", action="store_true",
+                    help="cfg2 at one GPU: leave out the adjoint and batched measurements added to the line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -686,6 +737,8 @@ def main():
             line = run_batched(args, local, adjoint=args.workload == "cfg5")
         else:
             line = run_ours(args, rank, world, local)
+            if world == 1 and args.workload == "cfg2" and not args.no_targets:
+                line.update(run_targets(args, local))
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -331,11 +331,13 @@ PGMPM_API int pgmpm_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* va
  * reference has no sort.  It calls no allocator.  Its scratch is a fixed
  * array in the library's device image (about 8.9 MB per GPU that loads the
  * library, held until exit), so n is limited to PGMPM_NOALLOC_MAX_PAIRS
- * (larger n returns PGMPM_ERR_ARG).  keys_out/vals_out must not alias the
- * inputs.  The first call on a device looks up the array's address and may
- * load the module: make it before any stream capture.  Calls share the
- * array, so calls that overlap on the GPU race; the caller orders them.
- * Asynchronous on `stream`. */
+ * (larger n returns PGMPM_ERR_ARG).  keys_out and vals_out must not overlap
+ * the inputs or each other (PGMPM_ERR_ARG).  The first call on a device
+ * looks up the array's address and may load the module: make it before any
+ * stream capture.  The address is kept for the process's life, so a
+ * cudaDeviceReset of a device after this entry point has been called on it
+ * is not supported.  Calls share the array, so calls that overlap on the GPU
+ * race; the caller orders them.  Asynchronous on `stream`. */
 #define PGMPM_NOALLOC_MAX_PAIRS (1 << 20)
 PGMPM_API int pgmpm_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                              uint32_t* vals_out, int64_t n, int32_t key_bits, void* stream);

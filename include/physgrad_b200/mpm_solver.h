@@ -15,6 +15,10 @@
 //   material_point_method.h (both define physgrad::mpm::MPMSolver).
 #pragma once
 
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <filesystem>
@@ -104,8 +108,12 @@ struct MPMSolverConfig {
     int max_materials = 8;
     int cuda_block_size = 256;
     bool enable_g2p2g_fusion = true;
+    // Accepted as in src/mpm_solver.h:53-55.  The reference's adaptive step
+    // (computeAdaptiveTimestep, :467-470) returns time_step unchanged and
+    // never reads the bounds; so does this implementation.
     bool enable_adaptive_timestep = false;
-    bool enable_profiling = false;
+    float min_timestep = 1e-6f;
+    float max_timestep = 1e-3f;
     // output (src/mpm_solver.h:57-60): run() writes the particles every
     // output_frequency seconds of simulated time as
     // output_directory/frame_NNNNN.vtk (legacy binary VTK).  Off by default
@@ -113,6 +121,13 @@ struct MPMSolverConfig {
     bool enable_output = false;
     float output_frequency = 0.01f;
     std::string output_directory = "./mpm_output";
+    // debug and profiling (src/mpm_solver.h:62-65).  enable_profiling times
+    // each kernel group with events (getMetrics' p2g/g2p/grid times);
+    // enable_debug_output and verify_conservation are accepted and, as in
+    // the reference, not read.
+    bool enable_profiling = false;
+    bool enable_debug_output = false;
+    bool verify_conservation = false;
     // additions of this implementation
     int physics = PGMPM_PHYSICS_MLS;
     int boundary = PGMPM_BC_STICKY;
@@ -137,37 +152,196 @@ struct MPMPerformanceMetrics {
     void reset() { *this = MPMPerformanceMetrics{}; }
 };
 
-// Host copy of the particle state with ParticleAoSoA's accessors
-// (src/mpm_data_structures.h:165-258); filled by MPMSolver::getParticles().
-template <typename T = float>
+// Host copy of the particle state with the accessors of the reference's
+// chunked container (src/mpm_data_structures.h:106-359).  Arrays are sized
+// to whole chunks, so get*Data() returns the same layout as the reference's
+// chunk arrays: per particle x, y, z (positions, velocities), one value
+// (mass, volume), F row-major (9), stress xx, yy, zz, xy, xz, yz (6).
+// MPMSolver::getParticles() fills positions, velocities, masses, volumes,
+// F, the APIC matrix C (getAffineMatrix) and material types; the stress is
+// not a state of the MLS step and stays as set.
+template <typename T = float, size_t ChunkSize = 256>
 class ParticleAoSoA {
 public:
-    size_t size() const { return x_.size() / 3; }
+    static constexpr size_t chunk_size = ChunkSize;
+    using scalar_type = T;
+
+    ParticleAoSoA() = default;
+    explicit ParticleAoSoA(size_t num_particles) { resize(num_particles); }
+
+    void resize(size_t num_particles) {
+        n_ = num_particles;
+        chunks_ = (num_particles + chunk_size - 1) / chunk_size;
+        const size_t cap = chunks_ * chunk_size;
+        x_.resize(3 * cap);
+        v_.resize(3 * cap);
+        m_.resize(cap);
+        V_.resize(cap);
+        F_.resize(9 * cap);
+        C_.resize(9 * cap);
+        stress_.resize(6 * cap);
+        type_.resize(cap, MaterialType::ELASTIC);
+        active_.resize(cap, 1u);
+    }
+    size_t size() const { return n_; }
+    size_t num_chunks() const { return chunks_; }
+
+    void setPosition(size_t i, T x, T y, T z) { x_[3 * i] = x; x_[3 * i + 1] = y; x_[3 * i + 2] = z; }
     void getPosition(size_t i, T& x, T& y, T& z) const { x = x_[3 * i]; y = x_[3 * i + 1]; z = x_[3 * i + 2]; }
+    void setVelocity(size_t i, T x, T y, T z) { v_[3 * i] = x; v_[3 * i + 1] = y; v_[3 * i + 2] = z; }
     void getVelocity(size_t i, T& x, T& y, T& z) const { x = v_[3 * i]; y = v_[3 * i + 1]; z = v_[3 * i + 2]; }
+    void setMass(size_t i, T m) { m_[i] = m; }
     T getMass(size_t i) const { return m_[i]; }
+    void setVolume(size_t i, T v) { V_[i] = v; }
     T getVolume(size_t i) const { return V_[i]; }
+    void setDeformationGradient(size_t i, const T F[9]) {
+        for (int k = 0; k < 9; ++k) F_[9 * i + k] = F[k];
+    }
     void getDeformationGradient(size_t i, T F[9]) const {
         for (int k = 0; k < 9; ++k) F[k] = F_[9 * i + k];
     }
     void getAffineMatrix(size_t i, T C[9]) const {
         for (int k = 0; k < 9; ++k) C[k] = C_[9 * i + k];
     }
-    std::vector<T> x_, v_, C_, F_, m_, V_;
+    void setStress(size_t i, const T s[6]) {
+        for (int k = 0; k < 6; ++k) stress_[6 * i + k] = s[k];
+    }
+    void getStress(size_t i, T s[6]) const {
+        for (int k = 0; k < 6; ++k) s[k] = stress_[6 * i + k];
+    }
+    void setMaterialType(size_t i, MaterialType t) { type_[i] = t; }
+    MaterialType getMaterialType(size_t i) const { return type_[i]; }
+    void setActive(size_t i, bool a) { active_[i] = a ? 1u : 0u; }
+    bool isActive(size_t i) const { return active_[i] != 0u; }
+
+    // bulk operations (src/mpm_data_structures.h:274-322)
+    void setPositions(const std::vector<std::array<T, 3>>& p) {
+        for (size_t i = 0; i < std::min(p.size(), size()); ++i) setPosition(i, p[i][0], p[i][1], p[i][2]);
+    }
+    void setVelocities(const std::vector<std::array<T, 3>>& p) {
+        for (size_t i = 0; i < std::min(p.size(), size()); ++i) setVelocity(i, p[i][0], p[i][1], p[i][2]);
+    }
+    void setMasses(const std::vector<T>& m) {
+        for (size_t i = 0; i < std::min(m.size(), size()); ++i) setMass(i, m[i]);
+    }
+    std::vector<std::array<T, 3>> getPositions() const { return triples(x_); }
+    std::vector<std::array<T, 3>> getVelocities() const { return triples(v_); }
+    std::vector<T> getMasses() const { return std::vector<T>(m_.begin(), m_.begin() + (ptrdiff_t)n_); }
+
+    // raw arrays (src/mpm_data_structures.h:325-342)
+    T* getPositionData() { return x_.data(); }
+    T* getVelocityData() { return v_.data(); }
+    T* getMassData() { return m_.data(); }
+    T* getVolumeData() { return V_.data(); }
+    T* getDeformationGradientData() { return F_.data(); }
+    T* getStressData() { return stress_.data(); }
+    MaterialType* getMaterialTypeData() { return type_.data(); }
+    uint32_t* getActiveData() { return active_.data(); }
+    const T* getPositionData() const { return x_.data(); }
+    const T* getVelocityData() const { return v_.data(); }
+    const T* getMassData() const { return m_.data(); }
+    const T* getVolumeData() const { return V_.data(); }
+    const T* getDeformationGradientData() const { return F_.data(); }
+    const T* getStressData() const { return stress_.data(); }
+    const MaterialType* getMaterialTypeData() const { return type_.data(); }
+    const uint32_t* getActiveData() const { return active_.data(); }
+    size_t getMemoryFootprint() const {
+        return chunks_ * chunk_size * (sizeof(T) * (3 + 3 + 1 + 1 + 9 + 6 + 9) + sizeof(MaterialType) + 2 * sizeof(uint32_t));
+    }
+
+private:
+    std::vector<std::array<T, 3>> triples(const std::vector<T>& a) const {
+        std::vector<std::array<T, 3>> r(n_);
+        for (size_t i = 0; i < n_; ++i) r[i] = {{a[3 * i], a[3 * i + 1], a[3 * i + 2]}};
+        return r;
+    }
+
+public:
+    // storage, filled by MPMSolver::getParticles() (also reachable through
+    // the get*Data() accessors above)
+    size_t n_ = 0, chunks_ = 0;
+    std::vector<T> x_, v_, m_, V_, F_, C_, stress_;
+    std::vector<MaterialType> type_;
+    std::vector<uint32_t> active_;
 };
 
+// Host copy of the grid after the last step's grid update, with the
+// reference's accessors (src/mpm_data_structures.h:369-530): index k nx ny +
+// j nx + i, masses, velocities, momentum (mass times velocity); forces are
+// not a state of the MLS step (the stress enters the momentum in P2G) and
+// read as zero, boundary flags as set.
 template <typename T = float>
 class MPMGrid {
 public:
+    using scalar_type = T;
+    MPMGrid() = default;
+    MPMGrid(int3_ dims, vec3<T> spacing, vec3<T> origin = {T(0), T(0), T(0)}) { reset(dims, spacing, origin); }
+
+    void reset(int3_ dims, vec3<T> spacing, vec3<T> origin) {
+        dims_ = dims;
+        spacing_ = spacing;
+        origin_ = origin;
+        const size_t n = (size_t)dims.x * dims.y * dims.z;
+        mass_.assign(n, T(0));
+        vel_.assign(3 * n, T(0));
+        force_.assign(3 * n, T(0));
+        mom_.assign(3 * n, T(0));
+        bc_.assign(n, 0u);
+    }
+    void clearGrid() {
+        std::fill(mass_.begin(), mass_.end(), T(0));
+        std::fill(vel_.begin(), vel_.end(), T(0));
+        std::fill(force_.begin(), force_.end(), T(0));
+        std::fill(mom_.begin(), mom_.end(), T(0));
+    }
+    std::array<T, 3> getGridSpacing() const { return {{spacing_.x, spacing_.y, spacing_.z}}; }
     int3_ getDimensions() const { return dims_; }
+    vec3<T> getSpacing() const { return spacing_; }
+    vec3<T> getOrigin() const { return origin_; }
     size_t getTotalNodes() const { return mass_.size(); }
     size_t getLinearIndex(int i, int j, int k) const {
         return (size_t)k * dims_.x * dims_.y + (size_t)j * dims_.x + (size_t)i;
     }
+    int3_ getGridIndex(size_t l) const {
+        const size_t layer = (size_t)dims_.x * dims_.y;
+        const int k = (int)(l / layer), r = (int)(l % layer);
+        return {r % dims_.x, r / dims_.x, k};
+    }
+    vec3<T> getWorldPosition(int i, int j, int k) const {
+        return {origin_.x + i * spacing_.x, origin_.y + j * spacing_.y, origin_.z + k * spacing_.z};
+    }
+    int3_ getGridPosition(T x, T y, T z) const {
+        return {(int)std::floor((x - origin_.x) / spacing_.x), (int)std::floor((y - origin_.y) / spacing_.y),
+                (int)std::floor((z - origin_.z) / spacing_.z)};
+    }
+    void setMass(size_t n, T m) { mass_[n] = m; }
     T getMass(size_t n) const { return mass_[n]; }
+    void setVelocity(size_t n, T vx, T vy, T vz) { vel_[3 * n] = vx; vel_[3 * n + 1] = vy; vel_[3 * n + 2] = vz; }
     void getVelocity(size_t n, T& vx, T& vy, T& vz) const { vx = vel_[3 * n]; vy = vel_[3 * n + 1]; vz = vel_[3 * n + 2]; }
+    void addVelocity(size_t n, T dx, T dy, T dz) { vel_[3 * n] += dx; vel_[3 * n + 1] += dy; vel_[3 * n + 2] += dz; }
+    void setForce(size_t n, T fx, T fy, T fz) { force_[3 * n] = fx; force_[3 * n + 1] = fy; force_[3 * n + 2] = fz; }
+    void addForce(size_t n, T fx, T fy, T fz) { force_[3 * n] += fx; force_[3 * n + 1] += fy; force_[3 * n + 2] += fz; }
+    void setBoundaryCondition(size_t n, uint32_t f) { bc_[n] = f; }
+    uint32_t getBoundaryCondition(size_t n) const { return bc_[n]; }
+    T* getMassData() { return mass_.data(); }
+    T* getVelocityData() { return vel_.data(); }
+    T* getForceData() { return force_.data(); }
+    T* getMomentumData() { return mom_.data(); }
+    uint32_t* getBoundaryConditionData() { return bc_.data(); }
+    const T* getMassData() const { return mass_.data(); }
+    const T* getVelocityData() const { return vel_.data(); }
+    const T* getForceData() const { return force_.data(); }
+    const T* getMomentumData() const { return mom_.data(); }
+    const uint32_t* getBoundaryConditionData() const { return bc_.data(); }
+    size_t getMemoryFootprint() const {
+        return sizeof(T) * (mass_.size() + vel_.size() + force_.size() + mom_.size()) + sizeof(uint32_t) * bc_.size();
+    }
+
+    // storage, filled by MPMSolver::getGrid()
     int3_ dims_{0, 0, 0};
-    std::vector<T> mass_, vel_;
+    vec3<T> spacing_{T(0), T(0), T(0)}, origin_{T(0), T(0), T(0)};
+    std::vector<T> mass_, vel_, force_, mom_;
+    std::vector<uint32_t> bc_;
 };
 
 template <typename T = float>
@@ -279,14 +453,14 @@ public:
         }
     }
 
-    const particle_container& getParticles() {
+    // Data access (src/mpm_solver.h:324-326), callable on a const solver:
+    // the host copies are refreshed from the device on each call.
+    const particle_container& getParticles() const {
         const size_t n = m_.size();
-        particles_.x_.resize(3 * n);
-        particles_.v_.resize(3 * n);
-        particles_.C_.resize(9 * n);
-        particles_.F_.resize(9 * n);
-        particles_.m_ = m_;
-        particles_.V_ = V_;
+        particles_.resize(n);
+        std::copy(m_.begin(), m_.end(), particles_.m_.begin());
+        std::copy(V_.begin(), V_.end(), particles_.V_.begin());
+        for (size_t i = 0; i < n; ++i) particles_.type_[i] = config_.materials[(size_t)mat_[i]].type;
         if (initialized_ && n)
             physgrad_b200_detail::check(pgmpm_download(h_, particles_.x_.data(), particles_.v_.data(),
                                                        particles_.C_.data(), particles_.F_.data(), PGMPM_PTR_HOST,
@@ -294,18 +468,19 @@ public:
         return particles_;
     }
 
-    const grid_container& getGrid() {
-        const size_t nodes = (size_t)config_.grid_dimensions.x * config_.grid_dimensions.y * config_.grid_dimensions.z;
-        grid_.dims_ = config_.grid_dimensions;
-        grid_.mass_.assign(nodes, 0.f);
-        grid_.vel_.assign(3 * nodes, 0.f);
-        if (initialized_)
+    const grid_container& getGrid() const {
+        grid_.reset(config_.grid_dimensions, {config_.grid_spacing.x, config_.grid_spacing.y, config_.grid_spacing.z},
+                    {config_.domain_origin.x, config_.domain_origin.y, config_.domain_origin.z});
+        if (initialized_) {
             physgrad_b200_detail::check(
                 pgmpm_download_grid(h_, 0, grid_.mass_.data(), grid_.vel_.data(), PGMPM_PTR_HOST, nullptr));
+            for (size_t n = 0; n < grid_.mass_.size(); ++n)
+                for (int a = 0; a < 3; ++a) grid_.mom_[3 * n + a] = grid_.mass_[n] * grid_.vel_[3 * n + a];
+        }
         return grid_;
     }
 
-    const MPMPerformanceMetrics& getMetrics() {
+    const MPMPerformanceMetrics& getMetrics() const {
         if (initialized_) {
             pgmpm_metrics m{};
             physgrad_b200_detail::check(pgmpm_get_metrics(h_, &m));
@@ -315,6 +490,10 @@ public:
             metrics_.g2p_time = m.g2p_ms * 1e-3;
             metrics_.grid_update_time = m.grid_ms * 1e-3;
             metrics_.average_particles_per_second = (float)m.particle_steps_per_s;
+            metrics_.particle_memory = m_.size() * (6 * 16 + 8 + 4);
+            metrics_.grid_memory = (size_t)config_.grid_dimensions.x * config_.grid_dimensions.y *
+                                   config_.grid_dimensions.z * 32;
+            metrics_.total_memory_usage = metrics_.particle_memory + metrics_.grid_memory;
         }
         return metrics_;
     }
@@ -333,9 +512,10 @@ private:
     bool initialized_ = false;
     std::vector<float> x_, v_, m_, V_;
     std::vector<int32_t> mat_;
-    particle_container particles_;
-    grid_container grid_;
-    MPMPerformanceMetrics metrics_;
+    // host copies refreshed by the const getters
+    mutable particle_container particles_;
+    mutable grid_container grid_;
+    mutable MPMPerformanceMetrics metrics_;
     // the step that ended at simulated time t crossed a multiple of output_frequency
     bool crosses_output(float t) const {
         return config_.output_frequency > 0.f && (int)(t / config_.output_frequency) >

@@ -19,8 +19,10 @@ namespace {
 
 // ------------------------------------------------------- host parallelism
 // std::thread range split (the image has no OpenMP runtime) and CAS-based
-// floating-point atomic add for the scatter loops.
-int g_threads = 1;
+// floating-point atomic add for the scatter loops.  The worker count is per
+// calling thread, so that several host threads may run the oracle at once
+// (each spawning its own workers); it is read only on the calling thread.
+thread_local int g_threads = 1;
 
 template <class Fn> void parallel_range(int64_t n, Fn fn) {
     int nt = g_threads > 1 ? g_threads : 1;
@@ -905,14 +907,22 @@ extern "C" int oracle_adjoint(const oracle_scene* sc, const oracle_material* mat
     S.gp.assign(3 * S.g.nodes, 0);
     S.gvpre.assign(3 * S.g.nodes, 0);
     S.gv.assign(3 * S.g.nodes, 0);
-    std::vector<State<double>> hist(steps + 1);
-    hist[0].x.assign(x, x + 3 * n);
-    hist[0].v.assign(v, v + 3 * n);
-    hist[0].C.assign(C, C + 9 * n);
-    hist[0].F.assign(F, F + 9 * n);
-    for (int s = 0; s < steps; ++s) {
-        hist[s + 1] = hist[s];
-        mls_step(S, hist[s + 1]);
+    // States are kept every K steps and each segment is recomputed from its
+    // checkpoint before its reverse, so host memory stays at about
+    // (steps / K + K) states instead of steps + 1.
+    const int K = std::max(1, (int)std::ceil(std::sqrt((double)std::max(steps, 1))));
+    const int nseg = (steps + K - 1) / K;
+    std::vector<State<double>> ck(std::max(nseg, 1));
+    ck[0].x.assign(x, x + 3 * n);
+    ck[0].v.assign(v, v + 3 * n);
+    ck[0].C.assign(C, C + 9 * n);
+    ck[0].F.assign(F, F + 9 * n);
+    {
+        State<double> cur = ck[0];
+        for (int s = 0; s < steps; ++s) {
+            if (s % K == 0) ck[s / K] = cur;
+            mls_step(S, cur);
+        }
     }
     State<double> a;
     a.x.assign(gx, gx + 3 * n);
@@ -920,11 +930,20 @@ extern "C" int oracle_adjoint(const oracle_scene* sc, const oracle_material* mat
     a.C.assign(gC, gC + 9 * n);
     a.F.assign(gF, gF + 9 * n);
     std::vector<double> gEv(nmat, 0.0);
-    for (int s = steps - 1; s >= 0; --s) {
-        // rebuild the grid of step s
-        mls_p2g(S, hist[s]);
-        mls_grid(S);
-        mls_step_adjoint(S, hist[s], a, gEv);
+    std::vector<State<double>> hist(K);
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int s0 = seg * K, len = std::min(K, steps - s0);
+        hist[0] = ck[seg];
+        for (int j = 1; j < len; ++j) {
+            hist[j] = hist[j - 1];
+            mls_step(S, hist[j]);
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            // rebuild the grid of step s0 + j
+            mls_p2g(S, hist[j]);
+            mls_grid(S);
+            mls_step_adjoint(S, hist[j], a, gEv);
+        }
     }
     std::memcpy(gx, a.x.data(), sizeof(double) * 3 * n);
     std::memcpy(gv, a.v.data(), sizeof(double) * 3 * n);

@@ -48,11 +48,36 @@ class Material(ctypes.Structure):
     ]
 
 
+def reference_src() -> str | None:
+    """The reference's ``src`` directory, or None when it is not on this machine.
+
+    Taken from the environment variable PGMPM_REFERENCE_SRC, else from the
+    ``reference_path`` field of the repository's BASELINE.json (its ``src``
+    subdirectory).  The GPU hosts have no reference tree and use the files
+    built beforehand into oracle/_ref."""
+    env = os.environ.get("PGMPM_REFERENCE_SRC")
+    if env:
+        return env if os.path.isdir(env) else None
+    meta = os.path.join(os.path.dirname(HERE), "BASELINE.json")
+    try:
+        import json
+
+        with open(meta) as f:
+            root = json.load(f).get("reference_path")
+    except (OSError, ValueError):
+        return None
+    if not root:
+        return None
+    src = os.path.join(root, "src")
+    return src if os.path.isdir(src) else None
+
+
 def build(with_ref: bool = True) -> None:
     """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
     targets = ["all"]
-    if with_ref and os.path.isdir("/root/reference/src"):
-        targets.append("ref")
+    src = reference_src() if with_ref else None
+    if src:
+        targets += ["ref", "REF_SRC=" + src]
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -200,6 +225,60 @@ def adjoint(scene: Scene, mats, state: dict, steps: int, grads_out: dict, nthrea
     if rc != 0:
         raise RuntimeError(f"oracle_adjoint failed: {rc}")
     return {"x": gx, "v": gv, "C": gC.reshape(n, 3, 3), "F": gF.reshape(n, 3, 3), "E": gE}
+
+
+def com_loss(x, target=(0.5, 0.3, 0.5)) -> float:
+    """||mean(x) - target||^2: the centre-of-mass loss of the differentiable
+    configuration (equal particle masses, so the mean is the centre of mass)."""
+    c = np.asarray(x, dtype=np.float64).mean(0) - np.asarray(target, dtype=np.float64)
+    return float((c * c).sum())
+
+
+def fd_v0_com(scene: Scene, mats, state: dict, steps: int, coords, eps: float = 1e-3, target=(0.5, 0.3, 0.5),
+              workers: int = 0):
+    """FP64 central differences of com_loss after ``steps`` steps with respect
+    to the initial velocity coordinates ``coords`` ((particle, axis) pairs):
+    (L(v0 + eps e) - L(v0 - eps e)) / (2 eps).  The 2 len(coords) forward runs
+    go to concurrent host threads, one oracle worker each."""
+    import concurrent.futures
+
+    def one(c, sign):
+        st = dict(state)
+        v = np.array(state["v"], dtype=np.float64, copy=True)
+        v[c[0], c[1]] += sign * eps
+        st["v"] = v
+        return com_loss(run(scene, mats, st, steps, prec=64, nthreads=1)["x"], target)
+
+    jobs = [(c, s) for c in coords for s in (1.0, -1.0)]
+    nw = workers or min(len(jobs), os.cpu_count() or 1)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=nw) as ex:
+        vals = list(ex.map(lambda a: one(*a), jobs))
+    return np.array([(vals[2 * i] - vals[2 * i + 1]) / (2 * eps) for i in range(len(coords))])
+
+
+def ref_diff_available() -> bool:
+    return os.path.exists(REF_DIFF_PATH)
+
+
+def ref_diff_run(x, v, m, n, dx, dt, steps):
+    """The reference's own DifferentiableMPMSystem<float> (oracle/_ref): the
+    forward with gradient recording on (simulationStep(dt), default gravity),
+    then computeGradients().  Returns its final positions and the particle
+    velocity and position gradients it reports."""
+    R = ctypes.CDLL(REF_DIFF_PATH)
+    fp = ctypes.c_void_p
+    R.ref_diff_run.argtypes = [ctypes.c_int64, fp, fp, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                               ctypes.c_float, ctypes.c_int, fp, fp, fp]
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    m = np.ascontiguousarray(m, dtype=np.float32)
+    N = x.shape[0]
+    xo, gv, gx = np.empty_like(x), np.empty_like(x), np.empty_like(x)
+    rc = R.ref_diff_run(N, x.ctypes.data, v.ctypes.data, m.ctypes.data, n[0], n[1], n[2], dx, dt, steps,
+                        xo.ctypes.data, gv.ctypes.data, gx.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("ref_diff_run failed")
+    return {"x": xo, "grad_v": gv, "grad_x": gx}
 
 
 def ref_run(x, v, m, vol, n, dx, dt, gravity, steps, origin=(0.0, 0.0, 0.0), want_grid=False):

@@ -53,7 +53,24 @@ SORT_RADIX = 1
 PTR_HOST = 0
 PTR_DEVICE = 1
 
-NOALLOC_MAX_PAIRS = 1 << 20
+
+
+def _header_define(name: str) -> int:
+    """Integer value of a #define in include/pgmpm.h (the C-ABI's own header),
+    so that Python never carries a second copy of a limit the library uses."""
+    import re
+
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pgmpm.h")
+    with open(hdr) as f:
+        m = re.search(r"^#define\s+" + name + r"\s+\(?\s*(\d+)\s*(?:<<\s*(\d+))?\s*\)?", f.read(), re.M)
+    if not m:
+        raise RuntimeError(f"{name} not found in {hdr}")
+    v = int(m.group(1))
+    return v << int(m.group(2)) if m.group(2) else v
+
+
+# maximum pairs of pgmpm_radix_sort_pairs_noalloc (PGMPM_NOALLOC_MAX_PAIRS)
+NOALLOC_MAX_PAIRS = _header_define("PGMPM_NOALLOC_MAX_PAIRS")
 
 
 class SceneDesc(ctypes.Structure):

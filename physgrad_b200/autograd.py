@@ -29,7 +29,9 @@ class MPMSimulate(torch.autograd.Function):
 
     ``E`` is a float32 tensor [n_materials] of Young's moduli (bulk modulus
     for FLUID materials); gradients flow to x0, v0, C0, F0 and E.  m, V0 and
-    the material ids are constants of the simulation."""
+    the material ids are constants of the simulation.  The Simulator holds
+    one recording, so two rollouts in one autograd graph need two
+    Simulators: a backward whose recording was replaced raises PGMPMError."""
 
     @staticmethod
     def forward(ctx, sim: Simulator, n_steps: int, checkpoint_every: int, x0, v0, C0, F0, E, m, V0,
@@ -51,11 +53,17 @@ class MPMSimulate(torch.autograd.Function):
         sim.download(out, stream=stream)
         ctx.sim = sim
         ctx.N = N
+        ctx.generation = sim.forward_generation
         return out["x"], out["v"], out["C"], out["F"]
 
     @staticmethod
     def backward(ctx, gx, gv, gC, gF):
         sim, N = ctx.sim, ctx.N
+        if sim.forward_generation != ctx.generation:
+            # the solver keeps one recording: a later forward on the same
+            # Simulator replaced the one this node needs
+            raise PGMPMError(-3, "MPMSimulate.backward: the Simulator has run another forward since this rollout "
+                                 "(it keeps one recording); use one Simulator per rollout in a graph")
         c = lambda t: None if t is None else t.detach().to(torch.float32).contiguous()
         stream = torch.cuda.current_stream()
         grads = sim.backward({"x": c(gx), "v": c(gv), "C": None if gC is None else c(gC).reshape(N, 9),

@@ -20,6 +20,11 @@
 // first call made on that device.  That first call may load the module, so
 // make it before starting any stream capture.
 //
+// The address found on the first call is kept for the life of the process.
+// A cudaDeviceReset after that call reloads the module and would leave the
+// kept address stale, so resetting a device that this entry point has used
+// is not supported.
+//
 // Every call shares the one array and leaves its contents behind.  Nothing in
 // it needs to start at zero: each pass writes all the histogram words it
 // later reads, and the ping-pong buffer is fully written before it is read.
@@ -69,6 +74,14 @@ cudaError_t scratch_on_current_device(uint32_t** out) {
     return cudaSuccess;
 }
 
+// True when the byte ranges of two n-word arrays overlap (either may be null).
+bool overlaps(const uint32_t* a, const uint32_t* b, int64_t n) {
+    if (!a || !b) return false;
+    const uintptr_t pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t len = (uintptr_t)n * sizeof(uint32_t);
+    return pa < pb + len && pb < pa + len;
+}
+
 }  // namespace
 
 // Defined in pgmpm_capi.cu: records the message returned by pgmpm_last_error().
@@ -89,8 +102,14 @@ extern "C" int pgmpm_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uin
     if (n == 0) return PGMPM_OK;
     if (!keys_in || !keys_out || !vals_out)
         return pgmpm_set_error(PGMPM_ERR_ARG, "pgmpm_radix_sort_pairs_noalloc: null pointer");
-    if (keys_in == keys_out || (vals_in && vals_in == vals_out))
-        return pgmpm_set_error(PGMPM_ERR_ARG, "pgmpm_radix_sort_pairs_noalloc: outputs must not alias inputs");
+    // The first pass writes the caller's outputs (or the scratch) while it
+    // still reads the inputs, so no output may overlap an input or the other
+    // output.
+    if (overlaps(keys_in, keys_out, n) || overlaps(keys_in, vals_out, n) || overlaps(vals_in, keys_out, n) ||
+        overlaps(vals_in, vals_out, n) || overlaps(keys_out, vals_out, n))
+        return pgmpm_set_error(PGMPM_ERR_ARG,
+                               "pgmpm_radix_sort_pairs_noalloc: the output arrays must not overlap the input "
+                               "arrays or each other");
     uint32_t* scratch = nullptr;
     cudaError_t e = scratch_on_current_device(&scratch);
     if (e != cudaSuccess) {

@@ -175,6 +175,10 @@ class Simulator:
         check(L.pgmpm_create(sd, len(self.scenes), cn, md, len(self.materials), int(device), ctypes.byref(h)))
         self._h = h
         self.device = device
+        # incremented by every forward_checkpointed: a recording's identity,
+        # so that a backward can tell whether the recording it was made for
+        # is still the one the solver holds
+        self.forward_generation = 0
         if tuning:
             self.set_tuning(**tuning)
 
@@ -308,6 +312,9 @@ class Simulator:
 
     # -- differentiation
     def forward_checkpointed(self, n_steps: int, checkpoint_every: int, stream=None):
+        """Runs n_steps from the current state and records them for backward();
+        each call replaces the previous recording (forward_generation + 1)."""
+        self.forward_generation += 1
         check(lib().pgmpm_forward_checkpointed(self._h, int(n_steps), int(checkpoint_every), _stream_handle(stream)))
 
     def backward(self, grads_out: dict, grads_in: Optional[dict] = None, gE=None, stream=None):

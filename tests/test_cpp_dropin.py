@@ -30,6 +30,47 @@ def test_dropin_header_runs_on_gpu(gpu, built_lib, tmp_path):
 
 
 @pytest.mark.gpu
+def test_dropin_solver_matches_fp64_oracle_per_particle(gpu, oracle, built_lib, tmp_path):
+    """MPMSolver<float> of the drop-in header (config fields min_timestep,
+    max_timestep, enable_debug_output, verify_conservation set; 15 steps via
+    step() and run(); the state read through a const solver with
+    getPositions, getVelocities, getMasses, getPositionData and
+    getVelocityData) against the FP64 oracle on the same inputs, particle by
+    particle: |dx| <= 2e-5, |dv| <= 1e-3 max|v| + 1e-5 (the MLS bounds of
+    tests/test_gpu_forward.py)."""
+    import numpy as np
+
+    exe = str(tmp_path / "drop_in")
+    _build(built_lib, exe)
+    rng = np.random.default_rng(17)
+    N = 3000
+    x = rng.uniform(0.35, 0.65, (N, 3)).astype(np.float32)
+    v = rng.normal(0.0, 0.3, (N, 3)).astype(np.float32)
+    m = np.full(N, 1.25e-4, np.float32)
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(fin, "wb") as f:
+        np.asarray([N], np.int32).tofile(f)
+        for a in (x, v, m):
+            a.tofile(f)
+    r = subprocess.run([exe, "compare", fin, fout], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    out = np.fromfile(fout, np.float32)
+    ox, ov = out[:3 * N].reshape(N, 3), out[3 * N:].reshape(N, 3)
+    # the header's defaults: sticky walls 3 nodes thick, fixed-corotated E 1e4,
+    # nu 0.3, density 1000 (V0 = m / density)
+    sc = oracle.make_scene((32, 32, 32), np.float32(1 / 32), np.float32(1e-4), gravity=(0.0, np.float32(-9.8), 0.0),
+                           physics=oracle.MLS, boundary=oracle.BC_STICKY, bthick=3)
+    st = dict(x=x.astype(np.float64), v=v.astype(np.float64), C=np.zeros((N, 9)), F=np.tile(np.eye(3).ravel(), (N, 1)),
+              m=m.astype(np.float64), V0=(m / np.float32(1000.0)).astype(np.float64))
+    ref = oracle.run(sc, oracle.make_materials([(oracle.FIXED_COROTATED, 1e4, 0.3)]), st, 15, prec=64)
+    ex = np.abs(ox - ref["x"]).max()
+    ev = np.abs(ov - ref["v"]).max()
+    print(f"MPMSolver<float> drop-in vs FP64, 15 steps: |dx| {ex:.2e} |dv| {ev:.2e} (max |v| {np.abs(ref['v']).max():.2e})")
+    assert ex <= 2e-5, ex
+    assert ev <= 1e-3 * np.abs(ref["v"]).max() + 1e-5, ev
+
+
+@pytest.mark.gpu
 def test_dropin_run_writes_vtk_frames(gpu, built_lib, read_vtk, tmp_path):
     """enable_output: run() writes output_directory/frame_NNNNN.vtk whenever a
     step crosses a multiple of output_frequency (1e-3 s at 2.5e-4 s: 3 or 4

@@ -411,3 +411,96 @@ def test_mpm_timestep_function_rollout_vs_central_differences(gpu, oracle):
     grads = {"x": tx.grad.cpu().numpy(), "v": tv.grad.cpu().numpy(), "m": tm.grad.cpu().numpy(),
              "g": tg.grad.cpu().numpy()}
     _fd_check(oracle, rng, x, v, m, g, res, dt, steps, sx, sv, grads)
+
+
+def test_reference_adjoint_returns_zeros_where_ours_matches_fd(gpu, oracle):
+    """The reference's own MPM adjoint on the inputs of
+    test_adjoint_matches_fp64_oracle (x, v, m of its seeded case; C = 0, F = I,
+    the reference's starting state): DifferentiableMPMSystem<float> records an
+    empty backward (src/differentiable_mpm.h:871-876), so computeGradients()
+    returns zeros for every particle.  Our adjoint of the centre-of-mass loss
+    on the same inputs is non-zero and matches FP64 central differences
+    (eps 1e-3) at 8 seeded v0 coordinates to 1e-3 relative."""
+    if not oracle.ref_diff_available():
+        pytest.skip("oracle/_ref not built")
+    bc, k = 1, 2
+    rng = np.random.default_rng(40 + bc + k)
+    N, n, steps, dt = 1500, 16, 6, 1e-3
+    st = _case(rng, N, n)
+    ref = oracle.ref_diff_run(st["x"], st["v"], st["m"], (n, n, n), 1.0 / n, dt, steps)
+    assert np.abs(ref["x"] - st["x"]).max() > 0.0  # the reference did step the particles
+    mats = [gpu.createElasticMaterial(1000, 1e4, 0.3)]
+    scene = gpu.Scene((n, n, n), 1.0 / n, dt, (0, -9.8, 0), (0, 0, 0), 0, bc, 3)
+    sim = gpu.Simulator([scene], [N], mats)
+    sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"])
+    sim.forward_checkpointed(steps, k)
+    x = sim.download()["x"].astype(np.float64)
+    tgt = np.array([0.5, 0.3, 0.5])
+    g = sim.backward({"x": np.tile(2.0 * (x.mean(0) - tgt) / N, (N, 1)).astype(np.float32)})
+    osc = oracle.make_scene((n, n, n), 1.0 / n, dt, physics=oracle.MLS, boundary=bc, bthick=3)
+    ost = {"x": st["x"].astype(np.float64), "v": st["v"].astype(np.float64), "C": np.zeros((N, 9)),
+           "F": np.tile(np.eye(3).ravel(), (N, 1)), "m": st["m"].astype(np.float64), "V0": st["V0"].astype(np.float64)}
+    coords = [(int(p), int(a)) for p, a in zip(rng.choice(N, 8, replace=False), rng.integers(0, 3, 8))]
+    fd = oracle.fd_v0_com(osc, oracle.make_materials([(oracle.FIXED_COROTATED, 1e4, 0.3)]), ost, steps, coords,
+                          eps=1e-3, target=tgt)
+    ours = np.array([g["v"][p, c] for p, c in coords])
+    theirs = np.array([ref["grad_v"][p, c] for p, c in coords])
+    for (p, c), a, b, f in zip(coords, ours, theirs, fd):
+        print(f"dL/dv0[{p},{c}]: ours {a:+.6e}  reference {b:+.1e}  FP64 central difference {f:+.6e}")
+    assert not np.any(ref["grad_v"]) and not np.any(ref["grad_x"])
+    assert np.abs(ours).min() > 0.0
+    assert (np.abs(ours - fd) <= 1e-3 * np.abs(fd)).all(), (ours, fd)
+
+
+def test_backward_twice_on_one_recording_gives_the_same_gradients(gpu):
+    """A second backward over the same recording replays every segment
+    (including the one the forward left in the tape, which the first
+    backward overwrote) and must return the same non-zero gradients: the
+    reverse scatter takes its work from the cursor the replayed step's grid
+    update leaves at zero."""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.two_material_drop(n_particles=20000, n=32, seed=31)
+    N = counts[0]
+    sim = gpu.Simulator(scenes, counts, mats)
+    sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st["mat"])
+    sim.forward_checkpointed(24, 8)
+    out = sim.download()
+    go = {"x": (out["x"] - 0.5).astype(np.float32) / N, "v": out["v"] / N}
+    g1 = sim.backward(go)
+    g2 = sim.backward(go)
+    for key in ("x", "v", "C", "F", "E"):
+        a, b = np.asarray(g1[key]).ravel(), np.asarray(g2[key]).ravel()
+        assert np.abs(a).max() > 0.0, key
+        assert np.abs(a - b).max() <= 1e-4 * np.abs(a).max(), key
+
+
+def test_two_rollouts_on_one_simulator_refuse_a_stale_backward(gpu):
+    """MPMSimulate keeps the Simulator in its context; the Simulator holds one
+    recording.  Two rollouts on one Simulator in one graph: the first
+    rollout's backward would see the second's recording, so it raises."""
+    import torch
+
+    from physgrad_b200 import PGMPMError
+    from physgrad_b200.autograd import simulate
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=4096, n=32, v_sigma=0.1, seed=33)
+    sim = gpu.Simulator(scenes, counts, mats)
+    dev = torch.device("cuda")
+    x0 = torch.tensor(st["x"], device=dev)
+    m, V0 = torch.tensor(st["m"], device=dev), torch.tensor(st["V0"], device=dev)
+    E = torch.tensor([1e4], device=dev, requires_grad=True)
+    va = torch.tensor(st["v"], device=dev, requires_grad=True)
+    vb = torch.tensor(st["v"] * 0.5, device=dev, requires_grad=True)
+    xa = simulate(sim, x0, va, E, m, V0, 8, 4)[0]
+    xb = simulate(sim, x0, vb, E, m, V0, 8, 4)[0]
+    with pytest.raises(PGMPMError, match="another forward"):
+        (xa.sum() + xb.sum()).backward()
+    # one Simulator per rollout works
+    sim2 = gpu.Simulator(scenes, counts, mats)
+    va.grad = None
+    xa = simulate(sim, x0, va, E, m, V0, 8, 4)[0]
+    xb = simulate(sim2, x0, vb, E, m, V0, 8, 4)[0]
+    (xa.sum() + xb.sum()).backward()
+    assert va.grad is not None and vb.grad is not None

@@ -15,9 +15,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
 def _sort(L, fn, k, v, ko, vo, n, bits):
-    rc = getattr(L, fn)(ctypes.c_void_p(k.data_ptr()), ctypes.c_void_p(v.data_ptr()), ctypes.c_void_p(ko.data_ptr()),
-                        ctypes.c_void_p(vo.data_ptr()), n, bits, None)
+    """v = None passes a null value array (values = 0..n-1)."""
+    rc = getattr(L, fn)(_ptr(k), _ptr(v), _ptr(ko), _ptr(vo), n, bits, None)
     return rc
 
 
@@ -68,3 +72,48 @@ def test_noalloc_sort_rejects_sizes_beyond_its_maximum(gpu):
                C.NOALLOC_MAX_PAIRS + 1, 8)
     assert rc == C.PGMPM_ERR_ARG
     assert b"exceeds the maximum" in L.pgmpm_last_error()
+
+
+def test_noalloc_sort_null_values_is_the_stable_permutation(gpu):
+    """vals_in = NULL sorts the indices 0..n-1 along with the keys: the result
+    is the stable argsort, equal to the allocating entry point's, on two calls
+    in a row (the second reuses the scratch the first left behind)."""
+    import torch
+
+    from physgrad_b200 import _capi as C
+
+    L = C.lib()
+    for n, bits, seed in ((300007, 17, 21), (4099, 9, 22)):
+        rng = np.random.default_rng(seed)
+        kk = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+        k = torch.from_numpy(kk.view(np.int32)).cuda()
+        kn, vn, ka, va = (torch.empty_like(k) for _ in range(4))
+        C.check(_sort(L, "pgmpm_radix_sort_pairs_noalloc", k, None, kn, vn, n, bits))
+        C.check(_sort(L, "pgmpm_radix_sort_pairs", k, None, ka, va, n, bits))
+        torch.cuda.synchronize()
+        assert torch.equal(kn, ka) and torch.equal(vn, va)
+        ref = np.argsort(kk, kind="stable").astype(np.uint32)
+        assert np.array_equal(vn.cpu().numpy().view(np.uint32), ref)
+        assert np.array_equal(kn.cpu().numpy().view(np.uint32), kk[ref])
+
+
+def test_noalloc_sort_rejects_overlapping_outputs(gpu):
+    """An output that overlaps an input (or the other output) would be written
+    by the first pass while that pass still reads it: rejected before any
+    work, including the cross cases (keys out over values in, a partial
+    overlap) and both outputs in one array."""
+    import torch
+
+    from physgrad_b200 import _capi as C
+
+    L = C.lib()
+    n = 1024
+    buf = torch.zeros(4 * n, dtype=torch.int32, device="cuda")
+    k, v, ko, vo = buf[:n], buf[n:2 * n], buf[2 * n:3 * n], buf[3 * n:]
+    C.check(_sort(L, "pgmpm_radix_sort_pairs_noalloc", k, v, ko, vo, n, 8))
+    torch.cuda.synchronize()
+    bad = [(k, v, v, vo), (k, v, ko, k), (k, v, buf[n // 2:n // 2 + n], vo), (k, v, ko, buf[2 * n + 8:3 * n + 8]),
+           (k, None, ko, k)]
+    for a, b, c, d in bad:
+        assert _sort(L, "pgmpm_radix_sort_pairs_noalloc", a, b, c, d, n, 8) == C.PGMPM_ERR_ARG
+        assert b"must not overlap" in L.pgmpm_last_error()
