@@ -217,8 +217,17 @@ PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, i
  * 4: variant 3's lane pairs walking equal runs of each tile's sorted
  * particles instead of one cell each, cells shared by runs merged in shared
  * memory (MLS forward with the bin sort; with the radix step sort it runs
- * variant 3).  pgmpm_create picks 4 for MLS solvers that use the bin sort,
- * else 3 from 2^20 particles and 2 below; REF_COMPAT runs variant 2 for 2-4.
+ * variant 3);
+ * 5: variant 4, fused with G2P: from the second step of a chain, each
+ * step's G2P kernel also does the next step's P2G (one lane per run of a
+ * tile's sorted particles, the tile's node velocities staged in shared
+ * memory, the payload never written to memory), so a step is the sort, the
+ * grid update and that one kernel.  The pending P2G carries over to the
+ * next pgmpm_step call; uploads, material or scene changes and
+ * differentiation recompute it.  MLS with the bin sort (else variant 4's
+ * rules apply); p2g_tiles_per_sm 4 or 6 (its register budget).
+ * pgmpm_create picks 5 for MLS solvers that use the bin sort, else 3 from
+ * 2^20 particles and 2 below; REF_COMPAT runs variant 2 for 2-5.
  * g2p_variant 0: tile-staged gather (g2p_tiles_per_sm blocks per SM);
  * 1: direct gather in sorted order; 2: direct gather in physical order.
  * Negative keeps a value. */

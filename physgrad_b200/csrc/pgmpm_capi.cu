@@ -105,12 +105,14 @@ int refresh_payload(pgmpm_solver s, cudaStream_t st) {
     return PGMPM_OK;
 }
 
-int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc) {
+int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc, StepKind kind) {
     if (s->N == 0) {  // nothing to move; keep the timing events consistent
         if (timed)
             for (int i = 0; i < 5; ++i) CK(cudaEventRecord(s->ev[i], st));
         return PGMPM_OK;
     }
+    if (kind != STEP_SPLIT && !(s->pf.physics == PHYS_MLS && s->tune.step_sort == 0))
+        return fail(PGMPM_ERR_STATE, "internal: fused step without the bin sort");
     View V = s->view_for(b);
     // P2G variant 1 builds its payload from the state's v and C
     V.write_vc = write_vc || s->pf.physics != PHYS_MLS || s->tune.p2g_variant == 1 ? 1 : 0;
@@ -146,30 +148,50 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, 
         CK(launch_mark(V, st));
     }
     if (timed) CK(cudaEventRecord(s->ev[1], st));
-    CK(launch_p2g(V, s->pf, s->tune, s->num_sms, st));
+    // a fused step's P2G was done by the previous step's G2P2G
+    if (kind == STEP_SPLIT || kind == STEP_FUSED_FIRST) CK(launch_p2g(V, s->pf, s->tune, s->num_sms, st));
     if (timed) CK(cudaEventRecord(s->ev[2], st));
     CK(launch_grid(V, s->pf, s->tune, s->num_sms, st));
     if (timed) CK(cudaEventRecord(s->ev[3], st));
-    CK(launch_g2p(V, s->pf, s->tune, s->num_sms, st));
+    if (kind == STEP_FUSED_FIRST || kind == STEP_FUSED) {
+        V.pay_out = nullptr;  // the payload stays in the SM; the buffer goes stale
+        CK(launch_g2p2g(V, s->pf, s->tune, s->num_sms, st));
+    } else {
+        CK(launch_g2p(V, s->pf, s->tune, s->num_sms, st));
+    }
     if (timed) CK(cudaEventRecord(s->ev[4], st));
     return PGMPM_OK;
+}
+
+StepKind step_kind(pgmpm_solver s, int k, int n, bool primed, bool drain) {
+    if (!s->fused()) return STEP_SPLIT;
+    const bool first = k == 0 && !primed;
+    if (drain && k + 1 == n) return first ? STEP_SPLIT : STEP_FUSED_LAST;
+    return first ? STEP_FUSED_FIRST : STEP_FUSED;
+}
+
+int unprime(pgmpm_solver s, cudaStream_t st) {
+    if (!s->primed) return PGMPM_OK;
+    s->primed = false;
+    CK(cudaMemsetAsync(s->grid_mp.p, 0, s->grid_mp.bytes, st));
+    return refresh_payload(s, st);
 }
 
 }  // namespace pgmpm
 
 namespace {
 
-// The step graph (mid = false) or the graph of a step that another step of
-// the same call follows (mid = true: v and C are not stored).
-int build_graph(pgmpm_solver s, bool mid) {
-    cudaGraph_t& graph = mid ? s->step_graph_mid : s->step_graph;
-    cudaGraphExec_t& exec = mid ? s->step_exec_mid : s->step_exec;
+// The step graph of one kind (mid = false: the call's last step; mid = true:
+// a step that another step of the same call follows, v and C not stored).
+int build_graph(pgmpm_solver s, StepKind kind, bool mid) {
+    cudaGraph_t& graph = s->step_graph[kind][mid ? 1 : 0];
+    cudaGraphExec_t& exec = s->step_exec[kind][mid ? 1 : 0];
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     exec = nullptr;
     graph = nullptr;
     CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
-    int rc = record_step(s, s->live_bufs(), s->cap_stream, false, !mid);
+    int rc = record_step(s, s->live_bufs(), s->cap_stream, false, !mid, kind);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
     if (rc != PGMPM_OK) {
@@ -185,11 +207,19 @@ int build_graph(pgmpm_solver s, bool mid) {
 }  // namespace
 
 namespace pgmpm {
+// Live steps.  With the fused kernel a call leaves the next step's P2G in
+// grid_mp (s->primed), so a following call continues without a P2G of its
+// own; anything that changes the state or its parameters unprimes first.
 int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
     if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    if (!s->fused()) {
+        int rc = unprime(s, st);
+        if (rc) return rc;
+    }
     for (int k = 0; k < n_steps; ++k) {
+        const StepKind kind = step_kind(s, k, n_steps, s->primed, false);
         if (s->profiling) {
-            int rc = record_step(s, s->live_bufs(), st, true);
+            int rc = record_step(s, s->live_bufs(), st, true, true, kind);
             if (rc) return rc;
             CK(cudaEventSynchronize(s->ev[4]));
             float a, b, c, d;
@@ -207,21 +237,22 @@ int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st) {
             s->met.particle_steps_per_s = s->met.average_step_ms > 0 ? s->N / (s->met.average_step_ms * 1e-3) : 0;
         } else if (s->use_graph) {
             const bool mid = k + 1 < n_steps;
-            if (!(mid ? s->step_exec_mid : s->step_exec)) {
-                int rc = build_graph(s, mid);
+            if (!s->step_exec[kind][mid ? 1 : 0]) {
+                int rc = build_graph(s, kind, mid);
                 if (rc) return rc;
             }
-            CK(cudaGraphLaunch(mid ? s->step_exec_mid : s->step_exec, st));
+            CK(cudaGraphLaunch(s->step_exec[kind][mid ? 1 : 0], st));
         } else {
-            int rc = record_step(s, s->live_bufs(), st, false, k + 1 == n_steps);
+            int rc = record_step(s, s->live_bufs(), st, false, k + 1 == n_steps, kind);
             if (rc) return rc;
         }
+        if (kind == STEP_FUSED_FIRST || kind == STEP_FUSED) s->primed = true;
         s->met.total_steps++;
     }
     return PGMPM_OK;
 }
 
-}  // namespace
+}  // namespace pgmpm
 
 // ============================================================== C-ABI
 extern "C" {
@@ -360,7 +391,7 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     // without it, two lanes per cell pays off when the occupied tiles
     // outnumber the resident blocks (many particles), one lane otherwise
     s->tune.p2g_variant = s->pf.physics != PHYS_MLS ? 2
-                          : s->tune.step_sort == 0  ? 4
+                          : s->tune.step_sort == 0  ? 5
                           : N >= (int64_t)1 << 20   ? 3
                                                     : 2;
     if (e == cudaSuccess && s->tune.step_sort == 0 && alloc_bin_sort(s) != PGMPM_OK) e = cudaErrorMemoryAllocation;
@@ -414,8 +445,13 @@ int pgmpm_set_materials(pgmpm_solver s, const pgmpm_material* materials, int32_t
     s->mats_h.assign(materials, materials + n_materials);
     s->ck_valid = false;  // a replay would run with the new table
     if (s->uploaded) {
-        // the payload holds the stress of the old material table
+        // the payload (and a pending fused P2G) hold the stress of the old
+        // material table
         CK(cudaDeviceSynchronize());
+        if (s->primed) {
+            s->primed = false;
+            CK(cudaMemsetAsync(s->grid_mp.p, 0, s->grid_mp.bytes, s->cap_stream));
+        }
         int rc = refresh_payload(s, s->cap_stream);
         if (rc) return rc;
         CK(cudaStreamSynchronize(s->cap_stream));
@@ -444,8 +480,12 @@ int pgmpm_set_scene_params(pgmpm_solver s, int32_t scene, float dt, const float*
     CK(cudaMemcpy(s->d_scenes.as<SceneDev>() + scene, &sd, sizeof(SceneDev), cudaMemcpyHostToDevice));
     s->ck_valid = false;  // a replay would run with the new dt / gravity
     if (s->uploaded && s->pf.physics == PHYS_MLS) {
-        // the payload holds -dt V0 D tau of the old dt
+        // the payload (and a pending fused P2G) hold -dt V0 D tau of the old dt
         CK(cudaDeviceSynchronize());
+        if (s->primed) {
+            s->primed = false;
+            CK(cudaMemsetAsync(s->grid_mp.p, 0, s->grid_mp.bytes, s->cap_stream));
+        }
         int rc = refresh_payload(s, s->cap_stream);
         if (rc) return rc;
         CK(cudaStreamSynchronize(s->cap_stream));
@@ -491,6 +531,10 @@ int pgmpm_upload(pgmpm_solver s, const float* x, const float* v, const float* C,
         return fail(PGMPM_ERR_ARG, "ptr_kind must be PGMPM_PTR_HOST or PGMPM_PTR_DEVICE");
     }
     if (mat && s->M == 1) dmat = nullptr;
+    if (s->primed) {  // the pending P2G is the old state's
+        s->primed = false;
+        CK(cudaMemsetAsync(s->grid_mp.p, 0, s->grid_mp.bytes, st));
+    }
     if (N > 0) {
         View V = s->view();
         // 1. identity pack (user order) to compute the keys
@@ -700,12 +744,16 @@ int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, int32_t g2p
 int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_variant, int32_t p2g_tiles_per_sm,
                               int32_t g2p_tiles_per_sm) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
-    if (p2g_variant > 4 || g2p_variant > 2 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
-        return fail(PGMPM_ERR_ARG, "p2g_variant 0..4, g2p_variant 0..2; blocks per SM at most 16");
+    if (p2g_variant > 5 || g2p_variant > 2 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
+        return fail(PGMPM_ERR_ARG, "p2g_variant 0..5, g2p_variant 0..2; blocks per SM at most 16");
+    if (p2g_variant == 5 && p2g_tiles_per_sm > 0 && p2g_tiles_per_sm != 4 && p2g_tiles_per_sm != 6)
+        return fail(PGMPM_ERR_ARG, "p2g_variant 5 runs 4 or 6 blocks per SM");
     if (p2g_variant >= 0) s->tune.p2g_variant = p2g_variant;
     if (g2p_variant >= 0) s->tune.g2p_variant = g2p_variant;
     if (p2g_tiles_per_sm > 0) {
-        if (s->tune.p2g_variant == 2)
+        if (s->tune.p2g_variant == 5)
+            s->tune.g2p2g_blocks_per_sm = p2g_tiles_per_sm;
+        else if (s->tune.p2g_variant == 2)
             s->tune.cell_blocks_per_sm = p2g_tiles_per_sm;
         else if (s->tune.p2g_variant >= 3)
             s->tune.pair_blocks_per_sm = std::min(p2g_tiles_per_sm, 5);
@@ -745,7 +793,8 @@ int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out) {
     s->met.graph_enabled = s->use_graph ? 1 : 0;
     s->met.p2g_variant = s->tune.p2g_variant;
     s->met.g2p_variant = s->tune.g2p_variant;
-    s->met.p2g_tiles_per_sm = s->tune.p2g_variant == 2   ? s->tune.cell_blocks_per_sm
+    s->met.p2g_tiles_per_sm = s->tune.p2g_variant == 5   ? s->tune.g2p2g_blocks_per_sm
+                              : s->tune.p2g_variant == 2 ? s->tune.cell_blocks_per_sm
                               : s->tune.p2g_variant >= 3 ? s->tune.pair_blocks_per_sm
                                                          : s->tune.tile_blocks_per_sm;
     s->met.g2p_tiles_per_sm = s->tune.g2p_tiles_per_sm;
@@ -760,6 +809,8 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
     DeviceGuard dg(s->device);
     cudaStream_t st = ST(stream);
     if (reps < 1) reps = 3;
+    int rc0 = unprime(s, st);  // the trials run split steps from the payload
+    if (rc0) return rc0;
     // save state (planes + keys) and restore after the trials
     DevBuf save;
     const size_t qb = sizeof(float4) * 6 * (size_t)s->N;
@@ -836,6 +887,11 @@ int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
             best.g2p_block = t.g2p_block;
             best.g2p_tiles_per_sm = t.g2p_tiles_per_sm;
         }
+    }
+    // the fused path runs variant 4's P2G for the first step of a chain
+    if (keep.p2g_variant == 5 && best.p2g_variant == 4) {
+        best.p2g_variant = 5;
+        best.g2p2g_blocks_per_sm = keep.g2p2g_blocks_per_sm;
     }
     // restore: state, keys, clean accumulator grid
     CK(cudaMemcpyAsync(s->q.p, save.p, qb, cudaMemcpyDeviceToDevice, st));

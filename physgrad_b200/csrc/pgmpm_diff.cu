@@ -130,10 +130,13 @@ int tape_graph(pgmpm_solver s, int kind, int len, Body&& body) {
     return PGMPM_OK;
 }
 
-// Forward of slots 0..len-1 of tape set t (state 0 and its payload in place).
+// Forward of slots 0..len-1 of tape set t (state 0 and its payload in place,
+// grid_mp clear).  With the fused kernel each slot's G2P2G does the next
+// slot's P2G; the last slot runs the split G2P, so nothing is left pending
+// in grid_mp and the payload buffer holds the final state's payload.
 int record_tape_forward(pgmpm_solver s, int len, cudaStream_t st, int t = 0) {
     for (int j = 0; j < len; ++j) {
-        int rc = record_step(s, tape_bufs(s, j, t), st, false);
+        int rc = record_step(s, tape_bufs(s, j, t), st, false, true, step_kind(s, j, len, false, true));
         if (rc) return rc;
     }
     return PGMPM_OK;
@@ -247,6 +250,8 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     if (rc) return rc;
     s->ck_valid = false;
     s->tape_has_last = false;
+    rc = unprime(s, st);  // checkpoints and replays start from the state alone
+    if (rc) return rc;
     for (int seg = 0; seg < nseg; ++seg) {
         CK(cudaMemcpyAsync(s->ck_q.as<float4>() + 6 * N * seg, s->q.p, sizeof(float4) * 6 * N,
                            cudaMemcpyDeviceToDevice, st));
@@ -260,6 +265,9 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
         }
         // last segment: run it in the tape slots, so that the backward does
         // not replay it, then hand the final state back to the live buffers
+        // (the tape starts from the state and its payload, with grid_mp clear)
+        rc = unprime(s, st);
+        if (rc) return rc;
         CK(cudaMemcpyAsync(s->tape_q.p, s->q.p, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_keys.p, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_pay.p, s->pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
@@ -299,6 +307,10 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
     const size_t Nz = (size_t)std::max<int64_t>(N, 1);
     const int M = s->M;
     int rc = ensure_tape(s, s->ck_every);
+    if (rc) return rc;
+    // the replays accumulate their P2G in grid_mp: drop a pending fused P2G
+    // of the live state (recomputed by its next step)
+    rc = unprime(s, st);
     if (rc) return rc;
     CK(s->adj_g.ensure(sizeof(float4) * 6 * Nz));
     CK(s->adj_grid_gv.ensure(sizeof(float4) * nodes_of(s)));

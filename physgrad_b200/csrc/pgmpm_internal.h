@@ -76,6 +76,19 @@ struct Tuning {
     int cell_blocks_per_sm = 6;  // persistent P2G thread-per-cell kernel (variant 2): blocks per SM
     int pair_blocks_per_sm = 5;  // persistent P2G two-threads-per-cell kernel (variant 3): blocks per SM
     int step_sort = 0;           // per-step sort: 0 = bin sort (counting sorts by tile, then cell), 1 = radix sort
+    int g2p2g_blocks_per_sm = 4; // fused kernel (P2G variant 5): 4 (255 registers) or 6 (168, some spilled)
+};
+// P2G variant 5 = variant 4's P2G, fused with the previous step's G2P when
+// steps follow one another (launch_g2p2g).
+
+// What one recorded step launches.  MLS with the fused G2P -> P2G kernel
+// (P2G variant 5) chains steps: a step's G2P2G does the next step's P2G.
+enum StepKind {
+    STEP_SPLIT = 0,    // sort, P2G, grid update, G2P (which writes the next payload)
+    STEP_FUSED_FIRST,  // sort, P2G, grid update, G2P2G
+    STEP_FUSED,        // sort, grid update, G2P2G (P2G done by the previous step's G2P2G)
+    STEP_FUSED_LAST,   // sort, grid update, G2P (nothing left pending in grid_mp)
+    STEP_KINDS
 };
 
 // pgmpm_sort.cu
@@ -125,6 +138,10 @@ cudaError_t launch_mark(const View& V, cudaStream_t st);
 cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
+// Fused G2P of this step and P2G of the next (MLS with the bin sort's cell
+// table): writes the new state and keys and accumulates the next step's
+// (m, p) into V.grid_mp; takes work from the G2P cursor.
+cudaError_t launch_g2p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st);
 cudaError_t launch_pack(const View& V, const float* x, const float* v, const float* C, const float* F,
                         const float* m, const float* V0, const int32_t* mat, const uint32_t* order,
                         uint32_t* user_of_phys, uint32_t* phys_of_user, float2* mV_out, int32_t* mat_out,

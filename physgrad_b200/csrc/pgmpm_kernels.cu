@@ -1333,6 +1333,71 @@ __global__ void k_grid(View V) {
 }
 
 // ------------------------------------------------------------------- G2P
+// APIC sums of one MLS particle over its 27 stencil nodes: nv = sum w v and
+// S = sum w v o^T (o the integer stencil offset, so B = sum w v d^T =
+// dx (S - nv f^T)).  row(j, k, g0, g1, g2) fetches the (v, m) float4 of the
+// three nodes (0..2, j, k) of the stencil.
+template <class Row>
+__device__ __forceinline__ void mls_gather(const Stencil& st, const Row& row, float nv[3], float S[9]) {
+    nv[0] = nv[1] = nv[2] = 0.f;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) S[a] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float wjk = st.w[1][j] * st.w[2][k];
+            float4 g0, g1, g2;
+            row(j, k, g0, g1, g2);
+            const float w0 = st.w[0][0] * wjk, w1 = st.w[0][1] * wjk, w2 = st.w[0][2] * wjk;
+            const float r1x = w1 * g1.x, r1y = w1 * g1.y, r1z = w1 * g1.z;
+            const float r2x = w2 * g2.x, r2y = w2 * g2.y, r2z = w2 * g2.z;
+            const float sx = w0 * g0.x + r1x + r2x, sy = w0 * g0.y + r1y + r2y, sz = w0 * g0.z + r1z + r2z;
+            nv[0] += sx; nv[1] += sy; nv[2] += sz;
+            S[0] += r1x + 2.f * r2x; S[3] += r1y + 2.f * r2y; S[6] += r1z + 2.f * r2z;
+            if (j) {
+                const float fj = (float)j;
+                S[1] += fj * sx; S[4] += fj * sy; S[7] += fj * sz;
+            }
+            if (k) {
+                const float fk = (float)k;
+                S[2] += fk * sx; S[5] += fk * sy; S[8] += fk * sz;
+            }
+        }
+    }
+}
+
+// APIC matrix C = D B = D dx (S - nv f^T) from the gathered sums.
+__device__ __forceinline__ void mls_affine(const SceneDev& sc, const Stencil& st, const float nv[3], const float S[9],
+                                           float C[9]) {
+    const float dx = sc.dx;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) C[3 * a + b] = sc.D * dx * (S[3 * a + b] - nv[a] * st.f[b]);
+}
+
+// F <- (I + dt C) F (a fluid's F reset to its volumetric part, cbrt(J) I)
+// and x <- x + dt v.
+template <bool MULTI, bool FLUID>
+__device__ __forceinline__ void mls_advance(const View& V, const SceneDev& sc, uint32_t p, const float nv[3],
+                                            const float C[9], const float F[9], float x[3], float Fn[9]) {
+    float M[9];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) M[a] = sc.dt * C[a] + (a % 4 == 0 ? 1.f : 0.f);
+    m3_mul(M, F, Fn);
+    if (FLUID) {
+        const int mid = MULTI ? V.mat[p] : 0;
+        if (V.mats[mid].model == MODEL_EOS) {
+            const float c = cbrtf(m3_det(Fn));
+#pragma unroll
+            for (int a = 0; a < 9; ++a) Fn[a] = (a % 4 == 0) ? c : 0.f;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) x[a] = x[a] + sc.dt * nv[a];
+}
+
 // Per-particle G2P update shared by both G2P variants; `fetch(i, j, k)`
 // returns the (v, m) float4 of grid node (i, j, k) of scene sc.
 // PLASTIC: the payload's stress includes the von Mises cap (launched when an
@@ -1358,44 +1423,15 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
             Y[a] = (gj >> 2) * (sc.nt[0] << 6) + ((gj & 3) << 2);
             Z[a] = (gk >> 2) * ((sc.nt[0] * sc.nt[1]) << 6) + ((gk & 3) << 4) + (sc.nt_base << 6);
         }
-        // S = sum w v o^T (o = integer stencil offset), nv = sum w v;
-        // B = sum w v d^T = dx (S - nv f^T)
-        float nv[3] = {0.f, 0.f, 0.f};
-        float S[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const float wjk = st.w[1][j] * st.w[2][k];
-                const int row = Y[j] + Z[k];
-                const float4 g0 = fetch(st.s[0], st.s[1] + j, st.s[2] + k, row + X[0]);
-                const float4 g1 = fetch(st.s[0] + 1, st.s[1] + j, st.s[2] + k, row + X[1]);
-                const float4 g2 = fetch(st.s[0] + 2, st.s[1] + j, st.s[2] + k, row + X[2]);
-                const float w0 = st.w[0][0] * wjk, w1 = st.w[0][1] * wjk, w2 = st.w[0][2] * wjk;
-                const float r1x = w1 * g1.x, r1y = w1 * g1.y, r1z = w1 * g1.z;
-                const float r2x = w2 * g2.x, r2y = w2 * g2.y, r2z = w2 * g2.z;
-                const float sx = w0 * g0.x + r1x + r2x, sy = w0 * g0.y + r1y + r2y, sz = w0 * g0.z + r1z + r2z;
-                nv[0] += sx; nv[1] += sy; nv[2] += sz;
-                S[0] += r1x + 2.f * r2x; S[3] += r1y + 2.f * r2y; S[6] += r1z + 2.f * r2z;
-                if (j) {
-                    const float fj = (float)j;
-                    S[1] += fj * sx; S[4] += fj * sy; S[7] += fj * sz;
-                }
-                if (k) {
-                    const float fk = (float)k;
-                    S[2] += fk * sx; S[5] += fk * sy; S[8] += fk * sz;
-                }
-            }
-        }
-        const float dx = sc.dx;
-        float C[9], Fn[9], M[9];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                C[3 * a + b] = sc.D * dx * (S[3 * a + b] - nv[a] * st.f[b]);
-                M[3 * a + b] = sc.dt * C[3 * a + b] + (a == b ? 1.f : 0.f);
-            }
+        float nv[3], S[9];
+        mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
+            const int row = Y[j] + Z[k];
+            g0 = fetch(st.s[0], st.s[1] + j, st.s[2] + k, row + X[0]);
+            g1 = fetch(st.s[0] + 1, st.s[1] + j, st.s[2] + k, row + X[1]);
+            g2 = fetch(st.s[0] + 2, st.s[1] + j, st.s[2] + k, row + X[2]);
+        }, nv, S);
+        float C[9], Fn[9];
+        mls_affine(sc, st, nv, S, C);
         float4* qo = V.q_out;
         if (V.write_vc) {  // else the next step of the call reads v, C from the payload only
             float4 o3, o4, o5;
@@ -1404,17 +1440,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
             qo[4 * N + p] = o4;
             qo[5 * N + p] = o5;
         }
-        m3_mul(M, F, Fn);
-        if (FLUID) {
-            const int mid = MULTI ? V.mat[p] : 0;
-            if (V.mats[mid].model == MODEL_EOS) {
-                const float c = cbrtf(m3_det(Fn));
-#pragma unroll
-                for (int a = 0; a < 9; ++a) Fn[a] = (a % 4 == 0) ? c : 0.f;
-            }
-        }
-#pragma unroll
-        for (int a = 0; a < 3; ++a) x[a] = x[a] + sc.dt * nv[a];
+        mls_advance<MULTI, FLUID>(V, sc, p, nv, C, F, x, Fn);
         float4 o0, o1, o2;
         pack_xF(x, Fn, o0, o1, o2);
         qo[p] = o0;
@@ -1569,6 +1595,300 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(View V) {
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
 
+// ------------------------------------------ fused G2P -> P2G (MLS, variant 5)
+// One pass over the particles that does the G2P of this step and the P2G of
+// the next: the P2G payload never leaves the SM (the split path writes it to
+// HBM in G2P and reads it back in P2G).  Work items are the occupied cell
+// tiles of this step's sort (or slices of them when tiles are few), largest
+// first, taken from the G2P work cursor (P2G's is left for the reverse
+// scatter).  Per item:
+//   * the tile's 6^3 node velocities are staged in shared memory: every
+//     particle of the tile gathers its 27 nodes from there;
+//   * the item's sorted particles are cut into two warp halves at the cell
+//     boundary nearest the midpoint and each lane walks an equal run of its
+//     half (one lane per run: 27 nodes x 4 channels of register
+//     accumulators);
+//   * per particle: G2P (v, C, F, x), the new state stored, the next cell
+//     key, the stress and the payload of the new state, accumulated into the
+//     run's sums.  Particles move less than a cell per step, so a particle's
+//     new cell is nearly always its cell of this step's sort: the run's sums
+//     stay one cell's sums.  A particle that changed cell adds its 27 nodes
+//     to the grid with vector atomics instead;
+//   * a run that passes a cell's last particle stores the cell's sums (one
+//     writer per cell); runs that end inside a cell are merged by a
+//     segmented scan over the warp's lanes; each of the 6^3 nodes the tile
+//     touches then sums its <= 27 cells and gets one vector atomic
+//     (red.global.add.v4.f32) into grid_mp, which the next grid update
+//     reads.
+// grid_mp must hold no other contributions on entry (the grid update of
+// this step cleared it).  Needs the bin sort's cell table.
+// MINB: resident blocks per SM the register budget is cut for (4: up to 255
+// registers, no spills; 6: 168 registers, some spilled).
+constexpr int G2_T = 64;
+
+template <bool MULTI, bool FLUID, bool PLASTIC, int MINB>
+__global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
+    __shared__ float4 box[TILE_NODES];           // grid_v of the tile's node block
+    __shared__ float4 T4[27 * 64];                // [offset o][cell]: (m, p) of cell's node o
+    __shared__ uint32_t s_end[G2_T / 32][64];     // per warp: end of each cell's range in the item
+    __shared__ uint32_t s_work;
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int64_t N = V.N;
+    uint32_t flags = 0;
+    uint32_t* const wend = s_end[wp];
+    const uint32_t ntiles = V.counters[CNT_CTILES];
+    // slices of a tile's particles when tiles are few (each slice flushes the
+    // tile's whole node block)
+    const uint32_t S = ntiles ? min(8u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
+    const uint32_t nwork = ntiles * S;
+    const bool early = nwork >= 2u * gridDim.x;
+    uint32_t next_work = 0;
+    if (threadIdx.x == 0) s_work = atomicAdd(&V.counters[CNT_G2P_CURSOR], 1u);
+    for (;;) {
+        __syncthreads();
+        const uint32_t w = s_work;
+        if (w >= nwork) break;
+        if (early && threadIdx.x == 0) next_work = atomicAdd(&V.counters[CNT_G2P_CURSOR], 1u);
+        const uint32_t wt = w / S, slice = w - wt * S;
+        const uint32_t ct = V.ptile_list ? V.ptile_list[wt] : V.ctile_list[wt];
+        const uint2 rg = V.ctile_range[ct];
+        const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
+        const SceneDev& sc = scene_ref(V, s);
+        const int lt = (int)ct - sc.ct_base;
+        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
+                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        for (int n = threadIdx.x; n < TILE_NODES; n += G2_T) {
+            const int gi = ox + n % TN, gj = oy + (n / TN) % TN, gk = oz0 + n / (TN * TN);
+            box[n] = (gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2]) ? V.grid_v[node_index(sc, gi, gj, gk)]
+                                                                    : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        // the item's particles [lo, hi) and its cells' ranges clamped to them
+        // (lane holds cells lane and lane + 32)
+        const uint32_t P = rg.y > rg.x ? rg.y - rg.x : 0u;
+        const uint32_t lo = rg.x + (uint32_t)(((uint64_t)P * slice) / S);
+        const uint32_t hi = rg.x + (uint32_t)(((uint64_t)P * (slice + 1)) / S);
+        const uint2 r0 = V.cell_range[(size_t)ct * 64 + lane], r1 = V.cell_range[(size_t)ct * 64 + 32 + lane];
+        const uint32_t s0 = min(max(r0.x, lo), hi), s1 = min(max(r1.x, lo), hi);
+        const uint32_t e0 = min(max(r0.y, lo), hi), e1 = min(max(r1.y, lo), hi);
+        if ((lane == 0 && s0 != lo) || (lane == 31 && e1 != hi)) flags |= FLAG_TILE_RANGE;
+        wend[lane] = e0;
+        wend[lane + 32] = e1;
+        // warp half [b0, b1): split at the cell start nearest the midpoint
+        uint32_t mid;
+        {
+            const uint32_t t = lo + ((hi - lo) >> 1);
+            const uint32_t a = __reduce_max_sync(FULL, max(s0 <= t ? s0 : lo, s1 <= t ? s1 : lo));
+            const uint32_t b = __reduce_min_sync(FULL, min(s0 >= t ? s0 : hi, s1 >= t ? s1 : hi));
+            mid = t - a <= b - t ? a : b;
+        }
+        const uint32_t b0 = wp == 0 ? lo : mid, b1 = wp == 0 ? mid : hi;
+        const uint32_t len = (b1 - b0 + 31u) >> 5;
+        const uint32_t i0 = min(b0 + (uint32_t)lane * len, b1), i1 = min(i0 + len, b1);
+        __syncwarp();
+        // cells without particles in the item get a zero entry (warp wp:
+        // cells 32 wp .. 32 wp + 31)
+        {
+            const int zc = 32 * wp + lane;
+            const uint32_t zs = zc == 0 ? lo : wend[zc - 1];
+            if (wend[zc] == zs)
+                for (int o = 0; o < 27; ++o) T4[o * 64 + zc] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();  // the node block is staged
+        float acc[27][4];
+#pragma unroll
+        for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = acc[o][3] = 0.f;
+        // the cell of particle i0: the first cell whose range ends after it
+        uint32_t c = 0, cend = 0;
+        if (i0 < i1) {
+            uint32_t l = 0, r = 63;
+            while (l < r) {
+                const uint32_t m = (l + r) >> 1;
+                if (wend[m] > i0) r = m; else l = m + 1;
+            }
+            c = l;
+            cend = wend[c];
+        }
+        uint32_t pn = i0 < i1 ? V.order[i0] : 0u;
+        for (uint32_t i = i0; i < i1; ++i) {
+            const uint32_t p = pn;
+            if (i + 1 < i1) pn = V.order[i + 1];
+            if (i == cend) {
+                // the run passed the last particle of cell c: its sums are final
+#pragma unroll
+                for (int o = 0; o < 27; ++o) {
+                    T4[o * 64 + c] = make_float4(acc[o][0], acc[o][1], acc[o][2], acc[o][3]);
+                    acc[o][0] = acc[o][1] = acc[o][2] = acc[o][3] = 0.f;
+                }
+                while (c < 63) {  // next cell with particles (c stays a cell index)
+                    ++c;
+                    if (wend[c] > i) break;
+                }
+                cend = wend[c];
+            }
+            if (p >= (uint32_t)N) {
+                flags |= FLAG_TILE_RANGE;
+                continue;
+            }
+            // ---- G2P of this step
+            float x[3], F[9];
+            unpack_xF(V.q[p], V.q[N + p], V.q[2 * N + p], x, F);
+            Stencil st;
+            make_stencil<PHYS_MLS>(sc, x, st, flags);
+            const int lx = st.s[0] - ox, ly = st.s[1] - oy, lz = st.s[2] - oz0;
+            const bool in_tile = (unsigned)lx <= 3u && (unsigned)ly <= 3u && (unsigned)lz <= 3u;
+            // the particle's stencil origin is the run's cell (its sorted key)
+            const bool own = in_tile && (uint32_t)(lx + 4 * ly + 16 * lz) == c;
+            if (!own) flags |= FLAG_TILE_RANGE;
+            float nv[3], Sg[9];
+            if (in_tile) {
+                const int base = lx + TN * (ly + TN * lz);
+                mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
+                    const float4* r = &box[base + TN * (j + TN * k)];
+                    g0 = r[0];
+                    g1 = r[1];
+                    g2 = r[2];
+                }, nv, Sg);
+            } else {
+                // not a particle of this tile's cells (the sort said otherwise):
+                // gather from the grid (reported above)
+                mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
+                    g0 = __ldg(&V.grid_v[node_index(sc, st.s[0], st.s[1] + j, st.s[2] + k)]);
+                    g1 = __ldg(&V.grid_v[node_index(sc, st.s[0] + 1, st.s[1] + j, st.s[2] + k)]);
+                    g2 = __ldg(&V.grid_v[node_index(sc, st.s[0] + 2, st.s[1] + j, st.s[2] + k)]);
+                }, nv, Sg);
+            }
+            float C[9], Fn[9];
+            mls_affine(sc, st, nv, Sg, C);
+            float4* qo = V.q_out;
+            if (V.write_vc) {
+                float4 o3, o4, o5;
+                pack_vC(nv, C, o3, o4, o5);
+                qo[3 * N + p] = o3;
+                qo[4 * N + p] = o4;
+                qo[5 * N + p] = o5;
+            }
+            mls_advance<MULTI, FLUID>(V, sc, p, nv, C, F, x, Fn);
+            {
+                float4 o0, o1, o2;
+                pack_xF(x, Fn, o0, o1, o2);
+                qo[p] = o0;
+                qo[N + p] = o1;
+                qo[2 * N + p] = o2;
+            }
+            // ---- next cell key and the payload of the new state
+            int so[3];
+            float fn[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                float u;
+                so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS_MLS, u, flags);
+                fn[a] = fminf(fmaxf(__fsub_rn(u, (float)so[a]), 0.5f), 1.5f);
+            }
+            V.keys[p] = cell_key(sc, so);
+            const float2 mv = V.mV[p];
+            float4 a0, a1, a2, a3;
+            mls_payload<PLASTIC>(sc, V.mats[MULTI ? V.mat[p] : 0], fn, Fn, nv, C, mv.x, mv.y, a0, a1, a2, a3);
+            float m, b[3], Ad[9], f[3];
+            unpack_payload(a0, a1, a2, a3, m, b, Ad, f);
+            float wt[3][3];
+            mls_weights(f[0], wt[0]);
+            mls_weights(f[1], wt[1]);
+            mls_weights(f[2], wt[2]);
+            // ---- P2G of the next step: node o gets w_o (m, b + Ad o)
+            if (own && so[0] == st.s[0] && so[1] == st.s[1] && so[2] == st.s[2]) {
+#pragma unroll
+                for (int zz = 0; zz < 3; ++zz) {
+                    const float bz0 = b[0] + Ad[2] * (float)zz, bz1 = b[1] + Ad[5] * (float)zz,
+                                bz2 = b[2] + Ad[8] * (float)zz;
+#pragma unroll
+                    for (int yy = 0; yy < 3; ++yy) {
+                        const float wyz = wt[1][yy] * wt[2][zz];
+                        float v0 = bz0 + Ad[1] * (float)yy, v1 = bz1 + Ad[4] * (float)yy,
+                              v2 = bz2 + Ad[7] * (float)yy;
+#pragma unroll
+                        for (int xx = 0; xx < 3; ++xx) {
+                            const int o = xx + 3 * yy + 9 * zz;
+                            const float wgt = wt[0][xx] * wyz;
+                            acc[o][0] += wgt * m;
+                            acc[o][1] += wgt * v0;
+                            acc[o][2] += wgt * v1;
+                            acc[o][3] += wgt * v2;
+                            v0 += Ad[0];
+                            v1 += Ad[3];
+                            v2 += Ad[6];
+                        }
+                    }
+                }
+            } else {
+                // the particle changed cell: its nodes are not the run's cell's
+                // (nor are they after an inconsistent sort, reported above)
+#pragma unroll
+                for (int zz = 0; zz < 3; ++zz)
+#pragma unroll
+                    for (int yy = 0; yy < 3; ++yy)
+#pragma unroll
+                        for (int xx = 0; xx < 3; ++xx) {
+                            const float wgt = wt[0][xx] * wt[1][yy] * wt[2][zz];
+                            const float4 add =
+                                make_float4(wgt * m, wgt * (b[0] + Ad[0] * xx + Ad[1] * yy + Ad[2] * zz),
+                                            wgt * (b[1] + Ad[3] * xx + Ad[4] * yy + Ad[5] * zz),
+                                            wgt * (b[2] + Ad[6] * xx + Ad[7] * yy + Ad[8] * zz));
+                            atomicAdd(&V.grid_mp[node_index(sc, so[0] + xx, so[1] + yy, so[2] + zz)], add);
+                        }
+            }
+        }
+        // a run that ends where its cell ends owns that cell; otherwise the
+        // cell's owner is a later lane of this warp and the sum is partial
+        const bool open = i0 < i1 && i1 != cend;
+        if (i0 < i1 && !open)
+#pragma unroll
+            for (int o = 0; o < 27; ++o) T4[o * 64 + c] = make_float4(acc[o][0], acc[o][1], acc[o][2], acc[o][3]);
+        __syncwarp();
+        // segmented inclusive scan of the partial sums over consecutive lanes
+        // of the same cell; the last lane of a segment then holds its total
+        const uint32_t key = open ? c : FULL;
+        const uint32_t pkey = __shfl_up_sync(FULL, key, 1), nkey = __shfl_down_sync(FULL, key, 1);
+        const bool head = open && (lane == 0 || pkey != key);
+        const uint32_t heads = __ballot_sync(FULL, head);
+        const int dist = open ? lane - (31 - __clz(heads & (FULL >> (31 - lane)))) : 0;
+        const int maxd = __reduce_max_sync(FULL, dist);
+        for (int d = 1; d <= maxd; d <<= 1) {
+            const bool take = dist >= d;
+#pragma unroll
+            for (int o = 0; o < 27; ++o) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float a = __shfl_up_sync(FULL, acc[o][k], d);
+                    if (take) acc[o][k] += a;
+                }
+            }
+        }
+        if (open && (lane == 31 || nkey != key)) {
+#pragma unroll
+            for (int o = 0; o < 27; ++o) {
+                float4 t = T4[o * 64 + c];
+                t.x += acc[o][0];
+                t.y += acc[o][1];
+                t.z += acc[o][2];
+                t.w += acc[o][3];
+                T4[o * 64 + c] = t;
+            }
+        }
+        __syncthreads();
+        for (int n = threadIdx.x; n < TILE_NODES; n += G2_T) {
+            const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
+            const float4 a4 = tile_node_sum(T4, nx, ny, nz);
+            const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
+            if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
+                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_work = early ? next_work : atomicAdd(&V.counters[CNT_G2P_CURSOR], 1u);
+    }
+    if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
 // ------------------------------------------------------------ pack / unpack
 __global__ void k_pack(View V, const float* __restrict__ x, const float* __restrict__ v,
                        const float* __restrict__ C, const float* __restrict__ F, const float* __restrict__ m,
@@ -1699,7 +2019,7 @@ cudaError_t launch_adj_scatter(const View& V, const AdjView& A, const PhysFlags&
                                cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
     if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
-    if (t.p2g_variant == 4 && V.cell_range) {  // balanced runs over the sort's cell table
+    if (t.p2g_variant >= 4 && V.cell_range) {  // balanced runs over the sort's cell table
         const int nb = num_sms * 6;
         if (pf.multi_mat) {
             if (pf.has_fluid)
@@ -1748,13 +2068,13 @@ cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int 
     if (V.N == 0) return cudaSuccess;
     if (t.p2g_variant >= 3 && pf.physics == PHYS_MLS) {
         if (!V.pay) return cudaErrorInvalidValue;
-        if (t.p2g_variant == 4 && V.cell_range)  // without the sort's cell table: variant 3
+        if (t.p2g_variant >= 4 && V.cell_range)  // without the sort's cell table: variant 3
             k_p2g_runs<<<num_sms * t.pair_blocks_per_sm, P2GR_T, 0, st>>>(V);
         else
             k_p2g_pairs<<<num_sms * t.pair_blocks_per_sm, P2GP_T, 0, st>>>(V);
         return cudaGetLastError();
     }
-    if (t.p2g_variant >= 2) {  // REF physics: variants 3 and 4 run variant 2
+    if (t.p2g_variant >= 2) {  // REF physics: variants 3 to 5 run variant 2
         const int nb = num_sms * t.cell_blocks_per_sm;
         const AdjView none{};
         if (pf.physics == PHYS_MLS) {
@@ -1841,6 +2161,35 @@ cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int 
         else
             PGMPM_G2P_DISPATCH(k_g2p_phys, nb, t.g2p_block);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g2p2g(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
+    if (V.N == 0) return cudaSuccess;
+    if (pf.physics != PHYS_MLS || !V.cell_range) return cudaErrorNotSupported;
+    const int minb = t.g2p2g_blocks_per_sm == 6 ? 6 : 4;
+    const int nb = num_sms * minb;
+#define PGMPM_G2P2G(M_, F_, P_)                                          \
+    do {                                                                 \
+        if (minb == 6)                                                   \
+            k_g2p2g<M_, F_, P_, 6><<<nb, G2_T, 0, st>>>(V);              \
+        else                                                             \
+            k_g2p2g<M_, F_, P_, 4><<<nb, G2_T, 0, st>>>(V);              \
+    } while (0)
+    if (pf.multi_mat) {
+        if (pf.has_fluid) {
+            if (pf.has_plastic) PGMPM_G2P2G(true, true, true); else PGMPM_G2P2G(true, true, false);
+        } else {
+            if (pf.has_plastic) PGMPM_G2P2G(true, false, true); else PGMPM_G2P2G(true, false, false);
+        }
+    } else {
+        if (pf.has_fluid) {
+            if (pf.has_plastic) PGMPM_G2P2G(false, true, true); else PGMPM_G2P2G(false, true, false);
+        } else {
+            if (pf.has_plastic) PGMPM_G2P2G(false, false, true); else PGMPM_G2P2G(false, false, false);
+        }
+    }
+#undef PGMPM_G2P2G
     return cudaGetLastError();
 }
 

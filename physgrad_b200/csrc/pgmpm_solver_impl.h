@@ -118,12 +118,16 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf ptile_list, tile_rank;  // largest-first occupied tile list (bin sort)
     uint32_t* h_counters = nullptr;  // pinned
 
-    // graph
+    // fused G2P -> P2G (p2g_variant 5): true while grid_mp holds the P2G of
+    // the live state, done by the last step's G2P2G (the payload buffer is
+    // then stale).  Cleared by pgmpm::unprime.
+    bool primed = false;
+
+    // graphs, one per step kind and [0] the call's last step / [1] a step
+    // that another step of the same call follows (v, C not stored)
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t step_exec = nullptr;      // one step
-    cudaGraph_t step_graph = nullptr;
-    cudaGraphExec_t step_exec_mid = nullptr;  // one step followed by another (v, C not stored)
-    cudaGraph_t step_graph_mid = nullptr;
+    cudaGraphExec_t step_exec[pgmpm::STEP_KINDS][2] = {};
+    cudaGraph_t step_graph[pgmpm::STEP_KINDS][2] = {};
     cudaEvent_t ev[6] = {};
 
     // metrics
@@ -220,13 +224,19 @@ struct pgmpm_solver_s {
     }
 
     void drop_graph() {
-        if (step_exec) cudaGraphExecDestroy(step_exec);
-        if (step_graph) cudaGraphDestroy(step_graph);
-        if (step_exec_mid) cudaGraphExecDestroy(step_exec_mid);
-        if (step_graph_mid) cudaGraphDestroy(step_graph_mid);
-        step_exec = step_exec_mid = nullptr;
-        step_graph = step_graph_mid = nullptr;
+        for (int k = 0; k < pgmpm::STEP_KINDS; ++k)
+            for (int m = 0; m < 2; ++m) {
+                if (step_exec[k][m]) cudaGraphExecDestroy(step_exec[k][m]);
+                if (step_graph[k][m]) cudaGraphDestroy(step_graph[k][m]);
+                step_exec[k][m] = nullptr;
+                step_graph[k][m] = nullptr;
+            }
         drop_tape_graphs();
+    }
+
+    // the live steps run the fused G2P -> P2G kernel
+    bool fused() const {
+        return pf.physics == pgmpm::PHYS_MLS && tune.p2g_variant == 5 && tune.step_sort == 0 && N > 0;
     }
 
     ~pgmpm_solver_s() {
@@ -251,11 +261,20 @@ namespace pgmpm {
 int refresh_payload(pgmpm_solver s, cudaStream_t st);
 // Allocate the bin sort's buffers (8 bytes per cell, counters cleared).
 int alloc_bin_sort(pgmpm_solver s);
-// Enqueue one step on `st` using buffers `b` (events ev[0..4] when timed).
-// write_vc = false lets an MLS step leave v and C (state planes 3-5) unwritten
-// when the next step follows in the same call: that step reads them only
-// through the payload, and the call's last step writes them.
-int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc = true);
+// Enqueue one step of kind `kind` on `st` using buffers `b` (events
+// ev[0..4] when timed).  write_vc = false lets an MLS step leave v and C
+// (state planes 3-5) unwritten when the next step follows in the same call:
+// that step reads them only through the payload (or the fused kernel does
+// not read them), and the call's last step writes them.
+int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc = true,
+                StepKind kind = STEP_SPLIT);
+// The kind of step k of n consecutive steps that start from a state whose
+// P2G is (primed) or is not already in grid_mp; drain: the last step leaves
+// nothing pending (G2P instead of G2P2G).
+StepKind step_kind(pgmpm_solver s, int k, int n, bool primed, bool drain);
+// Drops the pending P2G of the fused path (grid_mp cleared, payload
+// recomputed from the state), so that the next step starts with its own P2G.
+int unprime(pgmpm_solver s, cudaStream_t st);
 // Run n steps of the live state (graph, eager or profiled).
 int run_steps(pgmpm_solver s, int n_steps, cudaStream_t st);
 }  // namespace pgmpm

@@ -261,7 +261,7 @@ def test_mls_grid_download_matches_oracle(gpu, oracle):
 
 
 # --------------------------------------------------------- batching / misc
-@pytest.mark.parametrize("p2g_variant", [2, 3, 4])
+@pytest.mark.parametrize("p2g_variant", [2, 3, 4, 5])
 def test_batched_scenes_equal_single_scenes(gpu, p2g_variant):
     """One batched solver over scenes of uneven sizes and grids gives each
     scene's single-scene result (the per-cell and balanced-run P2G kernels)."""
@@ -286,7 +286,7 @@ def test_batched_scenes_equal_single_scenes(gpu, p2g_variant):
         off += c
 
 
-@pytest.mark.parametrize("p2g_variant,g2p_variant", [(0, 0), (1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (2, 2), (0, 2), (3, 2), (3, 0), (4, 2), (4, 0)])
+@pytest.mark.parametrize("p2g_variant,g2p_variant", [(0, 0), (1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (2, 2), (0, 2), (3, 2), (3, 0), (4, 2), (4, 0), (5, 2)])
 @pytest.mark.parametrize("physics", [0, 1])
 def test_kernel_variants_agree(gpu, oracle, p2g_variant, g2p_variant, physics):
     """Every P2G/G2P variant matches the checkers (MLS: FP64 oracle; REF:
@@ -492,7 +492,7 @@ def test_autotune_restores_state(gpu):
     after = sim.download()
     for k in ("x", "v", "C", "F"):
         assert np.array_equal(before[k], after[k])
-    assert best["p2g_variant"] in (0, 1, 2, 3, 4) and best["g2p_variant"] in (0, 1, 2)
+    assert best["p2g_variant"] in (0, 1, 2, 3, 4, 5) and best["g2p_variant"] in (0, 1, 2)
     ref = _sim(gpu, scenes, counts, mats, st)
     ref.step(5)
     sim.step(2)
@@ -655,3 +655,82 @@ def test_step_sorts_agree(gpu, oracle):
         a, b = outs[0][key], outs[1][key]
         err = np.abs(a - b).max() / max(np.abs(a).max(), 1e-30)
         assert err < 1e-4, (key, err)
+
+
+# ------------------------------------------------- fused G2P -> P2G (variant 5)
+def _fused_case(W, case):
+    if case == "two_material":
+        return W.two_material_drop(n_particles=100000, n=64, seed=41), 40
+    if case == "movers":
+        # dt 1e-3 and |v| ~ 3: about a tenth of the particles change cell per
+        # step and per axis, so the fused kernel's cell-change path is busy
+        return W.elastic_cube(n_particles=20000, n=32, v_sigma=3.0, seed=42, lo=0.25, hi=0.75, dt=1e-3,
+                              boundary=3), 25
+    return W.elastic_cube(n_particles=60000, n=64, v_sigma=0.1, seed=43), 64
+
+
+@pytest.mark.parametrize("blocks", [4, 6])
+@pytest.mark.parametrize("case", ["two_material", "movers", "elastic_cube"])
+def test_fused_step_matches_split_step_and_fp64(gpu, oracle, case, blocks):
+    """P2G variant 5 (each step's G2P kernel also does the next step's P2G)
+    at both register budgets against variant 4 (separate kernels, the payload
+    through memory) and the FP64 oracle: the same physics, summed in another
+    order."""
+    from physgrad_b200 import workloads as W
+
+    (scenes, counts, mats, st, _), steps = _fused_case(W, case)
+    outs = []
+    for variant in (5, 4):
+        sim = _sim(gpu, scenes, counts, mats, st)
+        sim.set_variants(p2g_variant=variant, p2g_tiles_per_sm=blocks if variant == 5 else 0)
+        sim.step(steps)
+        outs.append(sim.download())
+        assert sim.status() & 2 == 0
+        assert sim.metrics()["p2g_variant"] == variant
+    ref = oracle.run(_oracle_scene(oracle, scenes[0]),
+                     oracle.make_materials([(int(m.model), float(m.youngs_modulus), float(m.poisson_ratio))
+                                            for m in mats]), _oracle_state(st), steps, prec=64)
+    _assert_mls(outs[0], ref, f"fused ({blocks} blocks/SM) {case}")
+    _assert_mls(outs[1], ref, f"split {case}")
+    d = {k: np.abs(outs[0][k] - outs[1][k]).max() for k in ("x", "v", "F")}
+    print(f"fused vs split {case}: " + ", ".join(f"|d{k}| {v:.2e}" for k, v in d.items()))
+
+
+def test_fused_chain_across_calls_and_changes(gpu, oracle):
+    """The fused path leaves the next step's P2G pending between calls.  Calls
+    of 1 and 7 steps, a material change, a dt change and a re-upload between
+    them must give what the FP64 oracle gives for the same sequence."""
+    import dataclasses
+
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.two_material_drop(n_particles=40000, n=32, seed=44)
+    sim = _sim(gpu, scenes, counts, mats, st)
+    sim.step(1)
+    sim.step(7)
+    mid = sim.download()
+    osc = _oracle_scene(oracle, scenes[0])
+    om = lambda ms: oracle.make_materials([(int(m.model), float(m.youngs_modulus), float(m.poisson_ratio))
+                                           for m in ms])
+    ref = oracle.run(osc, om(mats), _oracle_state(st), 8, prec=64)
+    _assert_mls(mid, ref, "fused 1 + 7 steps")
+    # material change: the pending P2G held the old stress
+    mats2 = [dataclasses.replace(mats[0], youngs_modulus=2e5), mats[1]]
+    sim.set_materials(mats2)
+    sim.step(6)
+    st8 = dict(st, x=ref["x"], v=ref["v"], C=ref["C"], F=ref["F"])
+    ref = oracle.run(osc, om(mats2), _oracle_state(st8), 6, prec=64)
+    _assert_mls(sim.download(), ref, "after a material change")
+    # dt change
+    sim.set_scene_params(0, dt=2.5e-5)
+    sim.step(5)
+    st14 = dict(st, x=ref["x"], v=ref["v"], C=ref["C"], F=ref["F"])
+    osc2 = _oracle_scene(oracle, dataclasses.replace(scenes[0], dt=2.5e-5))
+    ref = oracle.run(osc2, om(mats2), _oracle_state(st14), 5, prec=64)
+    _assert_mls(sim.download(), ref, "after a dt change")
+    # re-upload the initial state: the pending P2G of the old state is dropped
+    sim.upload(st["x"], st["v"], st["C"].reshape(-1, 9), st["F"].reshape(-1, 9), st["m"], st["V0"], st["mat"])
+    sim.step(4)
+    ref = oracle.run(osc2, om(mats2), _oracle_state(st), 4, prec=64)
+    _assert_mls(sim.download(), ref, "after a re-upload")
+    assert sim.status() & 2 == 0

@@ -56,6 +56,7 @@ def _ostate(st):
 
 
 @pytest.mark.parametrize("bc,bthick,p2g_variant,sort", [(1, 3, 4, "bins"), (2, 3, 4, "bins"), (3, 2, 4, "bins"),
+                                                        (1, 3, 5, "bins"), (2, 3, 5, "bins"), (3, 2, 5, "bins"),
                                                         (1, 3, 2, "bins"), (3, 2, 2, "bins"), (2, 3, 3, "radix")])
 def test_mls_ragged_grid_vs_fp64_oracle(gpu, oracle, bc, bthick, p2g_variant, sort):
     from physgrad_b200 import _capi as C
@@ -122,7 +123,7 @@ def test_ref_compat_ragged_grid_vs_oracle(gpu, oracle):
     assert ex <= 2e-6 and ev <= 1e-4, (ex, ev)
 
 
-@pytest.mark.parametrize("p2g_variant", [2, 4])
+@pytest.mark.parametrize("p2g_variant", [2, 4, 5])
 def test_ragged_scenes_batched_equal_single(gpu, oracle, p2g_variant):
     """Three scenes of different ragged shapes, origins and walls in one
     batched solver give each scene's single-scene result."""
