@@ -226,7 +226,7 @@ PGMPM_API int pgmpm_set_tuning(pgmpm_solver s, int32_t p2g_block, int32_t ppt, i
  * next pgmpm_step call; uploads, material or scene changes and
  * differentiation recompute it.  MLS with the bin sort (else variant 4's
  * rules apply); p2g_tiles_per_sm 4 or 6 (its register budget).
- * pgmpm_create picks 5 for MLS solvers that use the bin sort, else 3 from
+ * pgmpm_create picks 4 for MLS solvers that use the bin sort, else 3 from
  * 2^20 particles and 2 below; REF_COMPAT runs variant 2 for 2-5.
  * g2p_variant 0: tile-staged gather (g2p_tiles_per_sm blocks per SM);
  * 1: direct gather in sorted order; 2: direct gather in physical order.

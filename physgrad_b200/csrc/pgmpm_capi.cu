@@ -391,7 +391,7 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     // without it, two lanes per cell pays off when the occupied tiles
     // outnumber the resident blocks (many particles), one lane otherwise
     s->tune.p2g_variant = s->pf.physics != PHYS_MLS ? 2
-                          : s->tune.step_sort == 0  ? 5
+                          : s->tune.step_sort == 0  ? 4
                           : N >= (int64_t)1 << 20   ? 3
                                                     : 2;
     if (e == cudaSuccess && s->tune.step_sort == 0 && alloc_bin_sort(s) != PGMPM_OK) e = cudaErrorMemoryAllocation;

@@ -1379,15 +1379,15 @@ __device__ __forceinline__ void mls_affine(const SceneDev& sc, const Stencil& st
 
 // F <- (I + dt C) F (a fluid's F reset to its volumetric part, cbrt(J) I)
 // and x <- x + dt v.
-template <bool MULTI, bool FLUID>
-__device__ __forceinline__ void mls_advance(const View& V, const SceneDev& sc, uint32_t p, const float nv[3],
+// mid: the particle's material id (0 with one material).
+template <bool FLUID>
+__device__ __forceinline__ void mls_advance(const View& V, const SceneDev& sc, int mid, const float nv[3],
                                             const float C[9], const float F[9], float x[3], float Fn[9]) {
     float M[9];
 #pragma unroll
     for (int a = 0; a < 9; ++a) M[a] = sc.dt * C[a] + (a % 4 == 0 ? 1.f : 0.f);
     m3_mul(M, F, Fn);
     if (FLUID) {
-        const int mid = MULTI ? V.mat[p] : 0;
         if (V.mats[mid].model == MODEL_EOS) {
             const float c = cbrtf(m3_det(Fn));
 #pragma unroll
@@ -1440,7 +1440,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
             qo[4 * N + p] = o4;
             qo[5 * N + p] = o5;
         }
-        mls_advance<MULTI, FLUID>(V, sc, p, nv, C, F, x, Fn);
+        mls_advance<FLUID>(V, sc, MULTI ? V.mat[p] : 0, nv, C, F, x, Fn);
         float4 o0, o1, o2;
         pack_xF(x, Fn, o0, o1, o2);
         qo[p] = o0;
@@ -1626,11 +1626,41 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(View V) {
 // registers, no spills; 6: 168 registers, some spilled).
 constexpr int G2_T = 64;
 
+// Asynchronous global -> shared copies (cp.async, no registers held while
+// the copy is in flight); completion per thread with cp_async_wait<n>.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N_>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N_) : "memory");
+}
+
+// One particle's G2P inputs staged in shared memory: q0..q2 (x, F), then
+// (m, V0) and the material id.
+struct G2Stage {
+    float4 q[3];
+    float2 mv;
+    int32_t mat;
+    int32_t pad;
+};
+
 template <bool MULTI, bool FLUID, bool PLASTIC, int MINB>
 __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
     __shared__ float4 box[TILE_NODES];           // grid_v of the tile's node block
     __shared__ float4 T4[27 * 64];                // [offset o][cell]: (m, p) of cell's node o
     __shared__ uint32_t s_end[G2_T / 32][64];     // per warp: end of each cell's range in the item
+    __shared__ G2Stage s_in[2][G2_T];             // per lane: inputs of this and the next particle
     __shared__ uint32_t s_work;
     constexpr uint32_t FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -1638,6 +1668,17 @@ __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
     uint32_t flags = 0;
     uint32_t* const wend = s_end[wp];
     const uint32_t ntiles = V.counters[CNT_CTILES];
+    // stage particle q's inputs into buffer b of this lane (copies in flight
+    // until the matching cp_async_wait)
+    auto stage = [&](uint32_t q, int b) {
+        if (q >= (uint32_t)N) return;
+        G2Stage& d = s_in[b][threadIdx.x];
+        cp_async16(&d.q[0], &V.q[q]);
+        cp_async16(&d.q[1], &V.q[N + q]);
+        cp_async16(&d.q[2], &V.q[2 * N + q]);
+        cp_async8(&d.mv, &V.mV[q]);
+        if (MULTI) cp_async4(&d.mat, &V.mat[q]);
+    };
     // slices of a tile's particles when tiles are few (each slice flushes the
     // tile's whole node block)
     const uint32_t S = ntiles ? min(8u, max(1u, (gridDim.x + ntiles - 1) / ntiles)) : 1u;
@@ -1709,10 +1750,21 @@ __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
             c = l;
             cend = wend[c];
         }
-        uint32_t pn = i0 < i1 ? V.order[i0] : 0u;
+        // Software pipeline over the run: the inputs of particle i + 1 are
+        // copied to shared memory while particle i is computed, and the
+        // sorted index two ahead is loaded, so an iteration does not wait on
+        // HBM for its own particle.
+        uint32_t pc = i0 < i1 ? V.order[i0] : 0u;
+        uint32_t pn = i0 + 1 < i1 ? V.order[i0 + 1] : 0u;
+        if (i0 < i1) stage(pc, 0);
+        cp_async_commit();
         for (uint32_t i = i0; i < i1; ++i) {
-            const uint32_t p = pn;
-            if (i + 1 < i1) pn = V.order[i + 1];
+            const uint32_t p = pc;
+            const int cur = (int)((i - i0) & 1u);
+            if (i + 1 < i1) stage(pn, cur ^ 1);
+            cp_async_commit();
+            pc = pn;
+            if (i + 2 < i1) pn = V.order[i + 2];
             if (i == cend) {
                 // the run passed the last particle of cell c: its sums are final
 #pragma unroll
@@ -1730,9 +1782,11 @@ __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
                 flags |= FLAG_TILE_RANGE;
                 continue;
             }
+            cp_async_wait<1>();  // this particle's copies are done (the next one's may not be)
+            const G2Stage& in = s_in[cur][threadIdx.x];
             // ---- G2P of this step
             float x[3], F[9];
-            unpack_xF(V.q[p], V.q[N + p], V.q[2 * N + p], x, F);
+            unpack_xF(in.q[0], in.q[1], in.q[2], x, F);
             Stencil st;
             make_stencil<PHYS_MLS>(sc, x, st, flags);
             const int lx = st.s[0] - ox, ly = st.s[1] - oy, lz = st.s[2] - oz0;
@@ -1768,7 +1822,7 @@ __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
                 qo[4 * N + p] = o4;
                 qo[5 * N + p] = o5;
             }
-            mls_advance<MULTI, FLUID>(V, sc, p, nv, C, F, x, Fn);
+            mls_advance<FLUID>(V, sc, MULTI ? in.mat : 0, nv, C, F, x, Fn);
             {
                 float4 o0, o1, o2;
                 pack_xF(x, Fn, o0, o1, o2);
@@ -1786,9 +1840,9 @@ __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
                 fn[a] = fminf(fmaxf(__fsub_rn(u, (float)so[a]), 0.5f), 1.5f);
             }
             V.keys[p] = cell_key(sc, so);
-            const float2 mv = V.mV[p];
+            const float2 mv = in.mv;
             float4 a0, a1, a2, a3;
-            mls_payload<PLASTIC>(sc, V.mats[MULTI ? V.mat[p] : 0], fn, Fn, nv, C, mv.x, mv.y, a0, a1, a2, a3);
+            mls_payload<PLASTIC>(sc, V.mats[MULTI ? in.mat : 0], fn, Fn, nv, C, mv.x, mv.y, a0, a1, a2, a3);
             float m, b[3], Ad[9], f[3];
             unpack_payload(a0, a1, a2, a3, m, b, Ad, f);
             float wt[3][3];
@@ -1838,6 +1892,7 @@ __global__ void __launch_bounds__(G2_T, MINB) k_g2p2g(View V) {
                         }
             }
         }
+        cp_async_wait<0>();  // no copy into the stage buffers outlives the item
         // a run that ends where its cell ends owns that cell; otherwise the
         // cell's owner is a later lane of this warp and the sum is partial
         const bool open = i0 < i1 && i1 != cend;
