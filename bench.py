@@ -503,6 +503,44 @@ def run_adjoint(args, device=0):
     return line
 
 
+def run_sparse(args, device=0):
+    """The two-material drop on a sparse grid (tile pool sized by the
+    library's default, max(4096, particles / 32) tiles) against the dense
+    grid: device ms per step of one call of K steps each, and the grid and
+    sort memory the sparse pool holds against the dense grid's."""
+    import torch
+
+    import physgrad_b200 as pg
+
+    torch.cuda.set_device(device)
+    scenes, counts, mats, st, meta = make_workload("cfg2")
+    N = int(sum(counts))
+    res = {}
+    for name, kw in (("dense", {}), ("sparse", {"sparse_tiles": 0})):
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(device)[0]
+        sim = pg.Simulator(scenes, counts, mats, device=device, **kw)
+        sim.upload(st["x"], st["v"], st["C"].reshape(N, 9), st["F"].reshape(N, 9), st["m"], st["V0"], st["mat"])
+        sim.step(args.warmup)
+        torch.cuda.synchronize()
+        used = free0 - torch.cuda.mem_get_info(device)[0]
+        e0, e1 = _events()
+        K = max(args.steps, 20)
+        e0.record()
+        sim.step(K)
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = {"ms_per_step": e0.elapsed_time(e1) / K, "device_bytes": int(used), "flags": sim.status()}
+        sim.close()
+    return {"n_particles": N, "grid": 128, "steps": max(args.steps, 20),
+            "dense_ms_per_step": round(res["dense"]["ms_per_step"], 5),
+            "sparse_ms_per_step": round(res["sparse"]["ms_per_step"], 5),
+            "ratio": round(res["sparse"]["ms_per_step"] / res["dense"]["ms_per_step"], 4),
+            "dense_device_bytes": res["dense"]["device_bytes"], "sparse_device_bytes": res["sparse"]["device_bytes"],
+            "flags": [res["dense"]["flags"], res["sparse"]["flags"]],
+            "note": "device bytes = the solver's allocations (state, grid, sort), read from cudaMemGetInfo"}
+
+
 def run_batched(args, device=0, adjoint=False, steps=None):
     """Config 4 (or 5 with adjoint): all scenes in one solver vs a loop of
     single-scene solvers (one launch sequence per scene per step).  steps:
@@ -594,6 +632,8 @@ def run_targets(args, device=0):
     step count."""
     import torch
 
+    sparse = run_sparse(args, device)
+    torch.cuda.empty_cache()
     adj = run_adjoint(args, device)
     torch.cuda.empty_cache()
     b4 = run_batched(args, device, adjoint=False, steps=500)
@@ -605,7 +645,9 @@ def run_targets(args, device=0):
         "grad_fd_rel_err": adj["grad_check"]["rel_err"],
         "batched_speedup_vs_loop": round(b4["speedup_vs_loop"], 3),
         "batched_adjoint_speedup_vs_loop": round(b5["speedup_vs_loop"], 3),
+        "sparse_vs_dense_step_ratio": sparse["ratio"],
         "targets": {
+            "sparse_grid_two_material_drop": sparse,
             "differentiable_elastic_cube": {
                 "n_particles": adj["config"]["n_particles"], "steps": adj["steps"], "checkpoint_every": 16,
                 "plain_forward_ms": round(adj["plain_forward_ms"], 3),

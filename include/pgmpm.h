@@ -56,7 +56,7 @@
 extern "C" {
 #endif
 
-#define PGMPM_ABI_VERSION 3
+#define PGMPM_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define PGMPM_API __attribute__((visibility("default")))
@@ -78,6 +78,7 @@ extern "C" {
 #define PGMPM_FLAG_NONFINITE 2u   /* non-finite position seen */
 #define PGMPM_FLAG_TILE_RANGE 4u  /* stencil fell outside its tile (internal) */
 #define PGMPM_FLAG_BAD_MATERIAL 8u /* material id outside [0, n_materials): used 0 */
+#define PGMPM_FLAG_TILE_POOL 16u   /* sparse grid: the tile pool was full (results invalid) */
 
 /* ---- enums ------------------------------------------------------------ */
 #define PGMPM_PHYSICS_MLS 0        /* MLS-MPM + APIC + stress + walls */
@@ -151,6 +152,22 @@ typedef struct {
     int32_t p2g_variant, g2p_variant, p2g_tiles_per_sm, g2p_tiles_per_sm;
 } pgmpm_metrics;
 
+/* Options of pgmpm_create_ex (zero-initialise; unset fields keep defaults). */
+typedef struct {
+    /* 1: a sparse grid.  Only the 4^3 node tiles that particles reach are
+     * stored, in a pool of slots found through a hash of the tile's
+     * coordinates, so memory follows the occupied region, not the domain:
+     * a 2048^3 domain holds what its particles touch.  One MLS scene, at
+     * most 4091 nodes per axis; the default kernels (P2G variant 4, G2P
+     * variant 2, bin sort); no differentiation.  A step that finds the
+     * pool full sets PGMPM_FLAG_TILE_POOL (create again with more tiles). */
+    int32_t sparse_grid;
+    int32_t reserved;
+    /* sparse: tiles the pool must hold (0: max(4096, particles / 32)); the
+     * pool is the next power of two of twice that. */
+    int64_t max_tiles;
+} pgmpm_create_options;
+
 /* ---- lifecycle ---------------------------------------------------------- */
 PGMPM_API const char* pgmpm_last_error(void);
 /* Empties the calling thread's last error message, so that a caller of the
@@ -163,6 +180,12 @@ PGMPM_API int pgmpm_abi_version(void);
  * per-particle material id.  device: CUDA ordinal. */
 PGMPM_API int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,
                  const pgmpm_material* materials, int32_t n_materials, int32_t device, pgmpm_solver* out);
+/* pgmpm_create with options (NULL: as pgmpm_create).  The reference's
+ * sparse structures (src/sparse_data_structures.h) are separate from its
+ * MPM grid; this makes the MPM grid itself sparse. */
+PGMPM_API int pgmpm_create_ex(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,
+                              const pgmpm_material* materials, int32_t n_materials, int32_t device,
+                              const pgmpm_create_options* options, pgmpm_solver* out);
 PGMPM_API int pgmpm_destroy(pgmpm_solver s);
 
 /* Replace the material table (same count), e.g. a new Young's modulus

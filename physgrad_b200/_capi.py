@@ -22,6 +22,8 @@ PGMPM_ERR_SIMULATION = -6
 FLAG_ESCAPE = 1
 FLAG_NONFINITE = 2
 FLAG_TILE_RANGE = 4
+FLAG_BAD_MATERIAL = 8
+FLAG_TILE_POOL = 16
 
 PHYSICS_MLS = 0
 PHYSICS_REF_COMPAT = 1
@@ -98,6 +100,14 @@ class Material(ctypes.Structure):
     ]
 
 
+class CreateOptions(ctypes.Structure):
+    _fields_ = [
+        ("sparse_grid", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("max_tiles", ctypes.c_int64),
+    ]
+
+
 class Metrics(ctypes.Structure):
     _fields_ = [
         ("total_steps", ctypes.c_int64),
@@ -143,6 +153,9 @@ SIGNATURES = {
     "pgmpm_clear_error": (None, []),
     "pgmpm_create": (ctypes.c_int, [ctypes.POINTER(SceneDesc), _i32, ctypes.POINTER(_i64), ctypes.POINTER(Material),
                                     _i32, _i32, ctypes.POINTER(_vp)]),
+    "pgmpm_create_ex": (ctypes.c_int, [ctypes.POINTER(SceneDesc), _i32, ctypes.POINTER(_i64),
+                                       ctypes.POINTER(Material), _i32, _i32, ctypes.POINTER(CreateOptions),
+                                       ctypes.POINTER(_vp)]),
     "pgmpm_destroy": (ctypes.c_int, [_vp]),
     "pgmpm_set_materials": (ctypes.c_int, [_vp, ctypes.POINTER(Material), _i32]),
     "pgmpm_set_scene_params": (ctypes.c_int, [_vp, _i32, ctypes.c_float, _vp]),

@@ -263,10 +263,25 @@ int pgmpm_abi_version(void) { return PGMPM_ABI_VERSION; }
 
 int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,
                  const pgmpm_material* materials, int32_t n_materials, int32_t device, pgmpm_solver* out) {
+    return pgmpm_create_ex(scenes, n_scenes, particle_counts, materials, n_materials, device, nullptr, out);
+}
+
+int pgmpm_create_ex(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t* particle_counts,
+                    const pgmpm_material* materials, int32_t n_materials, int32_t device,
+                    const pgmpm_create_options* options, pgmpm_solver* out) {
     if (!out) return fail(PGMPM_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (!scenes || n_scenes < 1 || !particle_counts) return fail(PGMPM_ERR_ARG, "need >= 1 scene and counts");
     if (!materials || n_materials < 1) return fail(PGMPM_ERR_ARG, "need >= 1 material");
+    const bool sparse = options && options->sparse_grid;
+    if (sparse) {
+        if (n_scenes != 1 || scenes[0].physics != PGMPM_PHYSICS_MLS)
+            return fail(PGMPM_ERR_UNSUPPORTED, "sparse grids: one scene with PGMPM_PHYSICS_MLS");
+        if (options->max_tiles < 0) return fail(PGMPM_ERR_ARG, "max_tiles must be >= 0");
+        for (int a = 0; a < 3; ++a)
+            if (scenes[0].n[a] > 4 * ((1 << 10) - 2) + 3)
+                return fail(PGMPM_ERR_ARG, "sparse grids: at most %d nodes per axis", 4 * ((1 << 10) - 2) + 3);
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
         return fail(PGMPM_ERR_CUDA, "no CUDA device available");
@@ -325,9 +340,9 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
         sd.inv_dx = 1.0f / d.dx;
         sd.dt = d.dt;
         s->scenes.push_back(sd);
-        if (ct_base * 64 > 0xFFFFFFFFll || nt_base * 64 >= 0x7FFFFFFFll) {
+        if (!sparse && (ct_base * 64 > 0xFFFFFFFFll || nt_base * 64 >= 0x7FFFFFFFll)) {
             delete s;
-            return fail(PGMPM_ERR_ARG, "grids too large for 32-bit cell keys");
+            return fail(PGMPM_ERR_ARG, "grids too large for 32-bit cell keys (a sparse grid stores only touched tiles)");
         }
     }
     if (N >= 0x7FFFFFFF) {
@@ -335,6 +350,22 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
         return fail(PGMPM_ERR_ARG, "too many particles (max 2^31-2)");
     }
     s->N = N;
+    if (sparse) {
+        // the tile pool: a power of two of at least twice the tiles asked for
+        // (the hash stays at most half full), one slot per cell / node tile
+        const int64_t want = options->max_tiles > 0 ? options->max_tiles : std::max<int64_t>(4096, N / 32);
+        int64_t cap = 1;
+        while (cap < 2 * want) cap <<= 1;
+        if (cap > ((int64_t)1 << 25)) {
+            delete s;
+            return fail(PGMPM_ERR_ARG, "sparse grids: max_tiles %lld above 2^24", (long long)want);
+        }
+        ct_base = nt_base = cap;
+        s->sp_cap = (uint32_t)cap;
+        int lg = 0;
+        while ((1ll << lg) < cap) ++lg;
+        s->sp_shift = 32 - lg;
+    }
     s->total_ct = (int)ct_base;
     s->total_nt = (int)nt_base;
     s->key_bits = bits_for((uint64_t)ct_base * 64);
@@ -383,10 +414,14 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     AL(s->ctile_list, sizeof(uint32_t) * (size_t)ct_base);
     AL(s->ctile_range, sizeof(uint2) * (size_t)ct_base);
     AL(s->counters, sizeof(uint32_t) * CNT_WORDS);
+    if (sparse) {
+        AL(s->sp_code, sizeof(uint32_t) * (size_t)s->sp_cap);
+        AL(s->sp_nbr, sizeof(uint4) * 2 * (size_t)s->sp_cap);
+    }
 #undef AL
     // the bin sort keeps 8 bytes per cell: default for grids with at most ~8
     // cells per particle, the radix sort (O(N) per pass) for sparser ones
-    s->tune.step_sort = (int64_t)ct_base * 64 <= 8 * std::max<int64_t>(N, 1) + (1 << 20) ? 0 : 1;
+    s->tune.step_sort = sparse || (int64_t)ct_base * 64 <= 8 * std::max<int64_t>(N, 1) + (1 << 20) ? 0 : 1;
     // P2G (MLS): balanced particle runs over the bin sort's cell table;
     // without it, two lanes per cell pays off when the occupied tiles
     // outnumber the resident blocks (many particles), one lane otherwise
@@ -401,6 +436,8 @@ int pgmpm_create(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int64_t
     if (e == cudaSuccess) e = cudaMemset(s->grid_v.p, 0, s->grid_v.bytes);
     if (e == cudaSuccess) e = cudaMemset(s->tile_flags.p, 0, s->tile_flags.bytes);
     if (e == cudaSuccess) e = cudaMemset(s->counters.p, 0, s->counters.bytes);
+    if (e == cudaSuccess && sparse) e = cudaMemset(s->sp_code.p, 0xFF, s->sp_code.bytes);  // every slot free
+    if (e == cudaSuccess && sparse) e = cudaMemset(s->sp_nbr.p, 0, s->sp_nbr.bytes);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking);
     for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_counters, sizeof(uint32_t) * CNT_WORDS);
@@ -746,6 +783,8 @@ int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_v
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
     if (p2g_variant > 5 || g2p_variant > 2 || p2g_tiles_per_sm > 16 || g2p_tiles_per_sm > 16)
         return fail(PGMPM_ERR_ARG, "p2g_variant 0..5, g2p_variant 0..2; blocks per SM at most 16");
+    if (s->sp_cap && ((p2g_variant >= 0 && p2g_variant != 4) || (g2p_variant >= 0 && g2p_variant != 2)))
+        return fail(PGMPM_ERR_UNSUPPORTED, "sparse grids run P2G variant 4 and G2P variant 2 only");
     if (p2g_variant == 5 && p2g_tiles_per_sm > 0 && p2g_tiles_per_sm != 4 && p2g_tiles_per_sm != 6)
         return fail(PGMPM_ERR_ARG, "p2g_variant 5 runs 4 or 6 blocks per SM");
     if (p2g_variant >= 0) s->tune.p2g_variant = p2g_variant;
@@ -769,6 +808,7 @@ int pgmpm_set_step_sort(pgmpm_solver s, int32_t kind) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
     if (kind != PGMPM_SORT_BINS && kind != PGMPM_SORT_RADIX)
         return fail(PGMPM_ERR_ARG, "kind must be PGMPM_SORT_BINS or PGMPM_SORT_RADIX");
+    if (s->sp_cap && kind != PGMPM_SORT_BINS) return fail(PGMPM_ERR_UNSUPPORTED, "sparse grids use the bin sort");
     if (kind == PGMPM_SORT_BINS) {
         DeviceGuard dg(s->device);
         int rc = alloc_bin_sort(s);
@@ -805,7 +845,7 @@ int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out) {
 int pgmpm_autotune(pgmpm_solver s, int32_t reps, void* stream) {
     if (!s) return fail(PGMPM_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(PGMPM_ERR_STATE, "upload particles before autotuning");
-    if (s->N == 0) return PGMPM_OK;
+    if (s->N == 0 || s->sp_cap) return PGMPM_OK;  // sparse grids have one kernel set
     DeviceGuard dg(s->device);
     cudaStream_t st = ST(stream);
     if (reps < 1) reps = 3;

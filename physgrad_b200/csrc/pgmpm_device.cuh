@@ -24,7 +24,7 @@ namespace pgmpm {
 enum { PHYS_MLS = 0, PHYS_REF = 1 };
 enum { BC_NONE = 0, BC_STICKY = 1, BC_SLIP = 2, BC_SEPARATE = 3 };
 enum { MODEL_FCR = 0, MODEL_NH = 1, MODEL_EOS = 2, MODEL_VM = 3 };  // VM: neo-Hookean + von Mises
-enum { FLAG_ESCAPE = 1u, FLAG_NONFINITE = 2u, FLAG_TILE_RANGE = 4u, FLAG_BAD_MATERIAL = 8u };
+enum { FLAG_ESCAPE = 1u, FLAG_NONFINITE = 2u, FLAG_TILE_RANGE = 4u, FLAG_BAD_MATERIAL = 8u, FLAG_TILE_POOL = 16u };
 
 struct SceneDev {
     int n[3];       // grid nodes per axis
@@ -192,6 +192,71 @@ __device__ __forceinline__ uint32_t cell_key(const SceneDev& sc, const int s[3])
 __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int i, int j, int k) {
     const int t = ((k >> 2) * sc.nt[1] + (j >> 2)) * sc.nt[0] + (i >> 2);
     return ((int64_t)(sc.nt_base + t) << 6) + ((k & 3) << 4) + ((j & 3) << 2) + (i & 3);
+}
+
+// ------------------------------------------------------------ sparse grid
+// A sparse grid stores only the 4^3 tiles that particles reach, in a pool
+// of `cap` slots found through an open-addressing hash of the tile's
+// coordinates (linear probing, slot = bucket).  One slot is both the cell
+// tile (cell keys slot * 64 + local cell) and the node tile (grid nodes
+// slot * 64 + local node) with those coordinates.  Slots are claimed with
+// atomicCAS and never released, so a slot's grid words stay at the zero
+// the grid update leaves them at.  nbr[c] lists, for an occupied cell tile c,
+// the slots of the 8 node tiles c + {0,1}^3 its particles' stencils reach
+// (rebuilt after every sort).
+struct SparseTiles {
+    uint32_t* code;  // [cap] packed tile coordinates of each slot, SP_EMPTY when free
+    uint4* nbr;      // [cap][2]: 8 node-tile slots (x + 2y + 4z offset order)
+    uint32_t cap;    // power of two (0: the grid is dense)
+    int shift;       // 32 - log2(cap)
+};
+constexpr uint32_t SP_EMPTY = 0xFFFFFFFFu;
+constexpr uint32_t SP_NONE = 0xFFFFFFFFu;
+constexpr int SP_MAX_PROBES = 64;
+constexpr int SP_AXIS_BITS = 10;  // tile coordinates < 1024 per axis (grids up to 4095 nodes)
+
+__device__ __forceinline__ uint32_t sp_code(int tx, int ty, int tz) {
+    return (uint32_t)tx | ((uint32_t)ty << SP_AXIS_BITS) | ((uint32_t)tz << (2 * SP_AXIS_BITS));
+}
+__device__ __forceinline__ void sp_decode(uint32_t code, int& tx, int& ty, int& tz) {
+    const uint32_t m = (1u << SP_AXIS_BITS) - 1u;
+    tx = (int)(code & m);
+    ty = (int)((code >> SP_AXIS_BITS) & m);
+    tz = (int)(code >> (2 * SP_AXIS_BITS));
+}
+// Slot of the tile with this code, claiming a free bucket when it has none;
+// SP_NONE (and FLAG_TILE_POOL) when SP_MAX_PROBES buckets were all taken.
+// Concurrent callers with one code get one slot: a bucket's code is written
+// once, by atomicCAS, and never changes.
+__device__ __forceinline__ uint32_t sp_find_or_insert(const SparseTiles& sp, uint32_t code, uint32_t& flags) {
+    uint32_t b = (code * 0x9E3779B1u) >> sp.shift;
+    for (int probe = 0; probe < SP_MAX_PROBES; ++probe) {
+        uint32_t k = *reinterpret_cast<volatile uint32_t*>(&sp.code[b]);
+        if (k == code) return b;
+        if (k == SP_EMPTY) {
+            k = atomicCAS(&sp.code[b], SP_EMPTY, code);
+            if (k == SP_EMPTY || k == code) return b;
+        }
+        b = (b + 1u) & (sp.cap - 1u);
+    }
+    flags |= FLAG_TILE_POOL;
+    return SP_NONE;
+}
+// Slot of node (i, j, k) from the 8 node-tile slots nb[] of the cell tile
+// whose lowest node is (ox, oy, oz); the node lies in [o, o + 6) per axis.
+__device__ __forceinline__ int64_t sp_node(const uint32_t nb[8], int i, int j, int k, int ox, int oy, int oz) {
+    const int lx = i - ox, ly = j - oy, lz = k - oz;
+    const int sel = (lx >> 2) | ((ly >> 2) << 1) | ((lz >> 2) << 2);
+    uint32_t slot = nb[0];
+#pragma unroll
+    for (int q = 1; q < 8; ++q)
+        if (sel == q) slot = nb[q];
+    return ((int64_t)slot << 6) + ((lz & 3) << 4) + ((ly & 3) << 2) + (lx & 3);
+}
+__device__ __forceinline__ void sp_load_nbr(const SparseTiles& sp, uint32_t c, uint32_t nb[8]) {
+    const uint4 a = sp.nbr[2 * (size_t)c], b = sp.nbr[2 * (size_t)c + 1];
+    nb[0] = a.x; nb[1] = a.y; nb[2] = a.z; nb[3] = a.w;
+    nb[4] = b.x; nb[5] = b.y; nb[6] = b.z; nb[7] = b.w;
 }
 
 // ----------------------------------------------------------- scene lookup

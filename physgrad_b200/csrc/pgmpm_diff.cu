@@ -237,6 +237,7 @@ extern "C" {
 int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoint_every, void* stream) {
     if (!s || n_steps < 1 || checkpoint_every < 1) return fail(PGMPM_ERR_ARG, "need n_steps >= 1, checkpoint_every >= 1");
     if (s->pf.physics != PHYS_MLS) return fail(PGMPM_ERR_UNSUPPORTED, "differentiation needs PGMPM_PHYSICS_MLS");
+    if (s->sp_cap) return fail(PGMPM_ERR_UNSUPPORTED, "differentiation needs a dense grid");
     if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
     if (int rc0 = check_differentiable(s)) return rc0;
     DeviceGuard dg(s->device);

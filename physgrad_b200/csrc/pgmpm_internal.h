@@ -23,9 +23,10 @@ enum {
     CNT_BUCKET = 6,
     CNT_RESET = CNT_BUCKET + CNT_BUCKETS,
     CNT_FLAGS = CNT_RESET,
+    CNT_STAMP = CNT_RESET + 1,  // sparse grids: step counter; a node tile is active when its flag equals it
     CNT_WORDS = 16
 };
-static_assert(CNT_FLAGS < CNT_WORDS, "counter layout");
+static_assert(CNT_STAMP < CNT_WORDS, "counter layout");
 
 // Everything a step kernel needs, passed by value.
 struct View {
@@ -55,6 +56,7 @@ struct View {
     const uint2* cell_range;   // per global cell: [begin, end) in sorted order (null: search skeys)
     uint32_t* counters;        // see CNT_*
     int total_ct, total_nt;
+    SparseTiles sp;            // sparse grid (sp.cap == 0: dense; tile ids are then slots)
 };
 
 // P2G variants: 0 = (cell, z-slice) register accumulation with a staged

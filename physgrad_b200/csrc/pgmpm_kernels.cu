@@ -47,9 +47,32 @@ __global__ void k_keys(View V) {
             float u;
             so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS, u, flags);
         }
-        V.keys[p] = cell_key(sc, so);
+        if (V.sp.cap) {  // sparse grid: the slot of the cell's tile, claimed if new
+            const uint32_t slot = sp_find_or_insert(V.sp, sp_code(so[0] >> 2, so[1] >> 2, so[2] >> 2), flags);
+            V.keys[p] = slot == SP_NONE ? SP_NONE
+                                        : slot * 64u + (uint32_t)((so[2] & 3) * 16 + (so[1] & 3) * 4 + (so[0] & 3));
+        } else {
+            V.keys[p] = cell_key(sc, so);
+        }
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
+}
+
+// Lowest node of cell tile ct (dense: from its index; sparse: from the
+// slot's coordinates).
+__device__ __forceinline__ void tile_origin(const View& V, const SceneDev& sc, uint32_t ct, int& ox, int& oy,
+                                            int& oz) {
+    if (V.sp.cap) {
+        sp_decode(V.sp.code[ct], ox, oy, oz);
+    } else {
+        const int lt = (int)ct - sc.ct_base;
+        ox = lt % sc.ct[0];
+        oy = (lt / sc.ct[0]) % sc.ct[1];
+        oz = lt / (sc.ct[0] * sc.ct[1]);
+    }
+    ox *= 4;
+    oy *= 4;
+    oz *= 4;
 }
 
 // --------------------------------------------------------------- payload
@@ -917,6 +940,7 @@ __device__ __forceinline__ void runs_store(float4* T4, uint32_t c, int h, const 
     for (int o = 0; o < 27; ++o) reinterpret_cast<float2*>(&T4[o * 64 + c])[h] = make_float2(accA[o], accB[o]);
 }
 
+template <bool SPARSE>
 __global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
     __shared__ float4 T4[27 * 64];                // [offset o][cell]: the 4 channels of cell's node o
     __shared__ uint32_t s_end[P2GR_T / 32][64];   // per warp: end of each cell's range in the item
@@ -944,9 +968,8 @@ __global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
         const uint2 rg = V.ctile_range[ct];
         const int s = V.S == 1 ? 0 : scene_of_cell_tile(V.scenes, V.S, (int)ct);
         const SceneDev& sc = scene_ref(V, s);
-        const int lt = (int)ct - sc.ct_base;
-        const int ox = 4 * (lt % sc.ct[0]), oy = 4 * ((lt / sc.ct[0]) % sc.ct[1]),
-                  oz0 = 4 * (lt / (sc.ct[0] * sc.ct[1]));
+        int ox, oy, oz0;
+        tile_origin(V, sc, ct, ox, oy, oz0);
         // the item's particles [lo, hi) and its cells' ranges clamped to them
         // (lane holds cells lane and lane + 32)
         const uint32_t P = rg.y > rg.x ? rg.y - rg.x : 0u;
@@ -1077,12 +1100,18 @@ __global__ void __launch_bounds__(P2GR_T, 5) k_p2g_runs(View V) {
             }
         }
         __syncthreads();
+        uint32_t nb[8];  // sparse: the slots of the 8 node tiles of the tile's node block
+        if (SPARSE) sp_load_nbr(V.sp, ct, nb);
         for (int n = threadIdx.x; n < TILE_NODES; n += P2GR_T) {
             const int nx = n % TN, ny = (n / TN) % TN, nz = n / (TN * TN);
             const float4 a4 = tile_node_sum(T4, nx, ny, nz);
             const int gi = ox + nx, gj = oy + ny, gk = oz0 + nz;
-            if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2])
-                atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+            if (a4.x != 0.f && gi < sc.n[0] && gj < sc.n[1] && gk < sc.n[2]) {
+                if (SPARSE)
+                    atomicAdd(&V.grid_mp[sp_node(nb, gi, gj, gk, ox, oy, oz0)], a4);
+                else
+                    atomicAdd(&V.grid_mp[node_index(sc, gi, gj, gk)], a4);
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) s_work = early ? next_work : atomicAdd(&V.counters[CNT_P2G_CURSOR], 1u);
@@ -1290,10 +1319,18 @@ __global__ void k_grid(View V) {
         if (nt >= (uint32_t)V.total_nt) continue;
         const int s = V.S == 1 ? 0 : scene_of_node_tile(V.scenes, V.S, (int)nt);
         const SceneDev& sc = scene_ref(V, s);
-        const int lt = (int)nt - sc.nt_base;
-        const int i = 4 * (lt % sc.nt[0]) + (l & 3);
-        const int j = 4 * ((lt / sc.nt[0]) % sc.nt[1]) + ((l >> 2) & 3);
-        const int k = 4 * (lt / (sc.nt[0] * sc.nt[1])) + (l >> 4);
+        int i, j, k;
+        if (V.sp.cap) {  // sparse: the slot's coordinates
+            sp_decode(V.sp.code[nt], i, j, k);
+        } else {
+            const int lt = (int)nt - sc.nt_base;
+            i = lt % sc.nt[0];
+            j = (lt / sc.nt[0]) % sc.nt[1];
+            k = lt / (sc.nt[0] * sc.nt[1]);
+        }
+        i = 4 * i + (l & 3);
+        j = 4 * j + ((l >> 2) & 3);
+        k = 4 * k + (l >> 4);
         const int64_t idx = ((int64_t)nt << 6) + l;
         const float4 mp = V.grid_mp[idx];
         float v[3] = {0.f, 0.f, 0.f};
@@ -1402,7 +1439,10 @@ __device__ __forceinline__ void mls_advance(const View& V, const SceneDev& sc, i
 // returns the (v, m) float4 of grid node (i, j, k) of scene sc.
 // PLASTIC: the payload's stress includes the von Mises cap (launched when an
 // ELASTOPLASTIC material is present).
-template <int PHYS, bool MULTI, bool FLUID, bool PLASTIC, class Fetch>
+// SPARSE (MLS, physical order, live solver only): the grid is the slot pool
+// of V.sp; the particle's tile is the slot of the key it was sorted by (read
+// before the new key overwrites it).
+template <int PHYS, bool MULTI, bool FLUID, bool PLASTIC, class Fetch, bool SPARSE = false>
 __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, uint32_t p, const Fetch& fetch,
                                              uint32_t& flags) {
     const int64_t N = V.N;
@@ -1414,22 +1454,58 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
         const float4 q1 = V.q[N + p], q2 = V.q[2 * N + p];
         float xx[3], F[9];
         unpack_xF(q0, q1, q2, xx, F);
-        // separable tiled node index: idx = X[i] + Y[j] + Z[k]
-        int X[3], Y[3], Z[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int gi = st.s[0] + a, gj = st.s[1] + a, gk = st.s[2] + a;
-            X[a] = ((gi >> 2) << 6) + (gi & 3);
-            Y[a] = (gj >> 2) * (sc.nt[0] << 6) + ((gj & 3) << 2);
-            Z[a] = (gk >> 2) * ((sc.nt[0] * sc.nt[1]) << 6) + ((gk & 3) << 4) + (sc.nt_base << 6);
-        }
         float nv[3], S[9];
-        mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
-            const int row = Y[j] + Z[k];
-            g0 = fetch(st.s[0], st.s[1] + j, st.s[2] + k, row + X[0]);
-            g1 = fetch(st.s[0] + 1, st.s[1] + j, st.s[2] + k, row + X[1]);
-            g2 = fetch(st.s[0] + 2, st.s[1] + j, st.s[2] + k, row + X[2]);
-        }, nv, S);
+        uint32_t oslot = 0;
+        int ox = 0, oy = 0, oz = 0;
+        if (SPARSE) {
+            const uint32_t okey = V.keys[p];
+            if (okey >= (uint32_t)V.total_ct * 64u) {  // no slot (a full pool): the particle is left as is
+                flags |= FLAG_TILE_POOL;
+                return;
+            }
+            oslot = okey >> 6;
+            sp_decode(V.sp.code[oslot], ox, oy, oz);
+            ox *= 4;
+            oy *= 4;
+            oz *= 4;
+            int l[3] = {st.s[0] - ox, st.s[1] - oy, st.s[2] - oz};
+            if ((unsigned)l[0] > 3u || (unsigned)l[1] > 3u || (unsigned)l[2] > 3u) {
+                // not in the tile it was sorted into: keep the gather inside
+                // that tile's node block and report it
+                flags |= FLAG_TILE_RANGE;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) l[a] = min(max(l[a], 0), 3);
+            }
+            uint32_t nb[8];
+            sp_load_nbr(V.sp, oslot, nb);
+            mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
+                const int yy = l[1] + j, zz = l[2] + k;
+                const int q = ((yy >> 2) << 1) | ((zz >> 2) << 2);  // 0, 2, 4 or 6
+                const uint32_t lo = q == 0 ? nb[0] : q == 2 ? nb[2] : q == 4 ? nb[4] : nb[6];
+                const uint32_t hi = q == 0 ? nb[1] : q == 2 ? nb[3] : q == 4 ? nb[5] : nb[7];
+                const int row = ((zz & 3) << 4) + ((yy & 3) << 2);
+                const int x0 = l[0], x1 = l[0] + 1, x2 = l[0] + 2;
+                g0 = fetch(0, 0, 0, (int)(((x0 >> 2) ? hi : lo) << 6) + row + (x0 & 3));
+                g1 = fetch(0, 0, 0, (int)(((x1 >> 2) ? hi : lo) << 6) + row + (x1 & 3));
+                g2 = fetch(0, 0, 0, (int)(((x2 >> 2) ? hi : lo) << 6) + row + (x2 & 3));
+            }, nv, S);
+        } else {
+            // separable tiled node index: idx = X[i] + Y[j] + Z[k]
+            int X[3], Y[3], Z[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int gi = st.s[0] + a, gj = st.s[1] + a, gk = st.s[2] + a;
+                X[a] = ((gi >> 2) << 6) + (gi & 3);
+                Y[a] = (gj >> 2) * (sc.nt[0] << 6) + ((gj & 3) << 2);
+                Z[a] = (gk >> 2) * ((sc.nt[0] * sc.nt[1]) << 6) + ((gk & 3) << 4) + (sc.nt_base << 6);
+            }
+            mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
+                const int row = Y[j] + Z[k];
+                g0 = fetch(st.s[0], st.s[1] + j, st.s[2] + k, row + X[0]);
+                g1 = fetch(st.s[0] + 1, st.s[1] + j, st.s[2] + k, row + X[1]);
+                g2 = fetch(st.s[0] + 2, st.s[1] + j, st.s[2] + k, row + X[2]);
+            }, nv, S);
+        }
         float C[9], Fn[9];
         mls_affine(sc, st, nv, S, C);
         float4* qo = V.q_out;
@@ -1455,7 +1531,16 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
             so[a] = stencil_origin(x[a], sc.origin[a], sc.dx, sc.inv_dx, sc.n[a], PHYS, u, flags);
             fn[a] = fminf(fmaxf(__fsub_rn(u, (float)so[a]), 0.5f), 1.5f);
         }
-        V.keys[p] = cell_key(sc, so);
+        if (SPARSE) {
+            const int tx = so[0] >> 2, ty = so[1] >> 2, tz = so[2] >> 2;
+            const uint32_t slot = (4 * tx == ox && 4 * ty == oy && 4 * tz == oz)
+                                      ? oslot
+                                      : sp_find_or_insert(V.sp, sp_code(tx, ty, tz), flags);
+            V.keys[p] = slot == SP_NONE ? SP_NONE
+                                        : slot * 64u + (uint32_t)((so[2] & 3) * 16 + (so[1] & 3) * 4 + (so[0] & 3));
+        } else {
+            V.keys[p] = cell_key(sc, so);
+        }
         if (V.pay_out) {
             const float2 mv = V.mV[p];
             float4 a0, a1, a2, a3;
@@ -1512,7 +1597,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
 // sorted at upload and particles drift less than a cell per step, so
 // neighbouring threads still share grid nodes, and the state loads are fully
 // coalesced with no dependent load of the order array.
-template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER, bool PLASTIC>
+template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER, bool PLASTIC, bool SPARSE = false>
 __device__ __forceinline__ void k_g2p_impl(const View& V) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1527,7 +1612,7 @@ __device__ __forceinline__ void k_g2p_impl(const View& V) {
         const SceneDev& sc = scene_ref(V, s);
         const float4* gv = V.grid_v;
         auto fetch = [&](int, int, int, int idx) { return __ldg(&gv[idx]); };
-        g2p_particle<PHYS, MULTI, FLUID, PLASTIC>(V, sc, p, fetch, flags);
+        g2p_particle<PHYS, MULTI, FLUID, PLASTIC, decltype(fetch), SPARSE>(V, sc, p, fetch, flags);
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
@@ -1546,6 +1631,11 @@ __global__ void __launch_bounds__(512, 2) k_g2p_phys(View V) {
 template <int PHYS, bool MULTI, bool FLUID>
 __global__ void __launch_bounds__(512, 2) k_g2p_phys_vm(View V) {
     k_g2p_impl<PHYS, MULTI, FLUID, true, true>(V);
+}
+// sparse grids (MLS)
+template <bool MULTI, bool FLUID, bool PLASTIC>
+__global__ void __launch_bounds__(512, 2) k_g2p_sparse(View V) {
+    k_g2p_impl<PHYS_MLS, MULTI, FLUID, true, PLASTIC, true>(V);
 }
 
 // G2P variant 0: one block per occupied cell tile; the tile's 6^3 node
@@ -2037,6 +2127,31 @@ __global__ void k_grid_download(View V, SceneDev sc, float* __restrict__ mass, f
     }
 }
 
+// Sparse grids: every node of the node tiles active in the last step (flag
+// equal to the step stamp) into the zeroed reference layout.
+__global__ void k_grid_download_sparse(View V, SceneDev sc, float* __restrict__ mass, float* __restrict__ vel) {
+    const uint32_t stamp = V.counters[CNT_STAMP];
+    const int64_t total = (int64_t)V.total_nt * 64;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const uint32_t slot = (uint32_t)(g >> 6);
+        if (V.tile_flags[slot] != stamp || V.sp.code[slot] == SP_EMPTY) continue;
+        const int l = (int)(g & 63);
+        int tx, ty, tz;
+        sp_decode(V.sp.code[slot], tx, ty, tz);
+        const int i = 4 * tx + (l & 3), j = 4 * ty + ((l >> 2) & 3), k = 4 * tz + (l >> 4);
+        if (i >= sc.n[0] || j >= sc.n[1] || k >= sc.n[2]) continue;
+        const int64_t li = ((int64_t)k * sc.n[1] + j) * sc.n[0] + i;
+        const float4 v = V.grid_v[g];
+        if (mass) mass[li] = v.w;
+        if (vel) {
+            vel[3 * li] = v.x;
+            vel[3 * li + 1] = v.y;
+            vel[3 * li + 2] = v.z;
+        }
+    }
+}
+
 inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
     int64_t g = (n + block - 1) / block;
     if (g < 1) g = 1;
@@ -2124,7 +2239,10 @@ cudaError_t launch_p2g(const View& V, const PhysFlags& pf, const Tuning& t, int 
     if (t.p2g_variant >= 3 && pf.physics == PHYS_MLS) {
         if (!V.pay) return cudaErrorInvalidValue;
         if (t.p2g_variant >= 4 && V.cell_range)  // without the sort's cell table: variant 3
-            k_p2g_runs<<<num_sms * t.pair_blocks_per_sm, P2GR_T, 0, st>>>(V);
+            if (V.sp.cap)
+                k_p2g_runs<true><<<num_sms * t.pair_blocks_per_sm, P2GR_T, 0, st>>>(V);
+            else
+                k_p2g_runs<false><<<num_sms * t.pair_blocks_per_sm, P2GR_T, 0, st>>>(V);
         else
             k_p2g_pairs<<<num_sms * t.pair_blocks_per_sm, P2GP_T, 0, st>>>(V);
         return cudaGetLastError();
@@ -2203,6 +2321,26 @@ cudaError_t launch_grid(const View& V, const PhysFlags& pf, const Tuning& t, int
 
 cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int num_sms, cudaStream_t st) {
     if (V.N == 0) return cudaSuccess;
+    if (V.sp.cap) {  // sparse grids run the physical-order MLS G2P only
+        if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
+        const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
+#define PGMPM_G2PS(M_, F_, P_) k_g2p_sparse<M_, F_, P_><<<nb, t.g2p_block, 0, st>>>(V)
+        if (pf.multi_mat) {
+            if (pf.has_fluid) {
+                if (pf.has_plastic) PGMPM_G2PS(true, true, true); else PGMPM_G2PS(true, true, false);
+            } else {
+                if (pf.has_plastic) PGMPM_G2PS(true, false, true); else PGMPM_G2PS(true, false, false);
+            }
+        } else {
+            if (pf.has_fluid) {
+                if (pf.has_plastic) PGMPM_G2PS(false, true, true); else PGMPM_G2PS(false, true, false);
+            } else {
+                if (pf.has_plastic) PGMPM_G2PS(false, false, true); else PGMPM_G2PS(false, false, false);
+            }
+        }
+#undef PGMPM_G2PS
+        return cudaGetLastError();
+    }
     if (t.g2p_variant == 0) {
         const int nb = num_sms * t.g2p_tiles_per_sm;
         PGMPM_G2P_DISPATCH(k_g2p_tiles, nb, 256);
@@ -2286,6 +2424,18 @@ cudaError_t launch_grid_download(const View& V, int scene, const SceneDev& sc, f
                                  cudaStream_t st) {
     (void)scene;
     const int64_t nodes = (int64_t)sc.n[0] * sc.n[1] * sc.n[2];
+    if (V.sp.cap) {  // the untouched nodes are zero
+        if (mass) {
+            cudaError_t e = cudaMemsetAsync(mass, 0, sizeof(float) * (size_t)nodes, st);
+            if (e != cudaSuccess) return e;
+        }
+        if (vel) {
+            cudaError_t e = cudaMemsetAsync(vel, 0, sizeof(float) * 3 * (size_t)nodes, st);
+            if (e != cudaSuccess) return e;
+        }
+        k_grid_download_sparse<<<grid_for((int64_t)V.total_nt * 64, 256), 256, 0, st>>>(V, sc, mass, vel);
+        return cudaGetLastError();
+    }
     k_grid_download<<<grid_for(nodes, 256), 256, 0, st>>>(V, sc, mass, vel);
     return cudaGetLastError();
 }

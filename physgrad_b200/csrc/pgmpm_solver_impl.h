@@ -116,6 +116,11 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf grid_mp, grid_v, grid_vpre, tile_flags, tile_list, ctile_list, ctile_range, counters, staging;
     pgmpm::DevBuf bs_ccount, bs_coff, bs_tcount, bs_toff, bs_bsum, bs_slot, cell_range;  // per-step bin sort
     pgmpm::DevBuf ptile_list, tile_rank;  // largest-first occupied tile list (bin sort)
+    // sparse grid (sp_cap > 0): tile pool hash (slot codes) and the per-tile
+    // node-tile slots; total_ct == total_nt == sp_cap
+    pgmpm::DevBuf sp_code, sp_nbr;
+    uint32_t sp_cap = 0;
+    int sp_shift = 0;
     uint32_t* h_counters = nullptr;  // pinned
 
     // fused G2P -> P2G (p2g_variant 5): true while grid_mp holds the P2G of
@@ -210,6 +215,10 @@ struct pgmpm_solver_s {
         V.counters = b.counters;
         V.total_ct = total_ct;
         V.total_nt = total_nt;
+        V.sp.code = sp_code.as<uint32_t>();
+        V.sp.nbr = sp_nbr.as<uint4>();
+        V.sp.cap = sp_cap;
+        V.sp.shift = sp_shift;
         return V;
     }
 
@@ -236,7 +245,7 @@ struct pgmpm_solver_s {
 
     // the live steps run the fused G2P -> P2G kernel
     bool fused() const {
-        return pf.physics == pgmpm::PHYS_MLS && tune.p2g_variant == 5 && tune.step_sort == 0 && N > 0;
+        return pf.physics == pgmpm::PHYS_MLS && tune.p2g_variant == 5 && tune.step_sort == 0 && N > 0 && !sp_cap;
     }
 
     ~pgmpm_solver_s() {

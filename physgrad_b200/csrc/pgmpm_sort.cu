@@ -252,6 +252,8 @@ __global__ void __launch_bounds__(BS_T) bs_count(const uint32_t* __restrict__ ke
     // the step's per-step counters start at zero: this is the step's first
     // kernel and it reads none of them (the step recording issues no memset)
     if (blockIdx.x == 0 && threadIdx.x < CNT_RESET) counters[threadIdx.x] = 0u;
+    // a new step stamp (sparse grids mark active node tiles with it)
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[CNT_STAMP] += 1u;
     const int64_t base = (int64_t)blockIdx.x * BS_TILE + warp * (32 * BS_ITEMS);
     uint32_t k[BS_ITEMS], cb[BS_ITEMS];
     int st[BS_ITEMS];
@@ -393,6 +395,25 @@ __global__ void __launch_bounds__(BS_T) bs_finish(View V, uint32_t* __restrict__
                 cell_range[(size_t)t * 64 + 2 * lane] = make_uint2(e, e + cc.x);
                 cell_range[(size_t)t * 64 + 2 * lane + 1] = make_uint2(e + cc.x, e + cc.x + cc.y);
             }
+            if (V.sp.cap) {
+                // sparse grid: lanes 0..7 find (or claim) the slots of the 8
+                // node tiles the cell tile's stencils reach, list them for the
+                // tile, and mark them active for this step (the first marker
+                // appends the tile to the active list)
+                uint32_t nslot = SP_NONE;
+                uint32_t f = 0;
+                if (lane < 8) {
+                    int tx, ty, tz;
+                    sp_decode(V.sp.code[t], tx, ty, tz);
+                    nslot = sp_find_or_insert(V.sp, sp_code(tx + (lane & 1), ty + ((lane >> 1) & 1), tz + (lane >> 2)),
+                                              f);
+                    reinterpret_cast<uint32_t*>(V.sp.nbr + 2 * (size_t)t)[lane] = nslot == SP_NONE ? 0u : nslot;
+                }
+                if (f) atomicOr(&V.counters[CNT_FLAGS], f);
+                const uint32_t stamp = V.counters[CNT_STAMP];
+                const bool fresh = lane < 8 && nslot != SP_NONE && atomicExch(&V.tile_flags[nslot], stamp) != stamp;
+                bs_append(V.tile_list, &V.counters[CNT_TILES], fresh, nslot, lane);
+            }
         }
         return;
     }
@@ -456,7 +477,8 @@ cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cuda
     bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, B.bsum, B.toff, B.ccount + ncells,
                                     B.ptile_list ? B.tile_rank : nullptr);
     const int cell_blocks = num_sms * 2;
-    const int node_blocks = (V.total_nt + BS_T - 1) / BS_T;
+    // sparse grids mark their node tiles from the occupied cell tiles
+    const int node_blocks = V.sp.cap ? 0 : (V.total_nt + BS_T - 1) / BS_T;
     bs_finish<<<cell_blocks + node_blocks, BS_T, 0, st>>>(V, B.ccount, B.toff, B.coff, B.cell_range, B.tile_rank,
                                                            B.ptile_list, cell_blocks);
     bs_scatter<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.slot, B.coff, B.toff + V.total_ct, B.out_k, B.out_v);

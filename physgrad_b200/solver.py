@@ -162,7 +162,9 @@ class Simulator:
     """Handle over pgmpm_* for one or more scenes (batched when > 1)."""
 
     def __init__(self, scenes: Sequence[Scene], counts: Sequence[int], materials: Sequence[MaterialParameters],
-                 device: int = 0, tuning: Optional[dict] = None):
+                 device: int = 0, tuning: Optional[dict] = None, sparse_tiles: Optional[int] = None):
+        """sparse_tiles: None for dense grids; else a sparse grid whose tile
+        pool holds that many 4^3 tiles (0: the library's default sizing)."""
         L = lib()
         self.scenes = list(scenes)
         self.counts = [int(c) for c in counts]
@@ -172,7 +174,13 @@ class Simulator:
         cn = (ctypes.c_int64 * len(self.counts))(*self.counts)
         md = (C.Material * len(self.materials))(*[m.to_c() for m in self.materials])
         h = ctypes.c_void_p()
-        check(L.pgmpm_create(sd, len(self.scenes), cn, md, len(self.materials), int(device), ctypes.byref(h)))
+        self.sparse = sparse_tiles is not None
+        if self.sparse:
+            opt = C.CreateOptions(1, 0, int(sparse_tiles))
+            check(L.pgmpm_create_ex(sd, len(self.scenes), cn, md, len(self.materials), int(device), ctypes.byref(opt),
+                                    ctypes.byref(h)))
+        else:
+            check(L.pgmpm_create(sd, len(self.scenes), cn, md, len(self.materials), int(device), ctypes.byref(h)))
         self._h = h
         self.device = device
         # incremented by every forward_checkpointed: a recording's identity,

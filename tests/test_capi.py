@@ -52,6 +52,7 @@ int main(void){
  printf("%zu %zu %zu %zu\n", sizeof(pgmpm_scene_desc), offsetof(pgmpm_scene_desc, dx), offsetof(pgmpm_scene_desc, gravity), offsetof(pgmpm_scene_desc, dt));
  printf("%zu %zu %zu\n", sizeof(pgmpm_material), offsetof(pgmpm_material, density), offsetof(pgmpm_material, viscosity));
  printf("%zu %zu %zu\n", sizeof(pgmpm_metrics), offsetof(pgmpm_metrics, p2g_block), offsetof(pgmpm_metrics, g2p_ms));
+ printf("%zu %zu\n", sizeof(pgmpm_create_options), offsetof(pgmpm_create_options, max_tiles));
  return 0;}
 ''')
     exe = tmp_path / "layout"
@@ -60,7 +61,8 @@ int main(void){
     got = [int(g) for g in got]
     exp = [ctypes.sizeof(C.SceneDesc), C.SceneDesc.dx.offset, C.SceneDesc.gravity.offset, C.SceneDesc.dt.offset,
            ctypes.sizeof(C.Material), C.Material.density.offset, C.Material.viscosity.offset,
-           ctypes.sizeof(C.Metrics), C.Metrics.p2g_block.offset, C.Metrics.g2p_ms.offset]
+           ctypes.sizeof(C.Metrics), C.Metrics.p2g_block.offset, C.Metrics.g2p_ms.offset,
+           ctypes.sizeof(C.CreateOptions), C.CreateOptions.max_tiles.offset]
     assert got == exp
 
 
@@ -99,7 +101,20 @@ def test_argument_validation_without_gpu(built_lib):
     assert b"scene" in L.pgmpm_last_error()
     assert L.pgmpm_step(None, 1, None) == C.PGMPM_ERR_ARG
     assert L.pgmpm_radix_sort_pairs(None, None, None, None, 10, 8, None) == C.PGMPM_ERR_ARG
-    assert L.pgmpm_abi_version() == 3
+    assert L.pgmpm_abi_version() == 4
+    # sparse grids: one MLS scene, at most 4091 nodes per axis (refused before any device work)
+    sd = (C.SceneDesc * 2)()
+    for d in sd:
+        d.n[0] = d.n[1] = d.n[2] = 64
+        d.dx, d.dt = 1.0 / 64, 1e-4
+    cn = (ctypes.c_int64 * 2)(100, 100)
+    md = (C.Material * 1)()
+    md[0].type, md[0].model, md[0].youngs_modulus, md[0].poisson_ratio, md[0].density = 0, 0, 1e4, 0.3, 1000.0
+    opt = C.CreateOptions(1, 0, 0)
+    assert L.pgmpm_create_ex(sd, 2, cn, md, 1, 0, ctypes.byref(opt), ctypes.byref(h)) == C.PGMPM_ERR_UNSUPPORTED
+    sd[0].n[0] = 4096
+    assert L.pgmpm_create_ex(sd, 1, cn, md, 1, 0, ctypes.byref(opt), ctypes.byref(h)) == C.PGMPM_ERR_ARG
+    assert b"nodes per axis" in L.pgmpm_last_error()
 
 
 def test_workloads_are_seeded_and_shaped():
