@@ -341,6 +341,38 @@ PGMPM_API int pgmpm_hashgrid_get_table(pgmpm_hashgrid g, uint32_t* counts, uint3
 /* getStats() (:243-272); before a build the particle fields are zero. */
 PGMPM_API int pgmpm_hashgrid_stats(pgmpm_hashgrid g, pgmpm_hashgrid_info* out);
 
+/* ---- consumers of the particles ------------------------------------------------ */
+/* CouplingConfig of src/sph_mpm_coupling.h:391-407 (the fields its forces use). */
+typedef struct {
+    float coupling_stiffness;        /* k, normal spring (default there 1e5) */
+    float coupling_damping;          /* c, normal damping (1e3) */
+    float friction_coefficient;      /* mu (0.3) */
+    float coupling_radius;           /* pairs closer than this (0.15) */
+    int32_t enable_two_way_coupling; /* 1: add the fluid forces to sph_force */
+    int32_t reserved;
+} pgmpm_sph_coupling_config;
+/* SPHMPMCouplingSystem::findCouplingPairs + computeCouplingForces +
+ * getNumCouplingPairs + getTotalCouplingEnergy (src/sph_mpm_coupling.h:
+ * 453-575) with the solver's particles (one scene, their current x and v)
+ * as the MPM side: every (SPH, MPM) pair closer than the radius, normal
+ * force k (r - d) + c (dv . n) along n = (x_mpm - x_sph) / d, friction
+ * -mu k (r - d) along the tangential relative velocity, nothing when
+ * d < 1e-6.  sph_x, sph_v [n_sph][3]; sph_force [n_sph][3]: the fluid forces
+ * are ADDED (as the reference adds them to SPHParticle::force), two-way only;
+ * mpm_force [N][3] (may be NULL): overwritten with each particle's summed
+ * solid force, upload order.  n_pairs, energy (sum of k (r - d)^2 / 2) may be
+ * NULL.  Pairs are found through the spatial hash grid of this library with
+ * a cell of one radius over the scene's grid domain.  Synchronises stream. */
+PGMPM_API int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, const float* sph_x,
+                                 const float* sph_v, int64_t n_sph, float* sph_force, float* mpm_force,
+                                 int64_t* n_pairs, double* energy, int32_t ptr_kind, void* stream);
+/* The energy monitor of FSISimulationManager (computeTotalEnergy,
+ * src/fsi_coupling.h:837-858): sum of m |v|^2 / 2 over the particles,
+ * per material id (per_material [n_materials], may be NULL) and in total
+ * (may be NULL); with a fluid and a solid material, the two sets that
+ * monitor sums.  FP64 sums.  Synchronises stream. */
+PGMPM_API int pgmpm_kinetic_energy(pgmpm_solver s, double* per_material, double* total, void* stream);
+
 /* ---- inspection ------------------------------------------------------------------ */
 #define PGMPM_ARRAY_USER_INDEX 0   /* physical slot -> upload index */
 #define PGMPM_ARRAY_KEYS 1         /* cell key per physical slot (input of the next sort) */

@@ -952,3 +952,73 @@ extern "C" int oracle_adjoint(const oracle_scene* sc, const oracle_material* mat
     for (int i = 0; i < nmat; ++i) gE[i] = gEv[i];
     return 0;
 }
+
+// ------------------------------------------------------------ consumers
+// SPH-MPM contact coupling, restating SPHMPMCouplingSystem::findCouplingPairs
+// (src/sph_mpm_coupling.h:453-485: every (SPH, MPM) pair closer than the
+// coupling radius, SPH index outer, MPM index inner), computeCouplingForces
+// (:487-545: normal spring k (r - d) plus damping c (dv . n) along
+// n = (x_mpm - x_sph) / d, friction -mu k (r - d) along the tangential
+// velocity, skipped when d < 1e-6; the fluid force, minus the solid force,
+// added to the SPH particle when two-way) and getTotalCouplingEnergy
+// (:563-575: sum of k (r - d)^2 / 2), in float and in the same order, so that
+// it matches the reference's own class bit for bit.
+extern "C" int oracle_sph_coupling(int64_t n_sph, const float* sph_x, const float* sph_v, int64_t n_mpm,
+                                   const float* mpm_x, const float* mpm_v, float k, float c, float mu, float r,
+                                   int two_way, float* sph_force, float* mpm_force, int64_t* n_pairs,
+                                   float* energy) {
+    int64_t pairs = 0;
+    float e = 0.f;
+    for (int64_t i = 0; i < 3 * n_mpm; ++i) mpm_force[i] = 0.f;
+    for (int64_t s = 0; s < n_sph; ++s) {
+        const float* y = &sph_x[3 * s];
+        const float* vy = &sph_v[3 * s];
+        float fs[3] = {0.f, 0.f, 0.f};
+        for (int64_t p = 0; p < n_mpm; ++p) {
+            const float rv[3] = {mpm_x[3 * p] - y[0], mpm_x[3 * p + 1] - y[1], mpm_x[3 * p + 2] - y[2]};
+            const float d = std::sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+            if (!(d < r)) continue;
+            ++pairs;
+            const float pen = r - d;
+            e += 0.5f * k * pen * pen;
+            if (d < 1e-6f) continue;
+            const float inv = 1.f / d;
+            const float n[3] = {rv[0] * inv, rv[1] * inv, rv[2] * inv};
+            const float dv[3] = {mpm_v[3 * p] - vy[0], mpm_v[3 * p + 1] - vy[1], mpm_v[3 * p + 2] - vy[2]};
+            const float fn = k * pen;
+            const float vn = dv[0] * n[0] + dv[1] * n[1] + dv[2] * n[2];
+            const float fd = c * vn;
+            float solid[3];
+            for (int a = 0; a < 3; ++a) solid[a] = n[a] * (fn + fd);
+            const float tv[3] = {dv[0] - n[0] * vn, dv[1] - n[1] * vn, dv[2] - n[2] * vn};
+            const float ts = std::sqrt(tv[0] * tv[0] + tv[1] * tv[1] + tv[2] * tv[2]);
+            if (ts > 1e-6f) {
+                const float it = 1.f / ts;
+                const float fm = mu * fn;
+                for (int a = 0; a < 3; ++a) solid[a] = solid[a] + (tv[a] * it) * (-fm);
+            }
+            for (int a = 0; a < 3; ++a) {
+                mpm_force[3 * p + a] += solid[a];
+                if (two_way) fs[a] += solid[a] * -1.f;
+            }
+        }
+        for (int a = 0; a < 3; ++a) sph_force[3 * s + a] = fs[a];
+    }
+    *n_pairs = pairs;
+    *energy = e;
+    return 0;
+}
+
+// Kinetic energy of particle sets, restating the energy monitor of
+// FSISimulationManager (computeTotalEnergy, src/fsi_coupling.h:837-858):
+// sum over particles of m |v|^2 / 2, here per material id (FP64).
+extern "C" int oracle_kinetic_energy(int64_t n, const double* v, const double* m, const int32_t* mat, int nmat,
+                                     double* per_material) {
+    for (int i = 0; i < nmat; ++i) per_material[i] = 0.0;
+    for (int64_t p = 0; p < n; ++p) {
+        const int id = mat ? mat[p] : 0;
+        if (id < 0 || id >= nmat) return -3;
+        per_material[id] += 0.5 * m[p] * (v[3 * p] * v[3 * p] + v[3 * p + 1] * v[3 * p + 1] + v[3 * p + 2] * v[3 * p + 2]);
+    }
+    return 0;
+}

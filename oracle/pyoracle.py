@@ -16,6 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libref_mpm.so")
 REF_DIFF_PATH = os.path.join(HERE, "_ref", "libref_diff.so")
+REF_COUPLING_PATH = os.path.join(HERE, "_ref", "libref_coupling.so")
+REF_FSI_PATH = os.path.join(HERE, "_ref", "libref_fsi.so")
 
 MLS, REF_COMPAT = 0, 1
 BC_NONE, BC_STICKY, BC_SLIP, BC_SEPARATE = 0, 1, 2, 3
@@ -305,3 +307,79 @@ def ref_run(x, v, m, vol, n, dx, dt, gravity, steps, origin=(0.0, 0.0, 0.0), wan
         out["grid_m"] = gm
         out["grid_v"] = gv
     return out
+
+
+# ------------------------------------------------------------ consumers
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _coupling_call(fn, sph_x, sph_v, mpm_x, mpm_v, stiffness, damping, friction, radius, two_way):
+    fp = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_int64, fp, fp, ctypes.c_int64, fp, fp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                   ctypes.c_float, ctypes.c_int, fp, fp, fp, fp]
+    sx, sv, mx, mv = _f32(sph_x), _f32(sph_v), _f32(mpm_x), _f32(mpm_v)
+    fs = np.empty_like(sx)
+    fm = np.empty_like(mx)
+    npairs = ctypes.c_int64()
+    e = ctypes.c_float()
+    rc = fn(sx.shape[0], sx.ctypes.data, sv.ctypes.data, mx.shape[0], mx.ctypes.data, mv.ctypes.data, stiffness,
+            damping, friction, radius, int(two_way), fs.ctypes.data, fm.ctypes.data, ctypes.byref(npairs),
+            ctypes.byref(e))
+    if rc != 0:
+        raise RuntimeError(f"coupling call failed: {rc}")
+    return {"sph_force": fs, "mpm_force": fm, "n_pairs": npairs.value, "energy": e.value}
+
+
+def sph_coupling(sph_x, sph_v, mpm_x, mpm_v, stiffness=1e5, damping=1e3, friction=0.3, radius=0.15, two_way=True):
+    """The oracle's restatement of the SPH-MPM contact coupling (float, the
+    reference's pair order): SPH forces (from zero), MPM solid-force sums,
+    pair count, coupling energy."""
+    return _coupling_call(lib().oracle_sph_coupling, sph_x, sph_v, mpm_x, mpm_v, stiffness, damping, friction,
+                          radius, two_way)
+
+
+def ref_coupling_available() -> bool:
+    return os.path.exists(REF_COUPLING_PATH)
+
+
+def ref_sph_coupling(sph_x, sph_v, mpm_x, mpm_v, stiffness=1e5, damping=1e3, friction=0.3, radius=0.15,
+                     two_way=True):
+    """The same through the reference's own SPHMPMCouplingSystem (oracle/_ref)."""
+    return _coupling_call(ctypes.CDLL(REF_COUPLING_PATH).ref_sph_coupling, sph_x, sph_v, mpm_x, mpm_v, stiffness,
+                          damping, friction, radius, two_way)
+
+
+def kinetic_energy(v, m, mat=None, n_materials=1):
+    """Kinetic energy per material id (FP64), the FSI energy monitor's sum."""
+    L = lib()
+    L.oracle_kinetic_energy.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int, ctypes.c_void_p]
+    vv = np.ascontiguousarray(v, dtype=np.float64)
+    mm = np.ascontiguousarray(m, dtype=np.float64)
+    mt = None if mat is None else np.ascontiguousarray(mat, dtype=np.int32)
+    out = np.zeros(n_materials)
+    rc = L.oracle_kinetic_energy(vv.shape[0], vv.ctypes.data, mm.ctypes.data, None if mt is None else mt.ctypes.data,
+                                 n_materials, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle_kinetic_energy failed: {rc}")
+    return out
+
+
+def ref_fsi_available() -> bool:
+    return os.path.exists(REF_FSI_PATH)
+
+
+def ref_fsi_energy(v_fluid, m_fluid, v_solid, m_solid) -> float:
+    """FSISimulationManager's computeTotalEnergy of a fluid and a solid set
+    (the reference's own code, oracle/_ref)."""
+    R = ctypes.CDLL(REF_FSI_PATH)
+    fp = ctypes.c_void_p
+    R.ref_fsi_energy.argtypes = [ctypes.c_int64, fp, fp, ctypes.c_int64, fp, fp, fp]
+    vf, mf, vs, ms = _f32(v_fluid), _f32(m_fluid), _f32(v_solid), _f32(m_solid)
+    e = ctypes.c_float()
+    rc = R.ref_fsi_energy(vf.shape[0], vf.ctypes.data, mf.ctypes.data, vs.shape[0], vs.ctypes.data, ms.ctypes.data,
+                          ctypes.byref(e))
+    if rc != 0:
+        raise RuntimeError(f"ref_fsi_energy failed: {rc}")
+    return e.value

@@ -108,6 +108,17 @@ class CreateOptions(ctypes.Structure):
     ]
 
 
+class SPHCouplingConfig(ctypes.Structure):
+    _fields_ = [
+        ("coupling_stiffness", ctypes.c_float),
+        ("coupling_damping", ctypes.c_float),
+        ("friction_coefficient", ctypes.c_float),
+        ("coupling_radius", ctypes.c_float),
+        ("enable_two_way_coupling", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class Metrics(ctypes.Structure):
     _fields_ = [
         ("total_steps", ctypes.c_int64),
@@ -157,6 +168,9 @@ SIGNATURES = {
                                        ctypes.POINTER(Material), _i32, _i32, ctypes.POINTER(CreateOptions),
                                        ctypes.POINTER(_vp)]),
     "pgmpm_destroy": (ctypes.c_int, [_vp]),
+    "pgmpm_sph_coupling": (ctypes.c_int, [_vp, ctypes.POINTER(SPHCouplingConfig), _vp, _vp, _i64, _vp, _vp,
+                                          ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_double), _i32, _vp]),
+    "pgmpm_kinetic_energy": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_double), _vp]),
     "pgmpm_set_materials": (ctypes.c_int, [_vp, ctypes.POINTER(Material), _i32]),
     "pgmpm_set_scene_params": (ctypes.c_int, [_vp, _i32, ctypes.c_float, _vp]),
     "pgmpm_upload": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),

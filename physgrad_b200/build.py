@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpgmpm.so")
 BUILD_DIR = os.path.join(PKG, "_build")
 SOURCES = ["pgmpm_sort.cu", "pgmpm_kernels.cu", "pgmpm_adjoint.cu", "pgmpm_capi.cu", "pgmpm_diff.cu",
-           "pgmpm_noalloc.cu", "pgmpm_hashgrid.cu", "pgmpm_ref_adjoint.cu"]
+           "pgmpm_noalloc.cu", "pgmpm_hashgrid.cu", "pgmpm_ref_adjoint.cu", "pgmpm_coupling.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]

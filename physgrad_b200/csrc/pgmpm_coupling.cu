@@ -1,0 +1,262 @@
+// pgmpm_coupling.cu -- consumers of the solver's particles on the device:
+//   * pgmpm_sph_coupling: the SPH-MPM contact coupling of
+//     SPHMPMCouplingSystem (src/sph_mpm_coupling.h:453-575), with the
+//     solver's particles as the MPM side.  Candidate MPM particles of each
+//     SPH particle come from the spatial hash grid (pgmpm_hashgrid_*, the
+//     reference's SpatialHashGrid) built on the current positions with a
+//     cell of one coupling radius; one thread per SPH particle keeps the
+//     pairs closer than the radius and forms their forces in the reference's
+//     float operations, in the same order, so pair membership is bit-exact;
+//     only the order in which a particle's pair forces are summed differs.
+//   * pgmpm_kinetic_energy: the energy monitor of FSISimulationManager
+//     (computeTotalEnergy, src/fsi_coupling.h:837-858), per material.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "pgmpm_solver_impl.h"
+
+using namespace pgmpm;
+
+namespace {
+
+// positions and velocities of the state (physical order) as [N][3]
+__global__ void k_state_xv(const float4* __restrict__ q, int64_t N, float* __restrict__ x, float* __restrict__ v) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        const float4 a = q[p], b = q[3 * N + p];
+        x[3 * p] = a.x;
+        x[3 * p + 1] = a.y;
+        x[3 * p + 2] = a.z;
+        v[3 * p] = b.x;
+        v[3 * p + 1] = b.y;
+        v[3 * p + 2] = b.z;
+    }
+}
+
+// One SPH particle per thread over its candidate MPM particles (physical
+// indices): the pairs closer than r, their contact forces (normal spring and
+// damping, friction along the tangential velocity), the fluid force summed
+// into sph_force (two-way), the solid force into mpm_force (upload order),
+// the pair count and k (r - d)^2 / 2 summed over pairs.
+__global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restrict__ sv, int64_t nq,
+                            const int64_t* __restrict__ off, const uint32_t* __restrict__ cand,
+                            const float* __restrict__ mx, const float* __restrict__ mv,
+                            const uint32_t* __restrict__ user_of_phys, pgmpm_sph_coupling_config cfg,
+                            float* __restrict__ sph_force, float* __restrict__ mpm_force,
+                            unsigned long long* __restrict__ npairs, double* __restrict__ energy) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const float k = cfg.coupling_stiffness, c = cfg.coupling_damping, mu = cfg.friction_coefficient,
+                r = cfg.coupling_radius;
+    unsigned long long cnt = 0;
+    double e = 0.0;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+        const float y0 = sx[3 * q], y1 = sx[3 * q + 1], y2 = sx[3 * q + 2];
+        const float w0 = sv[3 * q], w1 = sv[3 * q + 1], w2 = sv[3 * q + 2];
+        float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+        for (int64_t ci = off[q]; ci < off[q + 1]; ++ci) {
+            const uint32_t p = cand[ci];
+            // distance as the reference forms it (no contraction)
+            const float r0 = __fsub_rn(mx[3 * p], y0), r1 = __fsub_rn(mx[3 * p + 1], y1),
+                        r2 = __fsub_rn(mx[3 * p + 2], y2);
+            const float d = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2)));
+            if (!(d < r)) continue;
+            ++cnt;
+            const float pen = __fsub_rn(r, d);
+            e += (double)__fmul_rn(__fmul_rn(__fmul_rn(0.5f, k), pen), pen);
+            if (d < 1e-6f) continue;
+            const float inv = __fdiv_rn(1.f, d);
+            const float n0 = __fmul_rn(r0, inv), n1 = __fmul_rn(r1, inv), n2 = __fmul_rn(r2, inv);
+            const float d0 = __fsub_rn(mv[3 * p], w0), d1 = __fsub_rn(mv[3 * p + 1], w1),
+                        d2 = __fsub_rn(mv[3 * p + 2], w2);
+            const float fn = __fmul_rn(k, pen);
+            const float vn = __fadd_rn(__fadd_rn(__fmul_rn(d0, n0), __fmul_rn(d1, n1)), __fmul_rn(d2, n2));
+            const float ft = __fadd_rn(fn, __fmul_rn(c, vn));
+            float s0 = __fmul_rn(n0, ft), s1 = __fmul_rn(n1, ft), s2 = __fmul_rn(n2, ft);
+            const float t0 = __fsub_rn(d0, __fmul_rn(n0, vn)), t1 = __fsub_rn(d1, __fmul_rn(n1, vn)),
+                        t2 = __fsub_rn(d2, __fmul_rn(n2, vn));
+            const float ts = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(t0, t0), __fmul_rn(t1, t1)), __fmul_rn(t2, t2)));
+            if (ts > 1e-6f) {
+                const float it = __fdiv_rn(1.f, ts), fm = -__fmul_rn(mu, fn);
+                s0 = __fadd_rn(s0, __fmul_rn(__fmul_rn(t0, it), fm));
+                s1 = __fadd_rn(s1, __fmul_rn(__fmul_rn(t1, it), fm));
+                s2 = __fadd_rn(s2, __fmul_rn(__fmul_rn(t2, it), fm));
+            }
+            if (cfg.enable_two_way_coupling) {
+                f0 = __fadd_rn(f0, -s0);
+                f1 = __fadd_rn(f1, -s1);
+                f2 = __fadd_rn(f2, -s2);
+            }
+            if (mpm_force) {
+                const uint32_t u = user_of_phys[p];
+                atomicAdd(&mpm_force[3 * (size_t)u], s0);
+                atomicAdd(&mpm_force[3 * (size_t)u + 1], s1);
+                atomicAdd(&mpm_force[3 * (size_t)u + 2], s2);
+            }
+        }
+        if (cfg.enable_two_way_coupling) {
+            sph_force[3 * q] += f0;
+            sph_force[3 * q + 1] += f1;
+            sph_force[3 * q + 2] += f2;
+        }
+    }
+    // block sums of the pair count and the energy, one atomic each per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+        e += __shfl_down_sync(0xFFFFFFFFu, e, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (cnt) atomicAdd(npairs, cnt);
+        if (e != 0.0) atomicAdd(energy, e);
+    }
+}
+
+// m |v|^2 / 2 per particle, summed per material (FP64 accumulators)
+__global__ void k_kinetic(const float4* __restrict__ q, const float2* __restrict__ mV, const int32_t* __restrict__ mat,
+                          int64_t N, int M, double* __restrict__ out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    double e0 = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        const float4 v = q[3 * N + p];
+        const double ke = 0.5 * (double)mV[p].x * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+        if (mat) {
+            const int id = min(max(mat[p], 0), M - 1);
+            atomicAdd(&out[id], ke);
+        } else {
+            e0 += ke;
+        }
+    }
+    if (!mat) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) e0 += __shfl_down_sync(0xFFFFFFFFu, e0, o);
+        if ((threadIdx.x & 31) == 0 && e0 != 0.0) atomicAdd(&out[0], e0);
+    }
+}
+
+int nblocks(int64_t n, int t, int cap) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + t - 1) / t, cap)); }
+
+}  // namespace
+
+extern "C" {
+
+int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, const float* sph_x, const float* sph_v,
+                       int64_t n_sph, float* sph_force, float* mpm_force, int64_t* n_pairs, double* energy,
+                       int32_t ptr_kind, void* stream) {
+    if (!s || !cfg || n_sph < 0) return fail(PGMPM_ERR_ARG, "pgmpm_sph_coupling: bad arguments");
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    if (s->S != 1) return fail(PGMPM_ERR_UNSUPPORTED, "pgmpm_sph_coupling: one scene");
+    if (!(cfg->coupling_radius > 0.f) || !std::isfinite(cfg->coupling_radius))
+        return fail(PGMPM_ERR_ARG, "pgmpm_sph_coupling: coupling_radius must be positive");
+    if (n_sph > 0 && (!sph_x || !sph_v || (cfg->enable_two_way_coupling && !sph_force)))
+        return fail(PGMPM_ERR_ARG, "pgmpm_sph_coupling: sph_x, sph_v (and sph_force when two-way) are required");
+    if (ptr_kind != PGMPM_PTR_HOST && ptr_kind != PGMPM_PTR_DEVICE) return fail(PGMPM_ERR_ARG, "bad ptr_kind");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const int64_t N = s->N;
+    const size_t Nz = (size_t)std::max<int64_t>(N, 1), Qz = (size_t)std::max<int64_t>(n_sph, 1);
+    // the MPM side: current positions and velocities (physical order)
+    CK(s->cpl_xv.ensure(sizeof(float) * 6 * Nz));
+    float* mx = s->cpl_xv.as<float>();
+    float* mv = mx + 3 * Nz;
+    if (N > 0) k_state_xv<<<nblocks(N, 256, 148 * 16), 256, 0, st>>>(s->q.as<float4>(), N, mx, mv);
+    CK(cudaGetLastError());
+    // the SPH side on the device
+    const float *dsx = sph_x, *dsv = sph_v;
+    float* dsf = sph_force;
+    float* dmf = mpm_force;
+    if (ptr_kind == PGMPM_PTR_HOST) {
+        CK(s->cpl_stage.ensure(sizeof(float) * (9 * Qz + 3 * Nz)));
+        float* b = s->cpl_stage.as<float>();
+        if (n_sph > 0) {
+            CK(cudaMemcpyAsync(b, sph_x, sizeof(float) * 3 * n_sph, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(b + 3 * Qz, sph_v, sizeof(float) * 3 * n_sph, cudaMemcpyHostToDevice, st));
+            if (cfg->enable_two_way_coupling)
+                CK(cudaMemcpyAsync(b + 6 * Qz, sph_force, sizeof(float) * 3 * n_sph, cudaMemcpyHostToDevice, st));
+        }
+        dsx = b;
+        dsv = b + 3 * Qz;
+        dsf = b + 6 * Qz;
+        dmf = mpm_force ? b + 9 * Qz : nullptr;
+    }
+    if (dmf && N > 0) CK(cudaMemsetAsync(dmf, 0, sizeof(float) * 3 * N, st));
+    CK(s->cpl_acc.ensure(sizeof(double) * 2));
+    CK(cudaMemsetAsync(s->cpl_acc.p, 0, sizeof(double) * 2, st));
+    unsigned long long* d_pairs = s->cpl_acc.as<unsigned long long>();
+    double* d_energy = s->cpl_acc.as<double>() + 1;
+    if (N > 0 && n_sph > 0) {
+        // candidates: the MPM particles of the 27 hash cells (of one radius)
+        // around each SPH particle, over the scene's domain
+        const pgmpm_scene_desc& d = s->desc[0];
+        if (!s->cpl_grid || s->cpl_cell != cfg->coupling_radius || s->cpl_cap < N) {
+            if (s->cpl_grid) pgmpm_hashgrid_destroy(s->cpl_grid);
+            s->cpl_grid = nullptr;
+            float lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = d.origin[a];
+                hi[a] = d.origin[a] + (float)(d.n[a] - 1) * d.dx;
+            }
+            int rc = pgmpm_hashgrid_create(cfg->coupling_radius, lo, hi, N, s->device, &s->cpl_grid);
+            if (rc) return rc;
+            s->cpl_cell = cfg->coupling_radius;
+            s->cpl_cap = N;
+        }
+        int rc = pgmpm_hashgrid_build(s->cpl_grid, mx, N, PGMPM_PTR_DEVICE, stream);
+        if (rc) return rc;
+        CK(s->cpl_off.ensure(sizeof(int64_t) * (Qz + 1)));
+        int64_t total = 0;
+        rc = pgmpm_hashgrid_neighbors(s->cpl_grid, dsx, n_sph, cfg->coupling_radius, s->cpl_off.as<int64_t>(),
+                                      nullptr, 0, &total, PGMPM_PTR_DEVICE, stream);
+        if (rc) return rc;
+        CK(s->cpl_idx.ensure(sizeof(uint32_t) * (size_t)std::max<int64_t>(total, 1)));
+        rc = pgmpm_hashgrid_neighbors(s->cpl_grid, dsx, n_sph, cfg->coupling_radius, s->cpl_off.as<int64_t>(),
+                                      s->cpl_idx.as<uint32_t>(), total, &total, PGMPM_PTR_DEVICE, stream);
+        if (rc) return rc;
+        k_sph_pairs<<<nblocks(n_sph, 128, 148 * 16), 128, 0, st>>>(
+            dsx, dsv, n_sph, s->cpl_off.as<int64_t>(), s->cpl_idx.as<uint32_t>(), mx, mv,
+            s->user_of_phys.as<uint32_t>(), *cfg, dsf, dmf, d_pairs, d_energy);
+        CK(cudaGetLastError());
+    }
+    if (ptr_kind == PGMPM_PTR_HOST) {
+        if (cfg->enable_two_way_coupling && n_sph > 0)
+            CK(cudaMemcpyAsync(sph_force, dsf, sizeof(float) * 3 * n_sph, cudaMemcpyDeviceToHost, st));
+        if (mpm_force && N > 0) CK(cudaMemcpyAsync(mpm_force, dmf, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
+    }
+    unsigned long long h_pairs = 0;
+    double h_energy = 0.0;
+    CK(cudaMemcpyAsync(&h_pairs, d_pairs, sizeof(h_pairs), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&h_energy, d_energy, sizeof(h_energy), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (n_pairs) *n_pairs = (int64_t)h_pairs;
+    if (energy) *energy = h_energy;
+    return PGMPM_OK;
+}
+
+int pgmpm_kinetic_energy(pgmpm_solver s, double* per_material, double* total, void* stream) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(PGMPM_ERR_STATE, "no particles uploaded");
+    DeviceGuard dg(s->device);
+    cudaStream_t st = ST(stream);
+    const int M = s->M;
+    CK(s->cpl_acc.ensure(sizeof(double) * std::max(2, M)));
+    CK(cudaMemsetAsync(s->cpl_acc.p, 0, sizeof(double) * M, st));
+    if (s->N > 0)
+        k_kinetic<<<nblocks(s->N, 256, 148 * 8), 256, 0, st>>>(s->q.as<float4>(), s->mV.as<float2>(),
+                                                               s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr,
+                                                               s->N, M, s->cpl_acc.as<double>());
+    CK(cudaGetLastError());
+    std::vector<double> h(M);
+    CK(cudaMemcpyAsync(h.data(), s->cpl_acc.p, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double t = 0.0;
+    for (int i = 0; i < M; ++i) {
+        if (per_material) per_material[i] = h[i];
+        t += h[i];
+    }
+    if (total) *total = t;
+    return PGMPM_OK;
+}
+
+}  // extern "C"

@@ -121,6 +121,12 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf sp_code, sp_nbr;
     uint32_t sp_cap = 0;
     int sp_shift = 0;
+    // consumers (pgmpm_coupling.cu): particle x and v, host staging, the
+    // candidate hash grid and lists, the pair count and energy sums
+    pgmpm::DevBuf cpl_xv, cpl_stage, cpl_off, cpl_idx, cpl_acc;
+    pgmpm_hashgrid cpl_grid = nullptr;
+    float cpl_cell = 0.f;
+    int64_t cpl_cap = 0;
     uint32_t* h_counters = nullptr;  // pinned
 
     // fused G2P -> P2G (p2g_variant 5): true while grid_mp holds the P2G of
@@ -253,6 +259,7 @@ struct pgmpm_solver_s {
         cudaGetDevice(&prev);
         cudaSetDevice(device);
         drop_graph();
+        if (cpl_grid) pgmpm_hashgrid_destroy(cpl_grid);
         if (cap_stream) cudaStreamDestroy(cap_stream);
         if (side_stream) cudaStreamDestroy(side_stream);
         if (ev_fork) cudaEventDestroy(ev_fork);

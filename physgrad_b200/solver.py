@@ -318,6 +318,46 @@ class Simulator:
         check(lib().pgmpm_get_metrics(self._h, ctypes.byref(m)))
         return {k: getattr(m, k) for k, _ in C.Metrics._fields_}
 
+    # -- consumers of the particles
+    def sph_coupling(self, sph_x, sph_v, sph_force=None, mpm_force=None, stiffness=1e5, damping=1e3, friction=0.3,
+                     radius=0.15, two_way=True, stream=None):
+        """SPH-MPM contact coupling (SPHMPMCouplingSystem of the reference,
+        src/sph_mpm_coupling.h:453-575) with this solver's particles as the
+        MPM side.  The fluid forces are added to ``sph_force`` (zeros when
+        None); ``mpm_force`` receives each particle's summed solid force.
+        Arrays are numpy (host) or CUDA tensors, [n][3] float32.  Returns
+        (sph_force, mpm_force, n_pairs, energy)."""
+        n = int(sph_x.shape[0])
+        keep, kind = [], []
+        host = not _is_torch(sph_x)
+        if sph_force is None:
+            sph_force = np.zeros((n, 3), np.float32) if host else torch.zeros((n, 3), dtype=torch.float32,
+                                                                                device=sph_x.device)
+        if mpm_force is None:
+            mpm_force = np.zeros((self.N, 3), np.float32) if host else torch.zeros((self.N, 3), dtype=torch.float32,
+                                                                                     device=sph_x.device)
+        px = _ptr(sph_x, n, 3, np.float32, "sph_x", keep, kind)
+        pv = _ptr(sph_v, n, 3, np.float32, "sph_v", keep, kind)
+        pf = _ptr(sph_force, n, 3, np.float32, "sph_force", keep, kind)
+        pm = _ptr(mpm_force, self.N, 3, np.float32, "mpm_force", keep, kind)
+        if len(set(kind)) > 1:
+            raise ValueError("mix of host and device arrays")
+        cfg = C.SPHCouplingConfig(float(stiffness), float(damping), float(friction), float(radius), int(bool(two_way)),
+                                  0)
+        npairs = ctypes.c_int64()
+        energy = ctypes.c_double()
+        check(lib().pgmpm_sph_coupling(self._h, ctypes.byref(cfg), px, pv, n, pf, pm, ctypes.byref(npairs),
+                                       ctypes.byref(energy), kind[0] if kind else C.PTR_HOST, _stream_handle(stream)))
+        return keep[2], keep[3], npairs.value, energy.value  # the arrays written (a float32 copy if converted)
+
+    def kinetic_energy(self, stream=None):
+        """(per-material kinetic energies, total): the FSI energy monitor's
+        sum of m |v|^2 / 2 (src/fsi_coupling.h:837-858)."""
+        per = (ctypes.c_double * len(self.materials))()
+        tot = ctypes.c_double()
+        check(lib().pgmpm_kinetic_energy(self._h, per, ctypes.byref(tot), _stream_handle(stream)))
+        return np.array(per[:]), tot.value
+
     # -- differentiation
     def forward_checkpointed(self, n_steps: int, checkpoint_every: int, stream=None):
         """Runs n_steps from the current state and records them for backward();

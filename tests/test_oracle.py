@@ -281,3 +281,46 @@ def test_hashgrid_oracle_matches_reference_live():
         rc, rs, rix, ro, rl = H.reference_build_and_query(p, q, r, cs, mn, mx)
         for a, b in ((c, rc), (s, rs), (ix, rix), (o, ro), (l, rl)):
             assert np.array_equal(a, b)
+
+
+# ------------------------------------------------------------------ consumers
+def _coupling_inputs(seed, n_sph=400, n_mpm=900):
+    rng = np.random.default_rng(seed)
+    return (rng.uniform(0.3, 0.7, (n_sph, 3)).astype(np.float32), rng.normal(0, 0.5, (n_sph, 3)).astype(np.float32),
+            rng.uniform(0.3, 0.7, (n_mpm, 3)).astype(np.float32), rng.normal(0, 0.5, (n_mpm, 3)).astype(np.float32))
+
+
+@pytest.mark.parametrize("two_way,radius", [(True, 0.05), (False, 0.08), (True, 0.15)])
+def test_sph_coupling_restatement_equals_reference_class(oracle, two_way, radius):
+    """The oracle's SPH-MPM contact coupling equals the reference's own
+    SPHMPMCouplingSystem (src/sph_mpm_coupling.h:453-575, built from its
+    sources into oracle/_ref) bit for bit: forces, pair count, energy."""
+    if not oracle.ref_coupling_available():
+        pytest.skip("oracle/_ref not built")
+    sx, sv, mx, mv = _coupling_inputs(7 + int(radius * 100))
+    kw = dict(stiffness=2e4, damping=50.0, friction=0.4, radius=radius, two_way=two_way)
+    a = oracle.sph_coupling(sx, sv, mx, mv, **kw)
+    b = oracle.ref_sph_coupling(sx, sv, mx, mv, **kw)
+    assert a["n_pairs"] == b["n_pairs"] > 0
+    assert np.array_equal(a["sph_force"], b["sph_force"])
+    assert np.array_equal(a["mpm_force"], b["mpm_force"])
+    assert a["energy"] == b["energy"]
+    if not two_way:
+        assert not np.any(a["sph_force"])
+
+
+def test_kinetic_energy_restatement_matches_reference_monitor(oracle):
+    """The oracle's kinetic energy per material against the reference's
+    FSISimulationManager energy monitor (src/fsi_coupling.h:837-858) on a
+    fluid set and a solid set (float sums there: 1e-6 relative)."""
+    if not oracle.ref_fsi_available():
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(3)
+    vf, vs = rng.normal(0, 1, (5000, 3)), rng.normal(0, 2, (3000, 3))
+    mf, ms = rng.uniform(0.5, 1.5, 5000), rng.uniform(1, 3, 3000)
+    v = np.concatenate([vf, vs]).astype(np.float32).astype(np.float64)
+    m = np.concatenate([mf, ms]).astype(np.float32).astype(np.float64)
+    mat = np.concatenate([np.zeros(5000, np.int32), np.ones(3000, np.int32)])
+    ours = oracle.kinetic_energy(v, m, mat, 2)
+    ref = oracle.ref_fsi_energy(vf, mf, vs, ms)
+    assert abs(ours.sum() - ref) <= 1e-6 * ref
