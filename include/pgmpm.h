@@ -163,8 +163,8 @@ typedef struct {
      * pool full sets PGMPM_FLAG_TILE_POOL (create again with more tiles). */
     int32_t sparse_grid;
     int32_t reserved;
-    /* sparse: tiles the pool must hold (0: max(4096, particles / 32)); the
-     * pool is the next power of two of twice that. */
+    /* sparse: tiles the pool must hold (0: max(4096, particles / 128)); the
+     * pool is the next power of two of twice that, about 5.5 KB per slot. */
     int64_t max_tiles;
 } pgmpm_create_options;
 

@@ -353,7 +353,7 @@ int pgmpm_create_ex(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int6
     if (sparse) {
         // the tile pool: a power of two of at least twice the tiles asked for
         // (the hash stays at most half full), one slot per cell / node tile
-        const int64_t want = options->max_tiles > 0 ? options->max_tiles : std::max<int64_t>(4096, N / 32);
+        const int64_t want = options->max_tiles > 0 ? options->max_tiles : std::max<int64_t>(4096, N / 128);
         int64_t cap = 1;
         while (cap < 2 * want) cap <<= 1;
         if (cap > ((int64_t)1 << 25)) {
@@ -417,6 +417,8 @@ int pgmpm_create_ex(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int6
     if (sparse) {
         AL(s->sp_code, sizeof(uint32_t) * (size_t)s->sp_cap);
         AL(s->sp_nbr, sizeof(uint4) * 2 * (size_t)s->sp_cap);
+        AL(s->sp_box, sizeof(float4) * 216 * (size_t)s->sp_cap);
+        AL(s->sp_rev, sizeof(uint2) * 8 * (size_t)s->sp_cap);
     }
 #undef AL
     // the bin sort keeps 8 bytes per cell: default for grids with at most ~8
@@ -438,6 +440,8 @@ int pgmpm_create_ex(const pgmpm_scene_desc* scenes, int32_t n_scenes, const int6
     if (e == cudaSuccess) e = cudaMemset(s->counters.p, 0, s->counters.bytes);
     if (e == cudaSuccess && sparse) e = cudaMemset(s->sp_code.p, 0xFF, s->sp_code.bytes);  // every slot free
     if (e == cudaSuccess && sparse) e = cudaMemset(s->sp_nbr.p, 0, s->sp_nbr.bytes);
+    if (e == cudaSuccess && sparse) e = cudaMemset(s->sp_box.p, 0, s->sp_box.bytes);
+    if (e == cudaSuccess && sparse) e = cudaMemset(s->sp_rev.p, 0, s->sp_rev.bytes);  // stamp 0: no step yet
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking);
     for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_counters, sizeof(uint32_t) * CNT_WORDS);

@@ -204,9 +204,15 @@ __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int i, int j, 
 // the grid update leaves them at.  nbr[c] lists, for an occupied cell tile c,
 // the slots of the 8 node tiles c + {0,1}^3 its particles' stencils reach
 // (rebuilt after every sort).
+// The grid update also writes each occupied cell tile's 6^3 node velocities
+// contiguously (box[c]), so that G2P gathers them with dense local indices:
+// rev[n][q] = (c, stamp) names, for node tile n, the cell tile c = n - off(q)
+// whose box holds it, when c was occupied in the step of that stamp.
 struct SparseTiles {
     uint32_t* code;  // [cap] packed tile coordinates of each slot, SP_EMPTY when free
     uint4* nbr;      // [cap][2]: 8 node-tile slots (x + 2y + 4z offset order)
+    float4* box;     // [cap][216]: (v, m) of the cell tile's 6^3 node block, after the grid update
+    uint2* rev;      // [cap][8]: (cell tile, step stamp) whose box holds this node tile at offset q
     uint32_t cap;    // power of two (0: the grid is dense)
     int shift;       // 32 - log2(cap)
 };

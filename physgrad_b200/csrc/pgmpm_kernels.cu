@@ -1354,6 +1354,23 @@ __global__ void k_grid(View V) {
         }
         V.grid_v[idx] = make_float4(v[0], v[1], v[2], mp.x);
         V.grid_mp[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (V.sp.cap) {
+            // sparse: into the node block of every occupied cell tile that
+            // holds this node (offset q: the node tile is q above the cell
+            // tile; the node lies in its 6^3 block when its local
+            // coordinate is below 2 along each axis of q)
+            const uint32_t stamp = V.counters[CNT_STAMP];
+            const int lx = l & 3, ly = (l >> 2) & 3, lz = l >> 4;
+            const float4 gv = make_float4(v[0], v[1], v[2], mp.x);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int dx = q & 1, dy = (q >> 1) & 1, dz = q >> 2;
+                if ((dx && lx > 1) || (dy && ly > 1) || (dz && lz > 1)) continue;
+                const uint2 r = V.sp.rev[8 * (size_t)nt + q];
+                if (r.y != stamp) continue;
+                V.sp.box[216 * (size_t)r.x + (lx + 4 * dx) + TN * ((ly + 4 * dy) + TN * (lz + 4 * dz))] = gv;
+            }
+        }
     }
     // active node count: warp sums, then one atomic per block (a single
     // counter word takes every block's add)
@@ -1476,18 +1493,13 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
 #pragma unroll
                 for (int a = 0; a < 3; ++a) l[a] = min(max(l[a], 0), 3);
             }
-            uint32_t nb[8];
-            sp_load_nbr(V.sp, oslot, nb);
+            // the tile's node block, written by this step's grid update
+            const float4* box = V.sp.box + 216 * (size_t)oslot + l[0] + TN * (l[1] + TN * l[2]);
             mls_gather(st, [&](int j, int k, float4& g0, float4& g1, float4& g2) {
-                const int yy = l[1] + j, zz = l[2] + k;
-                const int q = ((yy >> 2) << 1) | ((zz >> 2) << 2);  // 0, 2, 4 or 6
-                const uint32_t lo = q == 0 ? nb[0] : q == 2 ? nb[2] : q == 4 ? nb[4] : nb[6];
-                const uint32_t hi = q == 0 ? nb[1] : q == 2 ? nb[3] : q == 4 ? nb[5] : nb[7];
-                const int row = ((zz & 3) << 4) + ((yy & 3) << 2);
-                const int x0 = l[0], x1 = l[0] + 1, x2 = l[0] + 2;
-                g0 = fetch(0, 0, 0, (int)(((x0 >> 2) ? hi : lo) << 6) + row + (x0 & 3));
-                g1 = fetch(0, 0, 0, (int)(((x1 >> 2) ? hi : lo) << 6) + row + (x1 & 3));
-                g2 = fetch(0, 0, 0, (int)(((x2 >> 2) ? hi : lo) << 6) + row + (x2 & 3));
+                const float4* r = box + TN * (j + TN * k);
+                g0 = __ldg(r);
+                g1 = __ldg(r + 1);
+                g2 = __ldg(r + 2);
             }, nv, S);
         } else {
             // separable tiled node index: idx = X[i] + Y[j] + Z[k]

@@ -118,7 +118,7 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf ptile_list, tile_rank;  // largest-first occupied tile list (bin sort)
     // sparse grid (sp_cap > 0): tile pool hash (slot codes) and the per-tile
     // node-tile slots; total_ct == total_nt == sp_cap
-    pgmpm::DevBuf sp_code, sp_nbr;
+    pgmpm::DevBuf sp_code, sp_nbr, sp_box, sp_rev;
     uint32_t sp_cap = 0;
     int sp_shift = 0;
     // consumers (pgmpm_coupling.cu): particle x and v, host staging, the
@@ -223,6 +223,8 @@ struct pgmpm_solver_s {
         V.total_nt = total_nt;
         V.sp.code = sp_code.as<uint32_t>();
         V.sp.nbr = sp_nbr.as<uint4>();
+        V.sp.box = sp_box.as<float4>();
+        V.sp.rev = sp_rev.as<uint2>();
         V.sp.cap = sp_cap;
         V.sp.shift = sp_shift;
         return V;

@@ -411,6 +411,9 @@ __global__ void __launch_bounds__(BS_T) bs_finish(View V, uint32_t* __restrict__
                 }
                 if (f) atomicOr(&V.counters[CNT_FLAGS], f);
                 const uint32_t stamp = V.counters[CNT_STAMP];
+                // node tile nslot lies at offset `lane` of this tile's box (one
+                // writer per (node tile, offset): t = nslot - offset)
+                if (lane < 8 && nslot != SP_NONE) V.sp.rev[8 * (size_t)nslot + lane] = make_uint2(t, stamp);
                 const bool fresh = lane < 8 && nslot != SP_NONE && atomicExch(&V.tile_flags[nslot], stamp) != stamp;
                 bs_append(V.tile_list, &V.counters[CNT_TILES], fresh, nslot, lane);
             }

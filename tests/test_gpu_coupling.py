@@ -71,15 +71,35 @@ def test_sph_coupling_adds_to_existing_forces(gpu):
     assert np.abs(f1 - (base + f0)).max() <= 1e-5 * (np.abs(f0).max() + 1.0)
 
 
+def _float_running_sum(v, m):
+    """The reference monitor's accumulation: a float total, each term
+    0.5 * m * |v|^2 formed in double and added in order (src/fsi_coupling.h:
+    841-856)."""
+    total = np.float32(0.0)
+    terms = 0.5 * m.astype(np.float64) * (v.astype(np.float32) ** 2).sum(1, dtype=np.float32).astype(np.float64)
+    for t in terms:
+        total = np.float32(np.float64(total) + t)
+    return total
+
+
 def test_kinetic_energy_matches_reference_monitor(gpu, oracle):
+    """The GPU sums in FP64 and equals the oracle's FP64 sum to 1e-9.  The
+    reference monitor keeps a float total: on nearly equal terms (the solid
+    falls at one speed) its rounding drifts one way, here by ~3e-4 relative.
+    It is pinned instead by replaying its float running sum on the same
+    particles, which it must equal to one float rounding."""
     if not oracle.ref_fsi_available():
         pytest.skip("oracle/_ref not built")
     sim, st = _drop(gpu, steps=20)
     out = sim.download()
     per, tot = sim.kinetic_energy()
     mat = st["mat"]
-    ref = oracle.ref_fsi_energy(out["v"][mat == 1], st["m"][mat == 1], out["v"][mat == 0], st["m"][mat == 0])
+    vf, mf, vs, ms = out["v"][mat == 1], st["m"][mat == 1], out["v"][mat == 0], st["m"][mat == 0]
+    ref = oracle.ref_fsi_energy(vf, mf, vs, ms)
     ours = oracle.kinetic_energy(out["v"].astype(np.float64), st["m"].astype(np.float64), mat, 2)
-    print(f"kinetic energy: GPU {tot:.8e} (solid {per[0]:.6e}, fluid {per[1]:.6e}), reference monitor {ref:.8e}")
-    assert abs(tot - ref) <= 1e-5 * ref
-    assert np.allclose(per, ours, rtol=1e-6)
+    replay = _float_running_sum(np.concatenate([vf, vs]), np.concatenate([mf, ms]))
+    print(f"kinetic energy: GPU {tot:.10e} (solid {per[0]:.6e}, fluid {per[1]:.6e}); FP64 oracle "
+          f"{ours.sum():.10e}; reference monitor {ref:.10e} (its float running sum replayed {float(replay):.10e})")
+    assert np.allclose(per, ours, rtol=1e-9)
+    assert abs(float(replay) - ref) <= 2 * np.spacing(np.float32(ref))
+    assert abs(tot - ref) <= 1e-3 * ref
