@@ -129,7 +129,8 @@ typedef struct {
  *   2 viscosity sym(grad v) of src/mpm_kernels.cu:131-149 (grad v = APIC C).
  * SAND and SNOW have no implementation in the reference and return
  * PGMPM_ERR_UNSUPPORTED.  Differentiation (pgmpm_forward_checkpointed,
- * pgmpm_backward) supports ELASTIC, JELLY and inviscid FLUID. */
+ * pgmpm_backward) covers every supported material, the von Mises cap and the
+ * fluid viscosity included (dL/dE: Young's modulus or bulk modulus). */
 typedef struct {
     int32_t type;          /* PGMPM_MAT_* */
     int32_t model;         /* PGMPM_MODEL_*; FLUID requires EOS_FLUID */

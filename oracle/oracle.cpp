@@ -215,6 +215,33 @@ template <class T> T kirchhoff_adj(const T F[9], const Mat<T>& mt, const T tb[9]
     T J = det3(F);
     T FiT[9];
     invT3(F, FiT);
+    if (mt.model == ORACLE_VON_MISES) {
+        // tau = p I + s dev(e), s = J Y / vm(e), above the yield stress (e the
+        // neo-Hookean predictor, p = tr(e)/3, vm = sqrt(3/2 |dev e|^2)):
+        //   <tb, dtau> = <tb_e, de> + s <tb, dev e> dJ / J,
+        //   tb_e = tr(tb)/3 I + s dev(tb) - s <tb, dev e> / |dev e|^2 dev e
+        T e[9];
+        Mat<T> nh = mt;
+        nh.model = ORACLE_NEO_HOOKEAN;
+        kirchhoff(F, nh, e);
+        const T pe = (e[0] + e[4] + e[8]) / T(3);
+        T d[9], ss = T(0);
+        for (int i = 0; i < 9; ++i) {
+            d[i] = e[i] - ((i % 4 == 0) ? pe : T(0));
+            ss += d[i] * d[i];
+        }
+        const T vm = std::sqrt(T(1.5) * ss);
+        if (!(vm > J * mt.yield)) return kirchhoff_adj(F, nh, tb, gF);
+        const T sc = J * mt.yield / vm;
+        const T pt = (tb[0] + tb[4] + tb[8]) / T(3);
+        T tbd = T(0);
+        for (int i = 0; i < 9; ++i) tbd += tb[i] * d[i];
+        T tbe[9];
+        for (int i = 0; i < 9; ++i)
+            tbe[i] = ((i % 4 == 0) ? pt : T(0)) + sc * (tb[i] - ((i % 4 == 0) ? pt : T(0))) - sc * tbd / ss * d[i];
+        for (int i = 0; i < 9; ++i) gF[i] += sc * tbd * FiT[i];  // (s <tb, d> / J) dJ/dF, dJ/dF = J F^-T
+        return kirchhoff_adj(F, nh, tbe, gF);
+    }
     T trt = tb[0] + tb[4] + tb[8];
     if (mt.model == ORACLE_FIXED_COROTATED) {
         T R[9], S[9];
@@ -779,6 +806,13 @@ void mls_step_adjoint(Sim<double>& S, const State<double>& st, State<double>& a,
             const Mat<T>& mt = S.mats[S.mat[p]];
             T tau[9];
             kirchhoff(&st.F[9 * p], mt, tau);
+            const bool viscous = mt.model == ORACLE_EOS_FLUID && mt.visc > T(0);
+            if (viscous) {  // as mls_p2g: tau += J mu_v (C + C^T)
+                const T* Cp = &st.C[9 * p];
+                const T J = det3(&st.F[9 * p]);
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) tau[3 * i + j] += J * mt.visc * (Cp[3 * i + j] + Cp[3 * j + i]);
+            }
             T A[9];
             const T mp = S.m[p];
             for (int i = 0; i < 9; ++i) A[i] = -dt * S.V0[p] * D * tau[i] + mp * st.C[9 * p + i];
@@ -831,12 +865,29 @@ void mls_step_adjoint(Sim<double>& S, const State<double>& st, State<double>& a,
             T tb[9];
             for (int i = 0; i < 9; ++i) tb[i] = -dt * S.V0[p] * D * Ab[i];
             gEl[S.mat[p]] += kirchhoff_adj(&st.F[9 * p], mt, tb, gF);
+            T gCv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (viscous) {
+                // tau_v = J mu_v (C + C^T): d/dC = J mu_v (tb + tb^T),
+                // d/dF = mu_v <tb, C + C^T> dJ/dF with dJ/dF = J F^-T
+                const T* Fp = &st.F[9 * p];
+                const T* Cp = &st.C[9 * p];
+                const T J = det3(Fp);
+                T FiT[9];
+                invT3(Fp, FiT);
+                T tc = T(0);
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        gCv[3 * i + j] = J * mt.visc * (tb[3 * i + j] + tb[3 * j + i]);
+                        tc += tb[3 * i + j] * (Cp[3 * i + j] + Cp[3 * j + i]);
+                    }
+                for (int i = 0; i < 9; ++i) gF[i] += mt.visc * tc * J * FiT[i];
+            }
             for (int aa = 0; aa < 3; ++aa) {
                 a.x[3 * p + aa] = gx[aa];
                 a.v[3 * p + aa] = gvp[aa];
             }
             for (int i = 0; i < 9; ++i) {
-                a.C[9 * p + i] = mp * Ab[i];
+                a.C[9 * p + i] = mp * Ab[i] + gCv[i];
                 a.F[9 * p + i] = gF[i];
             }
         }

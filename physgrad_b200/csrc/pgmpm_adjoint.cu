@@ -113,7 +113,8 @@ __global__ void __launch_bounds__(GATHER_T, 3) k_adj_gather(View V, AdjView A) {
         for (int a = 0; a < 9; ++a) gCt[a] = gC[a] + sc.dt * gFFt[a];
         // forward affine matrix (R kept for the stress adjoint)
         float tau[9], Am[9], R[9];
-        kirchhoff<false>(F, mt, tau, R);  // differentiation excludes ELASTOPLASTIC
+        kirchhoff<true>(F, mt, tau, R);
+        if (FLUID) add_viscous(F, C, mt, tau);
         const float kk = -sc.dt * mv.y * sc.D;
 #pragma unroll
         for (int a = 0; a < 9; ++a) Am[a] = kk * tau[a] + m * C[a];
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(GATHER_T, 3) k_adj_gather(View V, AdjView A) {
         float oC[9];
 #pragma unroll
         for (int a = 0; a < 9; ++a) oC[a] = m * Ab[a];
+        if (FLUID) add_viscous_adjoint(F, C, mt, tb, oF, oC);
         float4 g0, g1, g2, g3, g4, g5;
         pack_xF(ox, oF, g0, g1, g2);
         pack_vC(ogv, oC, g3, g4, g5);

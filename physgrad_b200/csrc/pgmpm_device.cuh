@@ -400,11 +400,54 @@ __device__ __forceinline__ void kirchhoff(const float F[9], const MatDev& m, flo
 // singular values) and stays invertible for det F > 0; no 1/(s_i^2 - s_j^2)
 // terms appear.
 // R: the rotation kirchhoff(F, m, tau, R) returned (fixed-corotated only).
+// MODEL_VM (neo-Hookean predictor e with the von Mises cap): above the
+// yield stress tau = p I + s dev(e), s = J Y / vm(e), p = tr(e)/3, and
+//   <tb, dtau> = <tb_e, de> + s <tb, dev e> dJ / J,
+//   tb_e = tr(tb)/3 I + s dev(tb) - s <tb, dev e> / |dev e|^2 dev e,
+// so the neo-Hookean adjoint runs with tb_e (below the yield stress, tb).
 __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const float R[9], const MatDev& m,
-                                                   const float tb[9], float gF[9]) {
+                                                   const float tb_in[9], float gF[9]) {
     float cofF[9];
     m3_cof(F, cofF);
     const float J = F[0] * cofF[0] + F[1] * cofF[1] + F[2] * cofF[2];  // cof = J F^{-T}
+    float tb[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) tb[i] = tb_in[i];
+    if (m.model == MODEL_VM) {
+        float B[9], d[9];
+        m3_mulT(F, F, B);
+        const float t = m.lam * logf(J);
+        float pe = 0.f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            d[i] = m.mu * (B[i] - ((i % 4 == 0) ? 1.f : 0.f)) + ((i % 4 == 0) ? t : 0.f);
+            if (i % 4 == 0) pe += d[i];
+        }
+        pe *= (1.f / 3.f);
+        float ss = 0.f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            d[i] -= (i % 4 == 0) ? pe : 0.f;
+            ss += d[i] * d[i];
+        }
+        const float vm = sqrtf(1.5f * ss);
+        if (vm > J * m.yield) {
+            const float sc = J * m.yield / vm;
+            const float pt = (tb[0] + tb[4] + tb[8]) * (1.f / 3.f);
+            float tbd = 0.f;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) tbd += tb[i] * d[i];
+            const float k = sc * tbd / ss;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const float dg = (i % 4 == 0) ? pt : 0.f;
+                tb[i] = dg + sc * (tb[i] - dg) - k * d[i];
+            }
+            const float cj = sc * tbd / J;  // times dJ/dF = cof F
+#pragma unroll
+            for (int i = 0; i < 9; ++i) gF[i] += cj * cofF[i];
+        }
+    }
     const float trt = tb[0] + tb[4] + tb[8];
     if (m.model == MODEL_FCR) {
         float D[9], tbF[9], tbTD[9];
@@ -446,7 +489,7 @@ __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const float
         for (int i = 0; i < 9; ++i) dmu += tb[i] * 2.f * tmu[i];
         const float dlam = trt * (J - 1.f) * J;
         return dmu * m.dmu_dE + dlam * m.dlam_dE;
-    } else if (m.model == MODEL_NH) {
+    } else if (m.model == MODEL_NH || m.model == MODEL_VM) {
         float a[9], b[9], B[9];
         m3_mul(tb, F, a);
         m3_Tmul(tb, F, b);
@@ -465,6 +508,27 @@ __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const float
         for (int i = 0; i < 9; ++i) gF[i] += c * cofF[i];
         return trt * J * (J - 1.f);
     }
+}
+
+// Adjoint of add_viscous: with tau_v = J mu_v (C + C^T), gC += J mu_v
+// (tb + tb^T) and gF += mu_v <tb, C + C^T> cof F (dJ/dF = cof F).
+__device__ __forceinline__ void add_viscous_adjoint(const float F[9], const float C[9], const MatDev& m,
+                                                    const float tb[9], float gF[9], float gC[9]) {
+    if (m.model != MODEL_EOS || !(m.visc > 0.f)) return;
+    float cofF[9];
+    m3_cof(F, cofF);
+    const float Jv = (F[0] * cofF[0] + F[1] * cofF[1] + F[2] * cofF[2]) * m.visc;
+    float tc = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            gC[3 * i + j] += Jv * (tb[3 * i + j] + tb[3 * j + i]);
+            tc += tb[3 * i + j] * (C[3 * i + j] + C[3 * j + i]);
+        }
+    const float c = m.visc * tc;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) gF[i] += c * cofF[i];
 }
 
 __device__ __forceinline__ float kirchhoff_adjoint(const float F[9], const MatDev& m, const float tb[9], float gF[9]) {

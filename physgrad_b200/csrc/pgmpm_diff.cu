@@ -221,14 +221,9 @@ int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
     return PGMPM_OK;
 }
 
-// The adjoint covers the elastic models and the inviscid EOS fluid.
-int check_differentiable(pgmpm_solver s) {
-    for (const pgmpm_material& m : s->mats_h)
-        if (m.type == PGMPM_MAT_ELASTOPLASTIC || (m.type == PGMPM_MAT_FLUID && m.viscosity > 0.f))
-            return fail(PGMPM_ERR_UNSUPPORTED,
-                        "differentiation of ELASTOPLASTIC materials and of viscous fluids is not built");
-    return PGMPM_OK;
-}
+// The adjoint covers every material model (the von Mises cap and the fluid
+// viscosity included, kirchhoff_adjoint / add_viscous_adjoint).
+int check_differentiable(pgmpm_solver) { return PGMPM_OK; }
 
 }  // namespace
 

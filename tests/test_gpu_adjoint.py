@@ -53,6 +53,50 @@ def test_adjoint_matches_fp64_oracle(gpu, oracle, bc, k):
         assert err <= 2e-3, (key, err)
 
 
+@pytest.mark.parametrize("case,k", [("plastic", 2), ("viscous", 3)])
+def test_plastic_and_viscous_adjoint_matches_fp64_oracle(gpu, oracle, case, k):
+    """The adjoint of the ELASTOPLASTIC model (von Mises cap active on most
+    particles: stretched F, a low yield stress) and of the viscous EOS fluid
+    (tau += J mu_v (C + C^T)) against the FP64 oracle's adjoint, which
+    matches FP64 central differences (tests/test_oracle.py)."""
+    rng = np.random.default_rng(80 + k)
+    N, n, steps, dt = 1500, 16, 6, 1e-3
+    st = _case(rng, N, n, spread=0.08)
+    MT, CM = gpu.MaterialType, gpu.ConstitutiveModel
+    if case == "plastic":
+        mats_o = [(3, 2e4, 0.3, 150.0), (oracle.FIXED_COROTATED, 1e4, 0.3), (3, 1e4, 0.25, 1e9)]
+        mats = [gpu.MaterialParameters(1000, 2e4, 0.3, MT.ELASTOPLASTIC, CM.NEO_HOOKEAN, yield_stress=150.0),
+                gpu.createElasticMaterial(1000, 1e4, 0.3),
+                gpu.MaterialParameters(1000, 1e4, 0.25, MT.ELASTOPLASTIC, CM.NEO_HOOKEAN, yield_stress=1e9)]
+    else:
+        mats_o = [(oracle.EOS_FLUID, 1e4, 0.0, 0.0, 30.0), (oracle.NEO_HOOKEAN, 3e4, 0.25),
+                  (oracle.EOS_FLUID, 2e4, 0.0, 0.0, 5.0)]
+        mats = [gpu.createFluidMaterial(1000, 30.0, 1e4), gpu.createElasticMaterial(1000, 3e4, 0.25, 1),
+                gpu.createFluidMaterial(1000, 5.0, 2e4)]
+    scene = gpu.Scene((n, n, n), 1.0 / n, dt, (0, -9.8, 0), (0, 0, 0), 0, 1, 3)
+    sim = gpu.Simulator([scene], [N], mats)
+    sim.upload(st["x"], st["v"], st["C"], st["F"], st["m"], st["V0"], st["mat"])
+    sim.forward_checkpointed(steps, k)
+    out = sim.download()
+    tgt = np.array([0.5, 0.3, 0.5])
+    go = {"x": np.tile(2 * (out["x"].mean(0) - tgt) / N, (N, 1)).astype(np.float32),
+          "v": (0.2 * out["v"]).astype(np.float32), "F": (0.02 * out["F"].reshape(N, 9)).astype(np.float32),
+          "C": (0.01 * out["C"].reshape(N, 9)).astype(np.float32)}
+    g = sim.backward(go)
+    assert sim.status() == 0
+    osc = oracle.make_scene((n, n, n), 1.0 / n, dt, physics=oracle.MLS, boundary=1, bthick=3)
+    ost = {k_: st[k_].astype(np.float64) for k_ in ("x", "v", "C", "F", "m", "V0")}
+    ost["mat"] = st["mat"]
+    ref = oracle.adjoint(osc, oracle.make_materials(mats_o), ost, steps,
+                         {k_: v.astype(np.float64) for k_, v in go.items()})
+    for key in ("x", "v", "C", "F", "E"):
+        a = np.asarray(g[key]).reshape(-1)
+        b = np.asarray(ref[key]).reshape(-1)
+        err = np.abs(a - b).max() / np.abs(b).max()
+        print(f"{case} d/d{key}: rel err {err:.2e} (max |ref| {np.abs(b).max():.3e})")
+        assert err <= 2e-3, (key, err)
+
+
 def test_adjoint_scatter_variants_agree(gpu):
     """The G2P-reverse scatter runs on the P2G kernel variant in use; the
     (cell, z-slice), thread-per-cell and balanced-run (variant 4) scatters

@@ -431,20 +431,12 @@ def test_plastic_and_viscous_vs_fp64_oracle(gpu, oracle, case):
     assert np.abs(ref["v"] - ref_el["v"]).max() > 100 * (np.abs(out["v"] - ref["v"]).max() + 1e-7)
 
 
-def test_plastic_and_viscous_reject_differentiation_and_bad_parameters(gpu):
-    """The adjoint covers the elastic models and the inviscid fluid: the
-    checkpointed forward refuses ELASTOPLASTIC and viscous materials; a
-    yield stress <= 0 or a negative viscosity is an argument error."""
+def test_plastic_and_viscous_bad_parameters(gpu):
+    """A yield stress <= 0 or a negative viscosity is an argument error."""
     from physgrad_b200 import workloads as W
 
-    MT, CM = gpu.MaterialType, gpu.ConstitutiveModel
+    MT = gpu.MaterialType
     scenes, counts, _, st, _ = W.elastic_cube(n_particles=2000, n=16, seed=33)
-    for mat in (gpu.MaterialParameters(1000, 1e4, 0.3, MT.ELASTOPLASTIC, CM.NEO_HOOKEAN, yield_stress=1e3),
-                gpu.createFluidMaterial(1000, 1.0, 1e4)):
-        sim = _sim(gpu, scenes, counts, [mat], st)
-        sim.step(2)
-        with pytest.raises(Exception, match="differentiation"):
-            sim.forward_checkpointed(4, 2)
     for mat, word in ((gpu.MaterialParameters(1000, 1e4, 0.3, MT.ELASTOPLASTIC, yield_stress=0.0), "yield_stress"),
                       (gpu.createFluidMaterial(1000, -1.0, 1e4), "viscosity")):
         with pytest.raises(Exception, match=word):

@@ -324,3 +324,51 @@ def test_kinetic_energy_restatement_matches_reference_monitor(oracle):
     ours = oracle.kinetic_energy(v, m, mat, 2)
     ref = oracle.ref_fsi_energy(vf, mf, vs, ms)
     assert abs(ours.sum() - ref) <= 1e-6 * ref
+
+
+@pytest.mark.parametrize("case", ["plastic", "viscous"])
+def test_oracle_adjoint_of_plastic_and_viscous_models(oracle, case):
+    """FP64 oracle adjoint vs central FD for the ELASTOPLASTIC model (the
+    von Mises cap active on most particles: a low yield stress and stretched
+    F) and the viscous EOS fluid (tau += J mu_v (C + C^T)), with an elastic
+    material beside it; every field and dL/dE."""
+    rng = np.random.default_rng(90 + (case == "viscous"))
+    N, dx, steps = 200, 1 / 16, 3
+    st = _small_state(rng, N, dx)
+    st["F"] = (np.tile(np.eye(3).ravel(), (N, 1)) + rng.normal(0, 0.08, (N, 9)))
+    sc = oracle.make_scene((16, 16, 16), dx, 2e-3, physics=oracle.MLS, boundary=1, bthick=3)
+    if case == "plastic":
+        mlist = [(3, 2e4, 0.3, 150.0), (oracle.FIXED_COROTATED, 1e4, 0.3), (3, 1e4, 0.25, 1e9)]
+    else:
+        mlist = [(oracle.EOS_FLUID, 1e4, 0.0, 0.0, 30.0), (oracle.NEO_HOOKEAN, 3e4, 0.25),
+                 (oracle.EOS_FLUID, 2e4, 0.0, 0.0, 5.0)]
+    mats = oracle.make_materials(mlist)
+    tgt = np.array([0.5, 0.3, 0.5])
+
+    def loss(s, mt=mats):
+        o = oracle.run(sc, mt, s, steps, prec=64)
+        return ((o["x"].mean(0) - tgt) ** 2).sum() + 0.1 * (o["v"] ** 2).sum() + 0.01 * (o["F"] ** 2).sum()
+
+    o = oracle.run(sc, mats, st, steps, prec=64)
+    g = oracle.adjoint(sc, mats, st, steps, dict(x=np.tile(2 * (o["x"].mean(0) - tgt) / N, (N, 1)), v=0.2 * o["v"],
+                                                 F=0.02 * o["F"].reshape(N, 9)))
+    eps = 1e-6
+    num, ana = [], []
+    for key, cols in (("x", 3), ("v", 3), ("C", 9), ("F", 9)):
+        for _ in range(5):
+            i, j = rng.integers(N), rng.integers(cols)
+            sp = {k: (a.copy() if isinstance(a, np.ndarray) else a) for k, a in st.items()}
+            sm = {k: (a.copy() if isinstance(a, np.ndarray) else a) for k, a in st.items()}
+            sp[key] = sp[key].reshape(N, cols)
+            sm[key] = sm[key].reshape(N, cols)
+            sp[key][i, j] += eps
+            sm[key][i, j] -= eps
+            num.append((loss(sp) - loss(sm)) / (2 * eps))
+            ana.append(g[key].reshape(N, -1)[i, j])
+    for mi in range(3):
+        hi = [tuple(b + (1e-2 if (k == mi and q == 1) else 0) for q, b in enumerate(m)) for k, m in enumerate(mlist)]
+        lo = [tuple(b - (1e-2 if (k == mi and q == 1) else 0) for q, b in enumerate(m)) for k, m in enumerate(mlist)]
+        num.append((loss(st, oracle.make_materials(hi)) - loss(st, oracle.make_materials(lo))) / 2e-2)
+        ana.append(g["E"][mi])
+    num, ana = np.array(num), np.array(ana)
+    assert np.abs(num - ana).max() <= 1e-4 * np.abs(num).max() + 1e-10
