@@ -41,6 +41,7 @@ int ensure_tape(pgmpm_solver s, int slots) {
     s->tape_slots = 0;
     s->tape_sets = 0;
     s->tape_has_last = false;
+    s->tape_has_prev = false;
     s->drop_tape_graphs();  // they hold the old tape's addresses
     CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1) * sets));
     CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1) * sets));
@@ -202,9 +203,13 @@ int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
         if (rc) return rc;
     }
     s->tape_has_last = false;  // the replays below overwrite it
+    // the forward left the second-to-last segment in set 1: no replay of it
+    const bool have_prev = s->tape_has_prev && last > 0;
+    s->tape_has_prev = false;
     int cur = 0;
     for (int seg = last; seg >= 0; --seg) {
-        if (seg > 0) {
+        const bool fork = seg > 0 && !(have_prev && seg == last);
+        if (fork) {
             CK(cudaEventRecord(s->ev_fork, st));
             CK(cudaStreamWaitEvent(side, s->ev_fork, 0));
             rc = replay(seg - 1, 1 - cur, side);
@@ -212,7 +217,7 @@ int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
         }
         rc = reverse(seg, cur, st);
         if (rc) return rc;
-        if (seg > 0) {
+        if (fork) {
             CK(cudaEventRecord(s->ev_join, side));
             CK(cudaStreamWaitEvent(st, s->ev_join, 0));
         }
@@ -246,31 +251,24 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     if (rc) return rc;
     s->ck_valid = false;
     s->tape_has_last = false;
+    s->tape_has_prev = false;
     rc = unprime(s, st);  // checkpoints and replays start from the state alone
     if (rc) return rc;
-    for (int seg = 0; seg < nseg; ++seg) {
-        CK(cudaMemcpyAsync(s->ck_q.as<float4>() + 6 * N * seg, s->q.p, sizeof(float4) * 6 * N,
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(s->ck_keys.as<uint32_t>() + N * seg, s->keys.p, sizeof(uint32_t) * N,
-                           cudaMemcpyDeviceToDevice, st));
-        const int len = std::min(k, n_steps - seg * k);
-        if (seg + 1 < nseg || s->N == 0) {
-            rc = run_steps(s, len, st);
-            if (rc) return rc;
-            continue;
-        }
-        // last segment: run it in the tape slots, so that the backward does
-        // not replay it, then hand the final state back to the live buffers
-        // (the tape starts from the state and its payload, with grid_mp clear)
-        rc = unprime(s, st);
-        if (rc) return rc;
-        CK(cudaMemcpyAsync(s->tape_q.p, s->q.p, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(s->tape_keys.p, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
+    // Runs a segment in the slots of tape set t, so that the backward does
+    // not replay it, then hands the final state back to the live buffers
+    // (the tape starts from the state and its payload, with grid_mp clear).
+    auto run_in_tape = [&](int len, int t) -> int {
+        int r = unprime(s, st);
+        if (r) return r;
+        const StepBufs first = tape_bufs(s, 0, t);
+        CK(cudaMemcpyAsync(first.q, s->q.p, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(first.keys_in, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_pay.p, s->pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
-        rc = tape_graph(s, 1, len, [&](cudaStream_t cs) { return record_tape_forward(s, len, cs); });
-        if (rc) return rc;
-        CK(cudaGraphLaunch(s->tape_exec[1], st));
-        const StepBufs last = tape_bufs(s, len - 1);
+        const int kind = t == 0 ? 1 : 6;
+        r = tape_graph(s, kind, len, [&](cudaStream_t cs) { return record_tape_forward(s, len, cs, t); });
+        if (r) return r;
+        CK(cudaGraphLaunch(s->tape_exec[kind], st));
+        const StepBufs last = tape_bufs(s, len - 1, t);
         CK(cudaMemcpyAsync(s->q.p, last.q_out, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->keys.p, last.keys_out, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->pay.p, s->tape_pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
@@ -280,9 +278,32 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->counters.as<uint32_t>() + CNT_ACTIVE, last.counters + CNT_ACTIVE, 2 * sizeof(uint32_t),
                            cudaMemcpyDeviceToDevice, st));
-        CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), len, s->counters.as<uint32_t>(), st));
+        CK(launch_merge_flags(s->tape_counters.as<uint32_t>() + (size_t)CNT_WORDS * s->tape_slots * t, len,
+                              s->counters.as<uint32_t>(), st));
         s->met.total_steps += len;
-        s->tape_has_last = true;
+        return PGMPM_OK;
+    };
+    // with two tape sets (the overlapped backward) the second-to-last
+    // segment runs in set 1 as well, so the backward replays one segment less
+    const bool prev_in_tape = s->tape_sets == 2 && s->tune.step_sort == 0 && nseg >= 2;
+    for (int seg = 0; seg < nseg; ++seg) {
+        CK(cudaMemcpyAsync(s->ck_q.as<float4>() + 6 * N * seg, s->q.p, sizeof(float4) * 6 * N,
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->ck_keys.as<uint32_t>() + N * seg, s->keys.p, sizeof(uint32_t) * N,
+                           cudaMemcpyDeviceToDevice, st));
+        const int len = std::min(k, n_steps - seg * k);
+        if (s->N == 0 || seg + 2 < nseg || (seg + 2 == nseg && !prev_in_tape)) {
+            rc = run_steps(s, len, st);
+            if (rc) return rc;
+            continue;
+        }
+        const int t = seg + 1 == nseg ? 0 : 1;
+        rc = run_in_tape(len, t);
+        if (rc) return rc;
+        if (t == 0)
+            s->tape_has_last = true;
+        else
+            s->tape_has_prev = true;
     }
     s->ck_steps = n_steps;
     s->ck_every = k;

@@ -158,12 +158,14 @@ struct pgmpm_solver_s {
     pgmpm::DevBuf tape_flags, tape_tiles, tape_ctiles, tape_crange, tape_counters;
     pgmpm::DevBuf tape_cells, tape_ptile;  // per slot: cell ranges and largest-first tile list (bin sort)
     bool tape_has_last = false;           // the tape holds the forward's last segment (no replay needed)
+    bool tape_has_prev = false;           // set 1 holds the forward's second-to-last segment
     // captured tape work, each for one segment length: [0] replay + reverse
     // of a segment (set 0), [1] forward of a segment into set 0, [2], [3]
-    // reverse of set 0 / 1, [4], [5] replay into set 0 / 1
-    static constexpr int kTapeGraphs = 6;
+    // reverse of set 0 / 1, [4], [5] replay into set 0 / 1, [6] forward of a
+    // segment into set 1
+    static constexpr int kTapeGraphs = 7;
     cudaGraphExec_t tape_exec[kTapeGraphs] = {};
-    int tape_exec_len[kTapeGraphs] = {-1, -1, -1, -1, -1, -1};
+    int tape_exec_len[kTapeGraphs] = {-1, -1, -1, -1, -1, -1, -1};
     cudaStream_t side_stream = nullptr;  // the replay that overlaps a segment's reverse
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     pgmpm::DevBuf adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;

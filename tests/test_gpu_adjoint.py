@@ -138,13 +138,14 @@ def test_checkpoint_interval_does_not_change_gradients(gpu):
             assert np.abs(a - b).max() <= 1e-3 * np.abs(b).max() + 1e-12, key
 
 
-@pytest.mark.parametrize("steps,k", [(40, 6), (32, 8), (5, 16)])
+@pytest.mark.parametrize("steps,k", [(40, 6), (32, 8), (12, 8), (5, 16)])
 def test_overlapped_and_sequential_backward_agree(gpu, steps, k):
-    """With the bin sort the backward replays segment s - 1 into a second
-    tape set on a side stream while segment s is reversed; with the radix
-    step sort each segment is replayed and reversed in turn.  Both give the
-    same gradients: segments of uneven length (40 = 6 x 6 + 4), of equal
-    length, and a single segment."""
+    """With the bin sort the forward leaves its last two segments in the two
+    tape sets, and the backward replays segment s - 1 into the free set on a
+    side stream while segment s is reversed; with the radix step sort each
+    segment is replayed and reversed in turn.  Both give the same gradients:
+    segments of uneven length (40 = 6 x 6 + 4), of equal length, two segments
+    (no replay at all) and a single segment."""
     from physgrad_b200 import _capi as C
     from physgrad_b200 import workloads as W
 
