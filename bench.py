@@ -445,14 +445,20 @@ def run_adjoint(args, device=0):
     up = lambda s: s.upload(st["x"], st["v"], None, None, st["m"], st["V0"])
     up(sim)
     sim.step(args.warmup)
-    up(sim)
     e0, e1 = _events()
-    torch.cuda.synchronize()
-    e0.record()
-    sim.step(steps)
-    e1.record()
-    torch.cuda.synchronize()
-    t_plain = e0.elapsed_time(e1)
+
+    def plain():
+        up(sim)
+        torch.cuda.synchronize()
+        e0.record()
+        sim.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    # each time is the median of 3 runs (both sides of the ratio alike)
+    reps = 3
+    t_plain = float(np.median([plain() for _ in range(reps)]))
     tgt = np.array([0.5, 0.3, 0.5])
     gx = torch.empty(N, 3, device="cuda")
 
@@ -472,7 +478,9 @@ def run_adjoint(args, device=0):
         return e0.elapsed_time(e1), float(((com.cpu().numpy() - tgt) ** 2).sum()), g
 
     fwd_adj()  # warm-up (allocates the tape)
-    t_fa, L, g = fwd_adj()
+    runs = [fwd_adj() for _ in range(reps)]
+    t_fa = float(np.median([r[0] for r in runs]))
+    _, L, g = runs[-1]
     # FD along a uniform v0 shift in y (full size, FP32 forward)
     eps = 1e-3
 
@@ -493,7 +501,8 @@ def run_adjoint(args, device=0):
             "ms_per_step": t_fa / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": "differentiable elastic cube (config 3)", "n_particles": N, "grid": 64,
-                       "steps": steps, "checkpoint_every": k, "loss": "||COM - (0.5,0.3,0.5)||^2"},
+                       "steps": steps, "checkpoint_every": k, "loss": "||COM - (0.5,0.3,0.5)||^2",
+                       "timing": f"median of {reps} runs of each, inputs re-uploaded before each"},
             "plain_forward_ms": t_plain, "forward_adjoint_ms": t_fa, "ratio_vs_plain_forward": t_fa / t_plain,
             "loss": L, "grad_check": {"direction": "uniform v0_y shift", "fd": fd, "adjoint": ad,
                                       "rel_err": abs(fd - ad) / abs(fd)},
@@ -653,6 +662,7 @@ def run_targets(args, device=0):
                 "plain_forward_ms": round(adj["plain_forward_ms"], 3),
                 "forward_adjoint_ms": round(adj["forward_adjoint_ms"], 3),
                 "ratio_vs_plain_forward": round(adj["ratio_vs_plain_forward"], 4), "target_ratio": 3.0,
+                "timing": adj["config"]["timing"],
                 "grad_check": adj["grad_check"],
                 "forward_adjoint_particle_steps_per_s": adj["value"]},
             "batched_forward_64_scenes": {

@@ -210,13 +210,14 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t* __restr
 //                with their loads and atomics issued back to back.
 //   bs_reduce / bs_down
 //                exclusive scan of the tile counts (block totals, then each
-//                block adds the totals before it); bs_down also emits each
+//                block adds the totals before it; on grids of up to 64 Ki
+//                cell tiles bs_down sums the counts before its range itself
+//                and bs_reduce is not launched); bs_down also emits each
 //                occupied tile (sorted range, entry in the occupied-tile
-//                list, rank in its size class) and clears the tile counters
-//                it read.
+//                list, rank in its size class).
 //   bs_finish    (a) one warp per occupied tile: scan of its 64 cell counts
 //                -> every cell's first sorted position and range, clearing
-//                the cell counters it read, and the tile's slot in the
+//                the cell and tile counters, and the tile's slot in the
 //                largest-first list P2G takes work from (the last tiles a
 //                persistent P2G block picks up are then small ones, which
 //                shortens the kernel's tail); (b) one thread per node tile:
@@ -230,6 +231,10 @@ constexpr int BS_T = 256;
 constexpr int BS_ITEMS = 8;                 // keys per thread in bs_count / bs_scatter
 constexpr int BS_TILE = BS_T * BS_ITEMS;    // keys per block
 constexpr int BS_SCAN = 1024;               // tile counts per scan block
+// up to this many scan blocks (64 Ki cell tiles, a 256^3 grid) bs_down sums
+// the counts before its range directly, without bs_reduce: the last block
+// reads at most 63 Ki words from L2
+constexpr int BS_DIRECT_BLOCKS = 64;
 
 // Run structure of `bin` over a warp: first lane of this lane's run and one
 // past its last lane.  A run is a maximal stretch of consecutive lanes with
@@ -317,7 +322,11 @@ __device__ __forceinline__ int bs_class(uint32_t count) {
     return min(CNT_BUCKETS - 1, max(0, 10 - lg));
 }
 
-__global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict__ tcount, int64_t n,
+// bsum: the per-block totals of bs_reduce, or null when the blocks are few
+// (BS_DIRECT_BLOCKS): each block then sums the tile counts before its own
+// range itself, and the step has no bs_reduce launch.  The tile counts are
+// left for bs_finish to clear, since later blocks read earlier blocks' range.
+__global__ void __launch_bounds__(BS_SCAN) bs_down(View V, const uint32_t* __restrict__ tcount, int64_t n,
                                                    const uint32_t* __restrict__ bsum, uint32_t* __restrict__ toff,
                                                    uint32_t* __restrict__ ccount_overflow,
                                                    uint32_t* __restrict__ tile_rank) {
@@ -325,17 +334,19 @@ __global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict_
     const int lane = threadIdx.x & 31;
     // this block's first position: the tile totals of the blocks before it
     uint32_t part = 0u;
-    for (uint32_t b = threadIdx.x; b < blockIdx.x; b += BS_SCAN) part += bsum[b];
+    if (bsum) {
+        for (uint32_t b = threadIdx.x; b < blockIdx.x; b += BS_SCAN) part += bsum[b];
+    } else {
+        const int64_t end = (int64_t)blockIdx.x * BS_SCAN;
+        for (int64_t i = threadIdx.x; i < end; i += BS_SCAN) part += tcount[i];
+    }
     uint32_t base;
     block_excl_scan(part, sh, base);
     const int64_t t = (int64_t)blockIdx.x * BS_SCAN + threadIdx.x;
     const uint32_t c = t < n ? tcount[t] : 0u;
     uint32_t tot;
     const uint32_t ex = block_excl_scan(c, sh, tot) + base;
-    if (t < n) {
-        toff[t] = ex;
-        tcount[t] = 0u;  // left clear for the next step
-    }
+    if (t < n) toff[t] = ex;
     if (t == n - 1) *ccount_overflow = 0u;
     const bool occ = t < (int64_t)V.total_ct && c > 0u;  // not the overflow bin
     if (occ) V.ctile_range[t] = make_uint2(ex, ex + c);
@@ -353,12 +364,16 @@ __global__ void __launch_bounds__(BS_SCAN) bs_down(View V, uint32_t* __restrict_
 }
 
 // Blocks [0, cell_blocks): (a), the rest: (b).  See the overview above.
+// (a) also clears the tile counts bs_count wrote (the occupied tiles' and
+// the overflow bin's, the only non-zero ones) for the next step.
 __global__ void __launch_bounds__(BS_T) bs_finish(View V, uint32_t* __restrict__ ccount,
+                                                  uint32_t* __restrict__ tcount,
                                                   const uint32_t* __restrict__ toff, uint32_t* __restrict__ coff,
                                                   uint2* __restrict__ cell_range, const uint32_t* __restrict__ tile_rank,
                                                   uint32_t* __restrict__ ptile_list, int cell_blocks) {
     const int lane = threadIdx.x & 31;
     if ((int)blockIdx.x < cell_blocks) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) tcount[V.total_ct] = 0u;
         const uint32_t ntiles = V.counters[CNT_CTILES];
         const uint32_t nwarps = (uint32_t)cell_blocks * (BS_T / 32);
         // first slot of each size class in the largest-first list
@@ -375,6 +390,7 @@ __global__ void __launch_bounds__(BS_T) bs_finish(View V, uint32_t* __restrict__
         }
         for (uint32_t w = (blockIdx.x * BS_T + threadIdx.x) >> 5; w < ntiles; w += nwarps) {
             const uint32_t t = V.ctile_list[w];
+            if (lane == 0) tcount[t] = 0u;
             if (ptile_list) {
                 const uint32_t tr = tile_rank[w];
                 const uint32_t off = __shfl_sync(0xFFFFFFFFu, cls_off, (int)(tr >> 28));
@@ -476,14 +492,15 @@ cudaError_t bin_sort_step(const View& V, const BinSortBufs& B, int num_sms, cuda
     const int nb = (int)bin_sort_scan_blocks(V.total_ct);
     const int gk = (int)((n + BS_TILE - 1) / BS_TILE);
     bs_count<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.ccount, B.tcount, B.slot, V.counters);
-    bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, ntb, B.bsum);
-    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, B.bsum, B.toff, B.ccount + ncells,
+    const bool direct = nb <= BS_DIRECT_BLOCKS;
+    if (!direct) bs_reduce<<<nb, BS_SCAN, 0, st>>>(B.tcount, ntb, B.bsum);
+    bs_down<<<nb, BS_SCAN, 0, st>>>(V, B.tcount, ntb, direct ? nullptr : B.bsum, B.toff, B.ccount + ncells,
                                     B.ptile_list ? B.tile_rank : nullptr);
     const int cell_blocks = num_sms * 2;
     // sparse grids mark their node tiles from the occupied cell tiles
     const int node_blocks = V.sp.cap ? 0 : (V.total_nt + BS_T - 1) / BS_T;
-    bs_finish<<<cell_blocks + node_blocks, BS_T, 0, st>>>(V, B.ccount, B.toff, B.coff, B.cell_range, B.tile_rank,
-                                                           B.ptile_list, cell_blocks);
+    bs_finish<<<cell_blocks + node_blocks, BS_T, 0, st>>>(V, B.ccount, B.tcount, B.toff, B.coff, B.cell_range,
+                                                           B.tile_rank, B.ptile_list, cell_blocks);
     bs_scatter<<<gk, BS_T, 0, st>>>(B.keys_in, n, ncells, B.slot, B.coff, B.toff + V.total_ct, B.out_k, B.out_v);
     return cudaGetLastError();
 }
