@@ -150,51 +150,60 @@ __global__ void __launch_bounds__(GATHER_T, 3) k_adj_gather(View V, AdjView A) {
             Y[a] = (gj >> 2) * (sc.nt[0] << 6) + ((gj & 3) << 2);
             Z[a] = (gk >> 2) * ((sc.nt[0] * sc.nt[1]) << 6) + ((gk & 3) << 4) + (sc.nt_base << 6);
         }
+        // The node loop keeps the x, y components of its 3-vectors as float2
+        // pairs and z alone.  In wb = v . h1 + gp . h2 + m gm the loaded
+        // (v_z, m_i) and (gp_z, gm_i) pairs meet (h1_z, 0) and (h2_z, m), so
+        // wb is four pair operations and one add.
+        const float2 G0a = make_float2(Gp[0], Gp[3]), G0b = make_float2(Gp[6], 0.f);  // Gp column 0
+        const float2 A0a = make_float2(Ap[0], Ap[3]), A0b = make_float2(Ap[6], 0.f);  // Ap column 0
         float ox[3] = {gx[0], gx[1], gx[2]};
-        float SWv[3] = {0.f, 0.f, 0.f}, SWg[3] = {0.f, 0.f, 0.f};
-        float Sg[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};  // [axis b][a] = sum w gp_a o_b
+        // sums over the stencil: (x, y) pairs and z scalars
+        float2 SWva = f2(0.f), SWga = f2(0.f), Sg0a = f2(0.f), Sg1a = f2(0.f), Sg2a = f2(0.f);
+        float SWvz = 0.f, SWgz = 0.f, Sg0z = 0.f, Sg1z = 0.f, Sg2z = 0.f;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                float h1[3], h2[3];
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    h1[a] = b1[a] + (float)j * Gp[3 * a + 1] + (float)k * Gp[3 * a + 2];
-                    h2[a] = b2[a] + (float)j * Ap[3 * a + 1] + (float)k * Ap[3 * a + 2];
-                }
+                const float fj = (float)j, fk = (float)k;
+                float2 H1a = make_float2(b1[0] + fj * Gp[1] + fk * Gp[2], b1[1] + fj * Gp[4] + fk * Gp[5]);
+                float2 H1b = make_float2(b1[2] + fj * Gp[7] + fk * Gp[8], 0.f);
+                float2 H2a = make_float2(b2[0] + fj * Ap[1] + fk * Ap[2], b2[1] + fj * Ap[4] + fk * Ap[5]);
+                float2 H2b = make_float2(b2[2] + fj * Ap[7] + fk * Ap[8], m);
                 float P0 = 0.f, P1 = 0.f;
-                float rv[3] = {0.f, 0.f, 0.f}, rg[3] = {0.f, 0.f, 0.f}, rgx[3] = {0.f, 0.f, 0.f};
+                float2 RVa = f2(0.f), RGa = f2(0.f), RXa = f2(0.f);
+                float RVz = 0.f, RGz = 0.f, RXz = 0.f;
                 const int row = Y[j] + Z[k];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     const int64_t n = (int64_t)(row + X[i]);
                     const float4 vi = __ldg(&V.grid_v[n]);
                     const float4 gpm = A.grid_gpm[n];
-                    const float wb = m * gpm.w + vi.x * h1[0] + vi.y * h1[1] + vi.z * h1[2] + gpm.x * h2[0] +
-                                     gpm.y * h2[1] + gpm.z * h2[2];
+                    const float2 Va = make_float2(vi.x, vi.y), Vb = make_float2(vi.z, vi.w);
+                    const float2 Ga = make_float2(gpm.x, gpm.y), Gb = make_float2(gpm.z, gpm.w);
+                    float2 wb2 = f2_mul(Va, H1a);
+                    wb2 = f2_fma(Vb, H1b, wb2);
+                    wb2 = f2_fma(Ga, H2a, wb2);
+                    wb2 = f2_fma(Gb, H2b, wb2);
+                    const float wb = wb2.x + wb2.y;
                     const float wx = st.w[0][i];
+                    const float2 W = f2(wx);
                     P0 += dw[0][i] * wb;
                     P1 += wx * wb;
-                    rv[0] += wx * vi.x;
-                    rv[1] += wx * vi.y;
-                    rv[2] += wx * vi.z;
-                    const float t0 = wx * gpm.x, t1 = wx * gpm.y, t2 = wx * gpm.z;
-                    rg[0] += t0;
-                    rg[1] += t1;
-                    rg[2] += t2;
+                    RVa = f2_fma(W, Va, RVa);
+                    RVz += wx * vi.z;
+                    const float2 Ta = f2_mul(W, Ga);
+                    const float Tz = wx * gpm.z;
+                    RGa = f2_add(RGa, Ta);
+                    RGz += Tz;
                     if (i) {
-                        const float fi = (float)i;
-                        rgx[0] += fi * t0;
-                        rgx[1] += fi * t1;
-                        rgx[2] += fi * t2;
+                        RXa = f2_fma(f2((float)i), Ta, RXa);
+                        RXz += (float)i * Tz;
                     }
                     if (i < 2) {
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            h1[a] += Gp[3 * a];
-                            h2[a] += Ap[3 * a];
-                        }
+                        H1a = f2_add(H1a, G0a);
+                        H1b = f2_add(H1b, G0b);
+                        H2a = f2_add(H2a, A0a);
+                        H2b = f2_add(H2b, A0b);
                     }
                 }
                 const float wyz = st.w[1][j] * st.w[2][k];
@@ -202,16 +211,27 @@ __global__ void __launch_bounds__(GATHER_T, 3) k_adj_gather(View V, AdjView A) {
                 ox[0] += P0 * R0;
                 ox[1] += P1 * R1;
                 ox[2] += P1 * R2;
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    SWv[a] += wyz * rv[a];
-                    SWg[a] += wyz * rg[a];
-                    Sg[0][a] += wyz * rgx[a];
-                    if (j) Sg[1][a] += ((float)j * wyz) * rg[a];
-                    if (k) Sg[2][a] += ((float)k * wyz) * rg[a];
+                const float2 WYZ = f2(wyz);
+                SWva = f2_fma(WYZ, RVa, SWva);
+                SWvz += wyz * RVz;
+                SWga = f2_fma(WYZ, RGa, SWga);
+                SWgz += wyz * RGz;
+                Sg0a = f2_fma(WYZ, RXa, Sg0a);
+                Sg0z += wyz * RXz;
+                if (j) {
+                    const float jw = fj * wyz;
+                    Sg1a = f2_fma(f2(jw), RGa, Sg1a);
+                    Sg1z += jw * RGz;
+                }
+                if (k) {
+                    const float kw = fk * wyz;
+                    Sg2a = f2_fma(f2(kw), RGa, Sg2a);
+                    Sg2z += kw * RGz;
                 }
             }
         }
+        const float SWv[3] = {SWva.x, SWva.y, SWvz}, SWg[3] = {SWga.x, SWga.y, SWgz};
+        const float Sg[3][3] = {{Sg0a.x, Sg0a.y, Sg0z}, {Sg1a.x, Sg1a.y, Sg1z}, {Sg2a.x, Sg2a.y, Sg2z}};
         float ogv[3], Ab[9];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {

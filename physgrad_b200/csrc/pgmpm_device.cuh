@@ -85,6 +85,15 @@ __device__ __forceinline__ float m3_det(const float A[9]) {
            A[2] * (A[3] * A[7] - A[4] * A[6]);
 }
 
+// ------------------------------------------------------ packed FP32 pairs
+// sm_100 issues an FP32 add, multiply or FMA on a pair of floats as one
+// instruction (per component the same rounding as the scalar operation), so
+// loops over 3-vectors keep two components per float2 and cut their FP issue.
+__device__ __forceinline__ float2 f2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
 // ------------------------------------------------------------ state packing
 __device__ __forceinline__ void unpack_xF(const float4 q0, const float4 q1, const float4 q2, float x[3], float F[9]) {
     x[0] = q0.x; x[1] = q0.y; x[2] = q0.z;
