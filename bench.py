@@ -192,11 +192,14 @@ class ClockSampler:
 
 
 # ------------------------------------------------------- reference CPU timing
-def reference_cpu_rate(st, scene, steps_per_thread, warmup=1, threads=None, sample_div=8):
+def reference_cpu_rate(st, scene, total_steps, warmup=1, threads=None):
     """The reference's own CPU solver (physgrad::mpm::MPMSolver<float,64>,
-    single-threaded by design) on `threads` host threads, each an
-    independent instance on a 1/sample_div particle sample of the workload on
-    the full grid.  Returns (particle-steps/s, threads, description)."""
+    single-threaded by design) on `threads` host threads: each thread runs an
+    independent instance of the whole workload (all particles, the full grid),
+    and the `total_steps` timed steps are split over the instances, so the
+    host's cores run the solver side by side.  Every instance first runs
+    max(1, warmup / threads) untimed steps (first touch of its arrays).
+    Returns (particle-steps/s, threads, description)."""
     import ctypes
 
     from oracle import pyoracle as O
@@ -208,29 +211,24 @@ def reference_cpu_rate(st, scene, steps_per_thread, warmup=1, threads=None, samp
                                  ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float]
     R.ref_mpm_step.argtypes = [vp, ctypes.c_int]
     R.ref_mpm_destroy.argtypes = [vp]
-    T = threads or min(os.cpu_count() or 1, 32)
+    T = max(1, min(threads or min(os.cpu_count() or 1, 32), total_steps))
     N = st["x"].shape[0]
-    handles, keep = [], []
+    x = np.ascontiguousarray(st["x"], np.float32)
+    v = np.ascontiguousarray(st["v"], np.float32)
+    m = np.ascontiguousarray(st["m"], np.float32)
+    V0 = np.ascontiguousarray(st["V0"], np.float32)
+    handles = []
     for t in range(T):
-        idx = np.arange(t % sample_div, N, sample_div)
-        x = np.ascontiguousarray(st["x"][idx], np.float32)
-        v = np.ascontiguousarray(st["v"][idx], np.float32)
-        m = np.ascontiguousarray(st["m"][idx], np.float32)
-        V0 = np.ascontiguousarray(st["V0"][idx], np.float32)
-        keep.append((x, v, m, V0))
-        h = R.ref_mpm_create(len(idx), x.ctypes.data, v.ctypes.data, m.ctypes.data, V0.ctypes.data,
+        h = R.ref_mpm_create(N, x.ctypes.data, v.ctypes.data, m.ctypes.data, V0.ctypes.data,
                              int(scene.n[0]), int(scene.n[1]), int(scene.n[2]), float(scene.dx), float(scene.dt),
                              float(scene.gravity[0]), float(scene.gravity[1]), float(scene.gravity[2]))
         if not h:
             raise RuntimeError("ref_mpm_create failed")
         handles.append(h)
-    ns = len(np.arange(0, N, sample_div))
+    per = [total_steps // T + (1 if t < total_steps % T else 0) for t in range(T)]
 
-    def run(h, k):
-        R.ref_mpm_step(h, k)
-
-    def par(k):
-        ths = [threading.Thread(target=run, args=(h, k)) for h in handles]
+    def par(ks):
+        ths = [threading.Thread(target=R.ref_mpm_step, args=(h, k)) for h, k in zip(handles, ks)]
         t0 = time.perf_counter()
         for th in ths:
             th.start()
@@ -238,15 +236,15 @@ def reference_cpu_rate(st, scene, steps_per_thread, warmup=1, threads=None, samp
             th.join()
         return time.perf_counter() - t0
 
-    if warmup:
-        par(warmup)
-    dt = par(steps_per_thread)
+    wu = max(1, -(-warmup // T))
+    par([wu] * T)
+    dt = par(per)
     for h in handles:
         R.ref_mpm_destroy(h)
-    rate = T * ns * steps_per_thread / dt
-    desc = (f"{T} independent reference MPMSolver<float,64> instances (single-threaded each), "
-            f"{ns} particles each (1/{sample_div} of the workload's particles) on the full "
-            f"{scene.n[0]}^3 grid, {steps_per_thread} steps each, wall {dt:.2f} s")
+    rate = N * total_steps / dt
+    desc = (f"{T} independent reference MPMSolver<float,64> instances (single-threaded each), each "
+            f"the whole workload ({N} particles on the {scene.n[0]}^3 grid); {total_steps} timed steps "
+            f"split over them ({min(per)}-{max(per)} each, after {wu} untimed), wall {dt:.2f} s")
     return rate, T, desc
 
 
@@ -405,7 +403,11 @@ def run_ours(args, rank, world, device):
         from oracle import pyoracle as O
 
         if O.ref_available():
-            rate, T, desc = reference_cpu_rate(st, scenes[0], steps_per_thread=60)
+            ncores = min(os.cpu_count() or 1, 32)
+            # batched workloads: the first scene (the reference solves one scene at a time)
+            n0 = int(counts[0])
+            st0 = {k: st[k][:n0] for k in ("x", "v", "m", "V0")}
+            rate, T, desc = reference_cpu_rate(st0, scenes[0], total_steps=2 * ncores, threads=ncores)
             cpu = {"value": rate, "unit": "particle-steps/s", "cores": T, "kind": "reference",
                    "sample": desc + "; physics = the reference CPU path (PIC, gravity, no stress)"}
     cfg = {"workload": meta.get("workload", args.workload), "n_particles": N, "n_scenes": len(scenes),
@@ -690,7 +692,9 @@ def run_reference(args):
     scenes, counts, mats, st, meta = make_workload(args.workload)
     N = int(sum(counts))
     rate_w, T, desc = None, None, None
-    rate, T, desc = reference_cpu_rate(st, scenes[0], steps_per_thread=args.steps, warmup=args.warmup)
+    n0 = int(counts[0])  # batched workloads: the first scene (the reference solves one scene at a time)
+    st0 = {k: st[k][:n0] for k in ("x", "v", "m", "V0")}
+    rate, T, desc = reference_cpu_rate(st0, scenes[0], total_steps=args.steps, warmup=args.warmup)
     line = {"impl": "reference", "metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
             "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform, same workload)",
