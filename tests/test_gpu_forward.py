@@ -79,16 +79,19 @@ def test_radix_sort_golden_fixture(gpu):
     assert np.array_equal(vo.cpu().numpy().view(np.uint32), g["order"])
 
 
+@pytest.mark.parametrize("n", [32, 264])
 @pytest.mark.parametrize("step_sort", ["radix", "bins"])
-def test_upload_order_and_step_sort_bit_exact(gpu, oracle, step_sort):
+def test_upload_order_and_step_sort_bit_exact(gpu, oracle, step_sort, n):
     """Upload order = stable sort of the keys.  Per step: the radix step sort
     reproduces the stable CPU sort exactly; the bin sort gives exactly the
     sorted keys and a permutation that realises them (particles sharing a
-    cell may come in any order)."""
+    cell may come in any order).  The 264^3 grid has 66^3 cell tiles, above
+    the 64 Ki tiles up to which the bin sort scans the tile counts in one
+    kernel, so it runs the two-kernel scan."""
     from physgrad_b200 import _capi as C
     from physgrad_b200 import workloads as W
 
-    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=20000, n=32, v_sigma=0.5, seed=3)
+    scenes, counts, mats, st, _ = W.elastic_cube(n_particles=20000, n=n, v_sigma=0.5, seed=3)
     sim = _sim(gpu, scenes, counts, mats, st)
     sim.set_step_sort(C.SORT_RADIX if step_sort == "radix" else C.SORT_BINS)
     osc = _oracle_scene(oracle, scenes[0])
