@@ -150,6 +150,15 @@ struct MPMPerformanceMetrics {
     int rejected_steps = 0;
     float average_particles_per_second = 0.0f;
     void reset() { *this = MPMPerformanceMetrics{}; }
+    // a summary on stdout (src/mpm_solver.h:92-100 has one of the same name)
+    void print() const {
+        const double t = total_simulation_time > 0.0 ? total_simulation_time : 1.0;
+        std::printf("MPM metrics: %d steps in %.6f s (%.4f ms per step), %.3f M particle-steps/s, %zu MB on the "
+                    "device; P2G %.1f%%, grid %.1f%%, G2P %.1f%%\n",
+                    total_steps, total_simulation_time, average_step_time * 1e3,
+                    average_particles_per_second / 1e6, total_memory_usage >> 20, 100.0 * p2g_time / t,
+                    100.0 * grid_update_time / t, 100.0 * g2p_time / t);
+    }
 };
 
 // Host copy of the particle state with the accessors of the reference's
