@@ -787,13 +787,115 @@ def run_hashgrid(args, device=0):
     return line
 
 
+def run_coupling(args, device=0):
+    """SPH-MPM contact coupling (pgmpm_sph_coupling, the reference's
+    SPHMPMCouplingSystem pair search + forces, src/sph_mpm_coupling.h:453-575)
+    and the FSI kinetic-energy monitor (pgmpm_kinetic_energy,
+    src/fsi_coupling.h:837-858) on config 2's particles as the MPM side
+    (2,097,152 particles, 128^3, uploaded state): 262,144 SPH particles seeded
+    uniform in a slab across the elastic block's top face, [0.2, 0.5] x
+    [0.49, 0.53] x [0.2, 0.5], contact radius 2 dx.  K calls timed with CUDA
+    events on device arrays; e2e through host arrays (SPH state in, forces
+    out).  CPU baseline: the reference's own class (oracle/_ref), whose pair
+    search tests every SPH x MPM pair, on a sample of SPH particles against all
+    MPM particles, one thread."""
+    import time
+
+    import torch
+
+    import physgrad_b200 as pg
+
+    torch.cuda.set_device(device)
+    scenes, counts, mats, st, meta = make_workload("cfg2")
+    N = int(sum(counts))
+    sim = pg.Simulator(scenes, counts, mats, device=device)
+    sim.upload(st["x"], st["v"], st["C"].reshape(N, 9), st["F"].reshape(N, 9), st["m"], st["V0"], st["mat"])
+    n_sph, r = 1 << 18, 2.0 / 128
+    rng = np.random.default_rng(11)
+    lo, hi = np.array([0.2, 0.49, 0.2]), np.array([0.5, 0.53, 0.5])
+    sx = (lo + (hi - lo) * rng.random((n_sph, 3))).astype(np.float32)
+    sv = rng.normal(0.0, 0.05, (n_sph, 3)).astype(np.float32)
+    dev = f"cuda:{device}"
+    dsx, dsv = torch.tensor(sx, device=dev), torch.tensor(sv, device=dev)
+    dsf = torch.zeros((n_sph, 3), dtype=torch.float32, device=dev)
+    dmf = torch.zeros((N, 3), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    kw = dict(stiffness=1e5, damping=1e3, friction=0.3, radius=r, two_way=True)
+    K = max(3, min(args.steps, 20))
+
+    def call():
+        dsf.zero_()
+        return sim.sph_coupling(dsx, dsv, dsf, dmf, stream=stream, **kw)
+
+    for _ in range(args.warmup):
+        _, _, npairs, energy = call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    # kinetic energy monitor
+    for _ in range(args.warmup):
+        sim.kinetic_energy(stream=stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        sim.kinetic_energy(stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ke_ms = e0.elapsed_time(e1) / K
+    # e2e: host SPH state in, host forces out
+    hsf, hmf = np.zeros((n_sph, 3), np.float32), np.zeros((N, 3), np.float32)
+    sim.sph_coupling(sx, sv, hsf, hmf, **kw)
+    t = []
+    for _ in range(3):
+        hsf[:] = 0.0
+        t0 = time.perf_counter()
+        sim.sph_coupling(sx, sv, hsf, hmf, **kw)
+        t.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(t))
+    line = {"metric": "SPH particles/s (SPH-MPM contact coupling)", "value": n_sph / (ms * 1e-3),
+            "unit": "SPH particles/s", "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (energy f64)",
+            "data": "synthetic (seeded uniform SPH slab over config 2's uploaded MPM state)",
+            "config": {"workload": "SPH-MPM contact coupling", "mpm_particles": N, "sph_particles": n_sph,
+                       "radius": r, "pairs": int(npairs), "grid": 128},
+            "pairs_per_s": npairs / (ms * 1e-3), "energy": energy,
+            "kinetic_energy_monitor": {"ms": ke_ms, "particles_per_s": N / (ke_ms * 1e-3)},
+            "e2e": {"value": n_sph / e2e_s, "unit": "SPH particles/s", "h2d_bytes_per_step": 2 * sx.nbytes + hsf.nbytes,
+                    "d2h_bytes_per_step": hsf.nbytes + hmf.nbytes,
+                    "call": "Simulator.sph_coupling with host arrays (pinned staging inside the library)"}}
+    try:
+        from oracle import pyoracle as O
+
+        if not args.no_cpu_baseline and O.ref_coupling_available():
+            out = sim.download()
+            # a sample of SPH particles that touch the block, against every MPM particle
+            near = np.nonzero(sx[:, 1] < 0.5 + r)[0]
+            ns = 256
+            pick = near[rng.choice(len(near), ns, replace=False)]
+            t0 = time.perf_counter()
+            O.ref_sph_coupling(sx[pick], sv[pick], out["x"], out["v"], **kw)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": ns / dt, "unit": "SPH particles/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{ns} SPH particles that touch the block against all {N} MPM "
+                                              f"particles (the reference tests every pair), wall {dt:.2f} s"}
+    except Exception as e:  # the baseline is optional
+        line["cpu_baseline"] = {"unavailable": str(e)[:120]}
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint", "hashgrid"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "cfg3_adjoint", "hashgrid",
+                                                       "coupling"])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="cfg4/cfg5: plain bench line instead of the batched comparison")
@@ -821,6 +923,8 @@ def main():
             line = run_adjoint(args, local)
         elif args.workload == "hashgrid" and world == 1:
             line = run_hashgrid(args, local)
+        elif args.workload == "coupling" and world == 1:
+            line = run_coupling(args, local)
         elif args.workload in ("cfg4", "cfg5") and world == 1 and not args.plain:
             line = run_batched(args, local, adjoint=args.workload == "cfg5")
         else:

@@ -115,24 +115,50 @@ __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restric
 }
 
 // m |v|^2 / 2 per particle, summed per material (FP64 accumulators)
+// Per-material sums of m |v|^2 / 2 in FP64.  Up to KE_REG_MATS materials each
+// thread keeps one register sum per material, and each warp adds its sums
+// with one atomic per material; with more, per-block shared-memory sums take
+// the particles' terms.  (One global atomic per particle on a handful of
+// addresses serialises: 3 ms for 2 M particles of two materials.)
+constexpr int KE_REG_MATS = 8;
+constexpr int KE_SMEM_MATS = 64;
+template <int MR>
 __global__ void k_kinetic(const float4* __restrict__ q, const float2* __restrict__ mV, const int32_t* __restrict__ mat,
                           int64_t N, int M, double* __restrict__ out) {
+    __shared__ double s_acc[KE_SMEM_MATS];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    double e0 = 0.0;
+    double acc[MR > 0 ? MR : 1];
+#pragma unroll
+    for (int m = 0; m < (MR > 0 ? MR : 1); ++m) acc[m] = 0.0;
+    if (MR == 0) {
+        for (int m = threadIdx.x; m < KE_SMEM_MATS; m += blockDim.x) s_acc[m] = 0.0;
+        __syncthreads();
+    }
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
         const float4 v = q[3 * N + p];
         const double ke = 0.5 * (double)mV[p].x * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
-        if (mat) {
-            const int id = min(max(mat[p], 0), M - 1);
-            atomicAdd(&out[id], ke);
+        const int id = mat ? min(max(mat[p], 0), M - 1) : 0;
+        if (MR > 0) {
+#pragma unroll
+            for (int m = 0; m < (MR > 0 ? MR : 1); ++m) acc[m] += id == m ? ke : 0.0;
+        } else if (M <= KE_SMEM_MATS) {
+            atomicAdd(&s_acc[id], ke);
         } else {
-            e0 += ke;
+            atomicAdd(&out[id], ke);
         }
     }
-    if (!mat) {
+    if (MR > 0) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) e0 += __shfl_down_sync(0xFFFFFFFFu, e0, o);
-        if ((threadIdx.x & 31) == 0 && e0 != 0.0) atomicAdd(&out[0], e0);
+        for (int m = 0; m < (MR > 0 ? MR : 1); ++m) {
+            double e = acc[m];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xFFFFFFFFu, e, o);
+            if ((threadIdx.x & 31) == 0 && e != 0.0 && m < M) atomicAdd(&out[m], e);
+        }
+    } else if (M <= KE_SMEM_MATS) {
+        __syncthreads();
+        for (int m = threadIdx.x; m < M; m += blockDim.x)
+            if (s_acc[m] != 0.0) atomicAdd(&out[m], s_acc[m]);
     }
 }
 
@@ -242,10 +268,22 @@ int pgmpm_kinetic_energy(pgmpm_solver s, double* per_material, double* total, vo
     const int M = s->M;
     CK(s->cpl_acc.ensure(sizeof(double) * std::max(2, M)));
     CK(cudaMemsetAsync(s->cpl_acc.p, 0, sizeof(double) * M, st));
-    if (s->N > 0)
-        k_kinetic<<<nblocks(s->N, 256, 148 * 8), 256, 0, st>>>(s->q.as<float4>(), s->mV.as<float2>(),
-                                                               s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr,
-                                                               s->N, M, s->cpl_acc.as<double>());
+    if (s->N > 0) {
+        const int nb = nblocks(s->N, 256, 148 * 8);
+        const int32_t* mt = s->pf.multi_mat ? s->mat.as<int32_t>() : nullptr;
+        if (!mt)
+            k_kinetic<1><<<nb, 256, 0, st>>>(s->q.as<float4>(), s->mV.as<float2>(), nullptr, s->N, M,
+                                             s->cpl_acc.as<double>());
+        else if (M <= 2)
+            k_kinetic<2><<<nb, 256, 0, st>>>(s->q.as<float4>(), s->mV.as<float2>(), mt, s->N, M,
+                                             s->cpl_acc.as<double>());
+        else if (M <= KE_REG_MATS)
+            k_kinetic<KE_REG_MATS><<<nb, 256, 0, st>>>(s->q.as<float4>(), s->mV.as<float2>(), mt, s->N, M,
+                                                       s->cpl_acc.as<double>());
+        else
+            k_kinetic<0><<<nb, 256, 0, st>>>(s->q.as<float4>(), s->mV.as<float2>(), mt, s->N, M,
+                                             s->cpl_acc.as<double>());
+    }
     CK(cudaGetLastError());
     std::vector<double> h(M);
     CK(cudaMemcpyAsync(h.data(), s->cpl_acc.p, sizeof(double) * M, cudaMemcpyDeviceToHost, st));

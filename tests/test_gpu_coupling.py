@@ -103,3 +103,31 @@ def test_kinetic_energy_matches_reference_monitor(gpu, oracle):
     assert np.allclose(per, ours, rtol=1e-9)
     assert abs(float(replay) - ref) <= 2 * np.spacing(np.float32(ref))
     assert abs(tot - ref) <= 1e-3 * ref
+
+
+@pytest.mark.parametrize("n_mats", [1, 5, 20, 70])
+def test_kinetic_energy_per_material_counts(gpu, oracle, n_mats):
+    """The monitor's per-material sums take three routes by the number of
+    materials (register sums up to 8, shared-memory sums up to 64, global
+    atomics above); each equals the FP64 oracle's sums to 1e-9, including
+    materials that no particle uses."""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, _, st, _ = W.elastic_cube(n_particles=50000, n=32, v_sigma=0.3, seed=12)
+    N = counts[0]
+    rng = np.random.default_rng(13)
+    mats = [gpu.createElasticMaterial(1000.0, 1e4 * (1 + 0.1 * k), 0.3) for k in range(n_mats)]
+    # the last material, if there are several, is left without particles
+    mat = rng.integers(0, max(1, n_mats - 1), N).astype(np.int32) if n_mats > 1 else None
+    sim = gpu.Simulator(scenes, counts, mats)
+    sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], mat)
+    sim.step(3)
+    out = sim.download()
+    per, tot = sim.kinetic_energy()
+    ref = oracle.kinetic_energy(out["v"].astype(np.float64), st["m"].astype(np.float64),
+                                mat if mat is not None else np.zeros(N, np.int32), n_mats)
+    assert per.shape == (n_mats,)
+    assert np.allclose(per, ref, rtol=1e-9, atol=1e-300)
+    if n_mats > 1:
+        assert per[-1] == 0.0
+    assert abs(tot - ref.sum()) <= 1e-9 * ref.sum()
