@@ -362,8 +362,9 @@ typedef struct {
  * are ADDED (as the reference adds them to SPHParticle::force), two-way only;
  * mpm_force [N][3] (may be NULL): overwritten with each particle's summed
  * solid force, upload order.  n_pairs, energy (sum of k (r - d)^2 / 2) may be
- * NULL.  Pairs are found through the spatial hash grid of this library with
- * a cell of one radius over the scene's grid domain.  Synchronises stream. */
+ * NULL.  Pairs are found through the spatial hash grid of this library over
+ * the scene's grid domain, with cells of half a radius (one radius when that
+ * would make more than max(4 N, 2^20) cells).  Synchronises stream. */
 PGMPM_API int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, const float* sph_x,
                                  const float* sph_v, int64_t n_sph, float* sph_force, float* mpm_force,
                                  int64_t* n_pairs, double* energy, int32_t ptr_kind, void* stream);

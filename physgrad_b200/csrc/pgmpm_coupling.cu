@@ -41,22 +41,28 @@ __global__ void k_state_xv(const float4* __restrict__ q, int64_t N, float* __res
 // damping, friction along the tangential velocity), the fluid force summed
 // into sph_force (two-way), the solid force into mpm_force (upload order),
 // the pair count and k (r - d)^2 / 2 summed over pairs.
+// One warp per SPH particle: the lanes take its candidates in turn (the
+// candidate list is read coalesced and the long lists of particles inside
+// the solid are shared by 32 lanes), and the warp sums the lanes' fluid
+// forces at the end.
 __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restrict__ sv, int64_t nq,
                             const int64_t* __restrict__ off, const uint32_t* __restrict__ cand,
                             const float* __restrict__ mx, const float* __restrict__ mv,
                             const uint32_t* __restrict__ user_of_phys, pgmpm_sph_coupling_config cfg,
                             float* __restrict__ sph_force, float* __restrict__ mpm_force,
                             unsigned long long* __restrict__ npairs, double* __restrict__ energy) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const float k = cfg.coupling_stiffness, c = cfg.coupling_damping, mu = cfg.friction_coefficient,
                 r = cfg.coupling_radius;
     unsigned long long cnt = 0;
     double e = 0.0;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nq; q += warps) {
         const float y0 = sx[3 * q], y1 = sx[3 * q + 1], y2 = sx[3 * q + 2];
         const float w0 = sv[3 * q], w1 = sv[3 * q + 1], w2 = sv[3 * q + 2];
         float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-        for (int64_t ci = off[q]; ci < off[q + 1]; ++ci) {
+        const int64_t end = off[q + 1];
+        for (int64_t ci = off[q] + lane; ci < end; ci += 32) {
             const uint32_t p = cand[ci];
             // distance as the reference forms it (no contraction)
             const float r0 = __fsub_rn(mx[3 * p], y0), r1 = __fsub_rn(mx[3 * p + 1], y1),
@@ -84,11 +90,9 @@ __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restric
                 s1 = __fadd_rn(s1, __fmul_rn(__fmul_rn(t1, it), fm));
                 s2 = __fadd_rn(s2, __fmul_rn(__fmul_rn(t2, it), fm));
             }
-            if (cfg.enable_two_way_coupling) {
-                f0 = __fadd_rn(f0, -s0);
-                f1 = __fadd_rn(f1, -s1);
-                f2 = __fadd_rn(f2, -s2);
-            }
+            f0 = __fadd_rn(f0, -s0);
+            f1 = __fadd_rn(f1, -s1);
+            f2 = __fadd_rn(f2, -s2);
             if (mpm_force) {
                 const uint32_t u = user_of_phys[p];
                 atomicAdd(&mpm_force[3 * (size_t)u], s0);
@@ -97,24 +101,31 @@ __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restric
             }
         }
         if (cfg.enable_two_way_coupling) {
-            sph_force[3 * q] += f0;
-            sph_force[3 * q + 1] += f1;
-            sph_force[3 * q + 2] += f2;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                f0 += __shfl_down_sync(0xFFFFFFFFu, f0, o);
+                f1 += __shfl_down_sync(0xFFFFFFFFu, f1, o);
+                f2 += __shfl_down_sync(0xFFFFFFFFu, f2, o);
+            }
+            if (lane == 0) {
+                sph_force[3 * q] += f0;
+                sph_force[3 * q + 1] += f1;
+                sph_force[3 * q + 2] += f2;
+            }
         }
     }
-    // block sums of the pair count and the energy, one atomic each per warp
+    // warp sums of the pair count and the energy, one atomic each per warp
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
         e += __shfl_down_sync(0xFFFFFFFFu, e, o);
     }
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         if (cnt) atomicAdd(npairs, cnt);
         if (e != 0.0) atomicAdd(energy, e);
     }
 }
 
-// m |v|^2 / 2 per particle, summed per material (FP64 accumulators)
 // Per-material sums of m |v|^2 / 2 in FP64.  Up to KE_REG_MATS materials each
 // thread keeps one register sum per material, and each warp adds its sums
 // with one atomic per material; with more, per-block shared-memory sums take
@@ -213,20 +224,27 @@ int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, con
     unsigned long long* d_pairs = s->cpl_acc.as<unsigned long long>();
     double* d_energy = s->cpl_acc.as<double>() + 1;
     if (N > 0 && n_sph > 0) {
-        // candidates: the MPM particles of the 27 hash cells (of one radius)
-        // around each SPH particle, over the scene's domain
+        // candidates: the MPM particles of the hash cells within one radius
+        // of each SPH particle, over the scene's domain.  Cells of half a
+        // radius (125 around a particle) hold 42% fewer candidates than cells
+        // of one radius (27), unless that makes more than 4 cells per MPM
+        // particle (or 2^20, if more).
         const pgmpm_scene_desc& d = s->desc[0];
-        if (!s->cpl_grid || s->cpl_cell != cfg->coupling_radius || s->cpl_cap < N) {
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = d.origin[a];
+            hi[a] = d.origin[a] + (float)(d.n[a] - 1) * d.dx;
+        }
+        double cells_half = 1.0;
+        for (int a = 0; a < 3; ++a) cells_half *= std::ceil((hi[a] - lo[a]) / (0.5 * cfg->coupling_radius));
+        const float cell = cells_half <= std::max(4.0 * (double)N, (double)(1 << 20)) ? 0.5f * cfg->coupling_radius
+                                                                                      : cfg->coupling_radius;
+        if (!s->cpl_grid || s->cpl_cell != cell || s->cpl_cap < N) {
             if (s->cpl_grid) pgmpm_hashgrid_destroy(s->cpl_grid);
             s->cpl_grid = nullptr;
-            float lo[3], hi[3];
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = d.origin[a];
-                hi[a] = d.origin[a] + (float)(d.n[a] - 1) * d.dx;
-            }
-            int rc = pgmpm_hashgrid_create(cfg->coupling_radius, lo, hi, N, s->device, &s->cpl_grid);
+            int rc = pgmpm_hashgrid_create(cell, lo, hi, N, s->device, &s->cpl_grid);
             if (rc) return rc;
-            s->cpl_cell = cfg->coupling_radius;
+            s->cpl_cell = cell;
             s->cpl_cap = N;
         }
         int rc = pgmpm_hashgrid_build(s->cpl_grid, mx, N, PGMPM_PTR_DEVICE, stream);
@@ -240,7 +258,7 @@ int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, con
         rc = pgmpm_hashgrid_neighbors(s->cpl_grid, dsx, n_sph, cfg->coupling_radius, s->cpl_off.as<int64_t>(),
                                       s->cpl_idx.as<uint32_t>(), total, &total, PGMPM_PTR_DEVICE, stream);
         if (rc) return rc;
-        k_sph_pairs<<<nblocks(n_sph, 128, 148 * 16), 128, 0, st>>>(
+        k_sph_pairs<<<nblocks(n_sph * 32, 256, 148 * 16), 256, 0, st>>>(
             dsx, dsv, n_sph, s->cpl_off.as<int64_t>(), s->cpl_idx.as<uint32_t>(), mx, mv,
             s->user_of_phys.as<uint32_t>(), *cfg, dsf, dmf, d_pairs, d_energy);
         CK(cudaGetLastError());
