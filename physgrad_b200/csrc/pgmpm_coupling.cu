@@ -23,16 +23,32 @@ using namespace pgmpm;
 namespace {
 
 // positions and velocities of the state (physical order) as [N][3]
+// physical-order float4 sums -> the caller's [N][3] array in upload order
+__global__ void k_mforce_out(const float4* __restrict__ mf, const uint32_t* __restrict__ user_of_phys, int64_t N,
+                             float* __restrict__ out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        const float4 f = mf[p];
+        const size_t u = user_of_phys[p];
+        out[3 * u] = f.x;
+        out[3 * u + 1] = f.y;
+        out[3 * u + 2] = f.z;
+    }
+}
+
 __global__ void k_state_xv(const float4* __restrict__ q, int64_t N, float* __restrict__ x, float* __restrict__ v) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
-        const float4 a = q[p], b = q[3 * N + p];
+        const float4 a = q[p];
         x[3 * p] = a.x;
         x[3 * p + 1] = a.y;
         x[3 * p + 2] = a.z;
-        v[3 * p] = b.x;
-        v[3 * p + 1] = b.y;
-        v[3 * p + 2] = b.z;
+        if (v) {
+            const float4 b = q[3 * N + p];
+            v[3 * p] = b.x;
+            v[3 * p + 1] = b.y;
+            v[3 * p + 2] = b.z;
+        }
     }
 }
 
@@ -45,11 +61,13 @@ __global__ void k_state_xv(const float4* __restrict__ q, int64_t N, float* __res
 // candidate list is read coalesced and the long lists of particles inside
 // the solid are shared by 32 lanes), and the warp sums the lanes' fluid
 // forces at the end.
+// The MPM side is read from the state planes (x from plane 0, v from plane
+// 3, one 16-byte load each), and each pair's solid force is added to
+// mforce[p] (physical order, float4) with one vector atomic.
 __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restrict__ sv, int64_t nq,
                             const int64_t* __restrict__ off, const uint32_t* __restrict__ cand,
-                            const float* __restrict__ mx, const float* __restrict__ mv,
-                            const uint32_t* __restrict__ user_of_phys, pgmpm_sph_coupling_config cfg,
-                            float* __restrict__ sph_force, float* __restrict__ mpm_force,
+                            const float4* __restrict__ state, int64_t N, pgmpm_sph_coupling_config cfg,
+                            float* __restrict__ sph_force, float4* __restrict__ mforce,
                             unsigned long long* __restrict__ npairs, double* __restrict__ energy) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -64,9 +82,9 @@ __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restric
         const int64_t end = off[q + 1];
         for (int64_t ci = off[q] + lane; ci < end; ci += 32) {
             const uint32_t p = cand[ci];
+            const float4 xp = state[p];
             // distance as the reference forms it (no contraction)
-            const float r0 = __fsub_rn(mx[3 * p], y0), r1 = __fsub_rn(mx[3 * p + 1], y1),
-                        r2 = __fsub_rn(mx[3 * p + 2], y2);
+            const float r0 = __fsub_rn(xp.x, y0), r1 = __fsub_rn(xp.y, y1), r2 = __fsub_rn(xp.z, y2);
             const float d = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2)));
             if (!(d < r)) continue;
             ++cnt;
@@ -75,8 +93,8 @@ __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restric
             if (d < 1e-6f) continue;
             const float inv = __fdiv_rn(1.f, d);
             const float n0 = __fmul_rn(r0, inv), n1 = __fmul_rn(r1, inv), n2 = __fmul_rn(r2, inv);
-            const float d0 = __fsub_rn(mv[3 * p], w0), d1 = __fsub_rn(mv[3 * p + 1], w1),
-                        d2 = __fsub_rn(mv[3 * p + 2], w2);
+            const float4 vp = state[3 * N + p];
+            const float d0 = __fsub_rn(vp.x, w0), d1 = __fsub_rn(vp.y, w1), d2 = __fsub_rn(vp.z, w2);
             const float fn = __fmul_rn(k, pen);
             const float vn = __fadd_rn(__fadd_rn(__fmul_rn(d0, n0), __fmul_rn(d1, n1)), __fmul_rn(d2, n2));
             const float ft = __fadd_rn(fn, __fmul_rn(c, vn));
@@ -93,12 +111,7 @@ __global__ void k_sph_pairs(const float* __restrict__ sx, const float* __restric
             f0 = __fadd_rn(f0, -s0);
             f1 = __fadd_rn(f1, -s1);
             f2 = __fadd_rn(f2, -s2);
-            if (mpm_force) {
-                const uint32_t u = user_of_phys[p];
-                atomicAdd(&mpm_force[3 * (size_t)u], s0);
-                atomicAdd(&mpm_force[3 * (size_t)u + 1], s1);
-                atomicAdd(&mpm_force[3 * (size_t)u + 2], s2);
-            }
+            if (mforce) atomicAdd(&mforce[p], make_float4(s0, s1, s2, 0.f));
         }
         if (cfg.enable_two_way_coupling) {
 #pragma unroll
@@ -194,11 +207,11 @@ int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, con
     cudaStream_t st = ST(stream);
     const int64_t N = s->N;
     const size_t Nz = (size_t)std::max<int64_t>(N, 1), Qz = (size_t)std::max<int64_t>(n_sph, 1);
-    // the MPM side: current positions and velocities (physical order)
-    CK(s->cpl_xv.ensure(sizeof(float) * 6 * Nz));
+    // the MPM side: current positions (physical order, [N][3]) for the hash
+    // grid build; the pair kernel reads the state planes
+    CK(s->cpl_xv.ensure(sizeof(float) * 3 * Nz));
     float* mx = s->cpl_xv.as<float>();
-    float* mv = mx + 3 * Nz;
-    if (N > 0) k_state_xv<<<nblocks(N, 256, 148 * 16), 256, 0, st>>>(s->q.as<float4>(), N, mx, mv);
+    if (N > 0) k_state_xv<<<nblocks(N, 256, 148 * 16), 256, 0, st>>>(s->q.as<float4>(), N, mx, nullptr);
     CK(cudaGetLastError());
     // the SPH side on the device
     const float *dsx = sph_x, *dsv = sph_v;
@@ -218,7 +231,12 @@ int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, con
         dsf = b + 6 * Qz;
         dmf = mpm_force ? b + 9 * Qz : nullptr;
     }
-    if (dmf && N > 0) CK(cudaMemsetAsync(dmf, 0, sizeof(float) * 3 * N, st));
+    float4* mf = nullptr;  // the solid forces, physical order
+    if (dmf && N > 0) {
+        CK(s->cpl_mf.ensure(sizeof(float4) * Nz));
+        mf = s->cpl_mf.as<float4>();
+        CK(cudaMemsetAsync(mf, 0, sizeof(float4) * N, st));
+    }
     CK(s->cpl_acc.ensure(sizeof(double) * 2));
     CK(cudaMemsetAsync(s->cpl_acc.p, 0, sizeof(double) * 2, st));
     unsigned long long* d_pairs = s->cpl_acc.as<unsigned long long>();
@@ -259,10 +277,13 @@ int pgmpm_sph_coupling(pgmpm_solver s, const pgmpm_sph_coupling_config* cfg, con
                                       s->cpl_idx.as<uint32_t>(), total, &total, PGMPM_PTR_DEVICE, stream);
         if (rc) return rc;
         k_sph_pairs<<<nblocks(n_sph * 32, 256, 148 * 16), 256, 0, st>>>(
-            dsx, dsv, n_sph, s->cpl_off.as<int64_t>(), s->cpl_idx.as<uint32_t>(), mx, mv,
-            s->user_of_phys.as<uint32_t>(), *cfg, dsf, dmf, d_pairs, d_energy);
+            dsx, dsv, n_sph, s->cpl_off.as<int64_t>(), s->cpl_idx.as<uint32_t>(), s->q.as<float4>(), N, *cfg, dsf, mf,
+            d_pairs, d_energy);
         CK(cudaGetLastError());
     }
+    if (mf)
+        k_mforce_out<<<nblocks(N, 256, 148 * 16), 256, 0, st>>>(mf, s->user_of_phys.as<uint32_t>(), N, dmf);
+    CK(cudaGetLastError());
     if (ptr_kind == PGMPM_PTR_HOST) {
         if (cfg->enable_two_way_coupling && n_sph > 0)
             CK(cudaMemcpyAsync(sph_force, dsf, sizeof(float) * 3 * n_sph, cudaMemcpyDeviceToHost, st));

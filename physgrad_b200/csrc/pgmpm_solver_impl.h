@@ -123,7 +123,7 @@ struct pgmpm_solver_s {
     int sp_shift = 0;
     // consumers (pgmpm_coupling.cu): particle x and v, host staging, the
     // candidate hash grid and lists, the pair count and energy sums
-    pgmpm::DevBuf cpl_xv, cpl_stage, cpl_off, cpl_idx, cpl_acc;
+    pgmpm::DevBuf cpl_xv, cpl_stage, cpl_off, cpl_idx, cpl_acc, cpl_mf;
     pgmpm_hashgrid cpl_grid = nullptr;
     float cpl_cell = 0.f;
     int64_t cpl_cap = 0;
