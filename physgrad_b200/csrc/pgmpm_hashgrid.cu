@@ -176,8 +176,22 @@ __global__ void k_hg_qfill(HGDev G, const float* __restrict__ q, int64_t nq, uin
             const uint32_t y = __shfl_up_sync(gmask, x, d, HG_FG);
             if (sub >= d) x += y;
         }
-        const int64_t base = o + (x - k);
-        for (uint32_t j = 0; j < k; ++j) out[base + j] = sorted_index[s0 + j];
+        const uint32_t kmax = __reduce_max_sync(gmask, k);
+        if (kmax < 2 * HG_FG) {
+            // short cells: each lane copies its own cell's entries
+            const int64_t base = o + (x - k);
+            for (uint32_t j = 0; j < k; ++j) out[base + j] = sorted_index[s0 + j];
+        } else {
+            // long cells: the query's lanes copy each cell together, so the
+            // list is written (and the sorted index read) in runs
+#pragma unroll 1
+            for (int m = 0; m < HG_FG; ++m) {
+                const uint32_t km = __shfl_sync(gmask, k, m, HG_FG);
+                const uint32_t sm = __shfl_sync(gmask, s0, m, HG_FG);
+                const int64_t bm = o + (__shfl_sync(gmask, x, m, HG_FG) - km);
+                for (uint32_t j = (uint32_t)sub; j < km; j += HG_FG) out[bm + j] = sorted_index[sm + j];
+            }
+        }
         o += __shfl_sync(gmask, x, HG_FG - 1, HG_FG);
     }
 }
