@@ -56,7 +56,7 @@
 extern "C" {
 #endif
 
-#define PGMPM_ABI_VERSION 4
+#define PGMPM_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define PGMPM_API __attribute__((visibility("default")))
@@ -278,6 +278,22 @@ PGMPM_API int pgmpm_get_metrics(pgmpm_solver s, pgmpm_metrics* out);
 /* Run n_steps from the current state, storing the state every
  * checkpoint_every steps, so that pgmpm_backward can differentiate them. */
 PGMPM_API int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoint_every, void* stream);
+/* on != 0 (the default): a pgmpm_forward_checkpointed with the bin sort and
+ * split steps records every step's sort (order, tile lists and cell ranges)
+ * and keys, about 12 bytes per particle + 530 bytes per cell tile per step,
+ * when the tape and the record take at most 1/16 of the device memory and
+ * leave a quarter of it free.  pgmpm_backward's replays
+ * then keep the recorded sorts instead of sorting again; a replayed step
+ * sorts again only when the previous step's G2P, rounding differently from
+ * the forward, put a particle in another cell.  Takes effect at the next
+ * pgmpm_forward_checkpointed.  on = 2 records too, but every replayed step
+ * after a segment's first sorts again (a check of that path: the gradients
+ * are those of on = 0).  No reference counterpart (the reference keeps no
+ * sort). */
+PGMPM_API int pgmpm_set_sort_record(pgmpm_solver s, int32_t on);
+/* Replayed steps that sorted again (see pgmpm_set_sort_record) over the
+ * solver's life; waits for the device.  No reference counterpart. */
+PGMPM_API int pgmpm_get_replay_resorts(pgmpm_solver s, int64_t* steps);
 /* Reverse pass over the last pgmpm_forward_checkpointed call.  g*_out: dL/d
  * of the final state (upload order, any may be NULL = 0).  g*_in: receives
  * dL/d of the initial state (any may be NULL).  gE [n_materials]: dL/dE per

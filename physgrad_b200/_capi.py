@@ -192,6 +192,8 @@ SIGNATURES = {
     "pgmpm_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
     "pgmpm_set_kernel_variants": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
     "pgmpm_set_step_sort": (ctypes.c_int, [_vp, _i32]),
+    "pgmpm_set_sort_record": (ctypes.c_int, [_vp, _i32]),
+    "pgmpm_get_replay_resorts": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "pgmpm_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "pgmpm_get_metrics": (ctypes.c_int, [_vp, ctypes.POINTER(Metrics)]),
     "pgmpm_forward_checkpointed": (ctypes.c_int, [_vp, _i32, _i32, _vp]),

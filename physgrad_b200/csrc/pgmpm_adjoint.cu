@@ -21,6 +21,10 @@ namespace {
 __device__ __forceinline__ const SceneDev& scene_ref(const View& V, int s) { return V.scenes[s]; }
 
 __global__ void k_adj_grid(View V, AdjView A) {
+    // the scatter has finished with the work cursor: leave it at zero, as the
+    // forward's grid update does, so that a later replay of this step that
+    // keeps its recorded sort (no counter reset) starts its P2G from zero
+    if (blockIdx.x == 0 && threadIdx.x == 0) V.counters[CNT_P2G_CURSOR] = 0u;
     const uint32_t count = V.counters[CNT_TILES];
     const int tiles_per_block = blockDim.x >> 6;
     const int l = threadIdx.x & 63;

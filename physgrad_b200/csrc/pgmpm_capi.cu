@@ -105,6 +105,51 @@ int refresh_payload(pgmpm_solver s, cudaStream_t st) {
     return PGMPM_OK;
 }
 
+// Sets the condition of a conditional graph node from *flag (or to 1 when
+// always), clears the flag and counts the steps that sort again in *count
+// (one thread).
+__global__ void k_resort_cond(cudaGraphConditionalHandle h, uint32_t* flag, uint32_t* count, int always) {
+    const uint32_t f = *flag | (always ? 1u : 0u);
+    *flag = 0u;
+    if (f) *count += 1u;
+    cudaGraphSetConditional(h, f ? 1u : 0u);
+}
+
+// Under stream capture on st: the bin sort as the body of an IF node whose
+// condition k_resort_cond takes from *flag, so that a replayed step sorts
+// only when its G2P found a key that differs from the recorded one.
+int conditional_sort(pgmpm_solver s, const View& V, const BinSortBufs& B, uint32_t* flag, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+    if (cs != cudaStreamCaptureStatusActive || !g)
+        return fail(PGMPM_ERR_STATE, "internal: a conditional sort needs a stream capture");
+    if (!s->body_stream) CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    k_resort_cond<<<1, 1, 0, st>>>(h, flag, s->rec_resort.as<uint32_t>() + 2, s->rec_mode == 2 ? 1 : 0);
+    CK(cudaGetLastError());
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t cn = nullptr;
+    CK(cudaGraphAddNode(&cn, g, deps, nd, &np));
+    CK(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t e = bin_sort_step(V, B, s->num_sms, s->body_stream);
+    cudaGraph_t out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s->body_stream, &out);
+    CK(e);
+    CK(e2);
+    return PGMPM_OK;
+}
+
 int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, bool write_vc, StepKind kind) {
     if (s->N == 0) {  // nothing to move; keep the timing events consistent
         if (timed)
@@ -113,6 +158,8 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, 
     }
     if (kind != STEP_SPLIT && !(s->pf.physics == PHYS_MLS && s->tune.step_sort == 0))
         return fail(PGMPM_ERR_STATE, "internal: fused step without the bin sort");
+    if (b.sort_mode != 0 && (s->tune.step_sort != 0 || kind != STEP_SPLIT || (b.sort_mode == 2 && !b.resort)))
+        return fail(PGMPM_ERR_STATE, "internal: a recorded sort needs the bin sort and split steps");
     View V = s->view_for(b);
     // P2G variant 1 builds its payload from the state's v and C
     V.write_vc = write_vc || s->pf.physics != PHYS_MLS || s->tune.p2g_variant == 1 ? 1 : 0;
@@ -139,7 +186,12 @@ int record_step(pgmpm_solver s, const StepBufs& b, cudaStream_t st, bool timed, 
         B.cell_range = b.cell_range;
         B.ptile_list = b.ptile_list;
         B.tile_rank = s->tile_rank.as<uint32_t>();
-        CK(bin_sort_step(V, B, s->num_sms, st));
+        if (b.sort_mode == 0) {
+            CK(bin_sort_step(V, B, s->num_sms, st));
+        } else if (b.sort_mode == 2) {
+            int rc = conditional_sort(s, V, B, b.resort, st);
+            if (rc) return rc;
+        }
     } else {
         int which = 0;
         CK(radix_sort_pairs(b.keys_in, nullptr, b.ka, b.va, b.kb, b.vb, s->sort_scratch.as<uint32_t>(), s->N,
@@ -805,6 +857,25 @@ int pgmpm_set_kernel_variants(pgmpm_solver s, int32_t p2g_variant, int32_t g2p_v
     }
     if (g2p_tiles_per_sm > 0) s->tune.g2p_tiles_per_sm = g2p_tiles_per_sm;
     s->drop_graph();
+    return PGMPM_OK;
+}
+
+int pgmpm_set_sort_record(pgmpm_solver s, int32_t on) {
+    if (!s) return fail(PGMPM_ERR_ARG, "null solver");
+    if (on < 0 || on > 2) return fail(PGMPM_ERR_ARG, "on must be 0, 1 or 2");
+    s->rec_mode = on;  // from the next pgmpm_forward_checkpointed on
+    s->drop_tape_graphs();
+    return PGMPM_OK;
+}
+
+int pgmpm_get_replay_resorts(pgmpm_solver s, int64_t* steps) {
+    if (!s || !steps) return fail(PGMPM_ERR_ARG, "null argument");
+    *steps = 0;
+    if (!s->rec_resort.p) return PGMPM_OK;
+    DeviceGuard dg(s->device);
+    uint32_t c = 0;
+    CK(cudaMemcpy(&c, s->rec_resort.as<uint32_t>() + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    *steps = c;
     return PGMPM_OK;
 }
 

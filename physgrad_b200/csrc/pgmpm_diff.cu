@@ -32,24 +32,39 @@ namespace {
 
 size_t nodes_of(pgmpm_solver s) { return (size_t)s->total_nt * 64; }
 
-int ensure_tape(pgmpm_solver s, int slots) {
+// Bytes one forward step adds to the record: sorted keys, order and the next
+// keys per particle, node-tile flags and list, cell-tile list and ranges,
+// cell ranges and the largest-first list, counters.
+size_t rec_step_bytes(pgmpm_solver s) {
+    const size_t N = (size_t)std::max<int64_t>(s->N, 1);
+    const size_t ct = std::max<size_t>((size_t)s->total_ct, 1);
+    return 12 * N + 8 * (size_t)s->total_nt + ct * (4 + 8 + 8 * 64 + 4) + 4 * CNT_WORDS;
+}
+
+// The tape: `slots` steps per set (states, keys, grid), and per-step sort
+// outputs for max(slots x sets, rec) steps (rec > 0: the recorded forward's
+// steps, indexed by forward step).
+int ensure_tape(pgmpm_solver s, int slots, int rec = 0) {
     const int sets = s->bs_ccount.p ? 2 : 1;  // the overlapped backward needs the bin sort
-    if (s->tape_slots >= slots && s->tape_sets == sets && s->tape_q.p) return PGMPM_OK;
+    if (s->tape_slots >= slots && s->tape_sets == sets && s->tape_q.p && s->tape_rec >= rec) return PGMPM_OK;
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
     const size_t nodes = nodes_of(s);
-    const size_t ss = (size_t)slots * sets;  // slots over all sets
+    const size_t gs = (size_t)slots * sets;           // grid slots over all sets
+    const size_t ss = std::max(gs, (size_t)rec);      // per-step sort slots
     s->tape_slots = 0;
     s->tape_sets = 0;
+    s->tape_rec = 0;
     s->tape_has_last = false;
     s->tape_has_prev = false;
+    s->ck_rec = false;      // the record goes with the old tape (the checkpoints stay)
     s->drop_tape_graphs();  // they hold the old tape's addresses
     CK(s->tape_q.alloc(sizeof(float4) * 6 * N * (slots + 1) * sets));
     CK(s->tape_keys.alloc(sizeof(uint32_t) * N * (slots + 1) * sets));
     if (s->pf.physics == PHYS_MLS) CK(s->tape_pay.alloc(sizeof(float4) * 4 * N));
     CK(s->tape_sk.alloc(sizeof(uint32_t) * N * ss));
     CK(s->tape_ord.alloc(sizeof(uint32_t) * N * ss));
-    CK(s->tape_gv.alloc(sizeof(float4) * nodes * ss));
-    CK(s->tape_gvpre.alloc(sizeof(float4) * nodes * ss));
+    CK(s->tape_gv.alloc(sizeof(float4) * nodes * gs));
+    CK(s->tape_gvpre.alloc(sizeof(float4) * nodes * gs));
     CK(s->tape_flags.alloc(sizeof(uint32_t) * (size_t)s->total_nt * ss));
     CK(s->tape_tiles.alloc(sizeof(uint32_t) * (size_t)s->total_nt * ss));
     CK(s->tape_ctiles.alloc(sizeof(uint32_t) * (size_t)s->total_ct * ss));
@@ -60,27 +75,29 @@ int ensure_tape(pgmpm_solver s, int slots) {
         CK(s->tape_cells.alloc(sizeof(uint2) * 64 * std::max<size_t>((size_t)s->total_ct, 1) * ss));
         CK(s->tape_ptile.alloc(sizeof(uint32_t) * std::max<size_t>((size_t)s->total_ct, 1) * ss));
     }
+    if (rec) {
+        CK(s->rec_keys.alloc(sizeof(uint32_t) * N * ((size_t)rec + 1)));
+        // [0], [1]: a replayed key changed (per tape set); [2]: replayed steps
+        // that sorted again, kept across tapes
+        if (!s->rec_resort.p) {
+            CK(s->rec_resort.alloc(sizeof(uint32_t) * 4));
+            CK(cudaMemset(s->rec_resort.p, 0, s->rec_resort.bytes));
+        }
+        CK(cudaMemset(s->rec_resort.p, 0, 2 * sizeof(uint32_t)));
+    } else {
+        s->rec_keys.release();
+    }
     s->tape_slots = slots;
     s->tape_sets = sets;
+    s->tape_rec = rec;
     return PGMPM_OK;
 }
 
-// Buffers of slot j of tape set t: the step from state j to state j+1.
-// States (and keys) of set t are t (slots + 1) + j; the per-step data of
-// slot j is slot t slots + j.
-StepBufs tape_bufs(pgmpm_solver s, int j, int t = 0) {
+// Points the sort outputs and counters of b at per-step slot js.
+void set_sort_slot(pgmpm_solver s, StepBufs& b, size_t js) {
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
-    const size_t nodes = nodes_of(s);
-    const size_t qs = (size_t)t * (s->tape_slots + 1) + j;  // state j of set t
-    j += t * s->tape_slots;                                  // per-step slot of set t
-    StepBufs b;
-    b.q = s->tape_q.as<float4>() + 6 * N * qs;
-    b.q_out = s->tape_q.as<float4>() + 6 * N * (qs + 1);
-    b.pay = s->pf.physics == PHYS_MLS ? s->tape_pay.as<float4>() : nullptr;
-    b.keys_in = s->tape_keys.as<uint32_t>() + N * qs;
-    b.keys_out = s->tape_keys.as<uint32_t>() + N * (qs + 1);
-    uint32_t* sk = s->tape_sk.as<uint32_t>() + N * j;
-    uint32_t* so = s->tape_ord.as<uint32_t>() + N * j;
+    uint32_t* sk = s->tape_sk.as<uint32_t>() + N * js;
+    uint32_t* so = s->tape_ord.as<uint32_t>() + N * js;
     // the sort's last pass must land in the slot: pair a when which == 0
     b.which = s->sort_which;
     if (b.which == 0) {
@@ -94,27 +111,63 @@ StepBufs tape_bufs(pgmpm_solver s, int j, int t = 0) {
         b.kb = sk;
         b.vb = so;
     }
-    b.grid_v = s->tape_gv.as<float4>() + nodes * j;
-    b.grid_vpre = s->tape_gvpre.as<float4>() + nodes * j;
-    b.tile_flags = s->tape_flags.as<uint32_t>() + (size_t)s->total_nt * j;
-    b.tile_list = s->tape_tiles.as<uint32_t>() + (size_t)s->total_nt * j;
-    b.ctile_list = s->tape_ctiles.as<uint32_t>() + (size_t)s->total_ct * j;
-    b.ctile_range = s->tape_crange.as<uint2>() + (size_t)s->total_ct * j;
+    b.tile_flags = s->tape_flags.as<uint32_t>() + (size_t)s->total_nt * js;
+    b.tile_list = s->tape_tiles.as<uint32_t>() + (size_t)s->total_nt * js;
+    b.ctile_list = s->tape_ctiles.as<uint32_t>() + (size_t)s->total_ct * js;
+    b.ctile_range = s->tape_crange.as<uint2>() + (size_t)s->total_ct * js;
     const size_t ct = std::max<size_t>((size_t)s->total_ct, 1);
-    b.cell_range = s->tape_cells.p ? s->tape_cells.as<uint2>() + ct * 64 * j : nullptr;
-    b.ptile_list = s->tape_ptile.p ? s->tape_ptile.as<uint32_t>() + ct * j : nullptr;
-    b.counters = s->tape_counters.as<uint32_t>() + CNT_WORDS * j;
+    b.cell_range = s->tape_cells.p ? s->tape_cells.as<uint2>() + ct * 64 * js : nullptr;
+    b.ptile_list = s->tape_ptile.p ? s->tape_ptile.as<uint32_t>() + ct * js : nullptr;
+    b.counters = s->tape_counters.as<uint32_t>() + CNT_WORDS * js;
+}
+
+// Buffers of slot j of tape set t: the step from state j to state j+1.
+// States of set t are t (slots + 1) + j; grid data of slot j is slot
+// t slots + j.  Without a record (g < 0) the sort outputs and keys are the
+// slot's too; with one, they are those of forward step g (keys g and g + 1).
+StepBufs tape_bufs(pgmpm_solver s, int j, int t = 0, int g = -1) {
+    const size_t N = (size_t)std::max<int64_t>(s->N, 1);
+    const size_t nodes = nodes_of(s);
+    const size_t qs = (size_t)t * (s->tape_slots + 1) + j;  // state j of set t
+    const size_t jg = (size_t)t * s->tape_slots + j;        // grid slot of set t
+    StepBufs b;
+    b.q = s->tape_q.as<float4>() + 6 * N * qs;
+    b.q_out = s->tape_q.as<float4>() + 6 * N * (qs + 1);
+    b.pay = s->pf.physics == PHYS_MLS ? s->tape_pay.as<float4>() : nullptr;
+    if (g >= 0) {
+        b.keys_in = s->rec_keys.as<uint32_t>() + N * (size_t)g;
+        b.keys_out = s->rec_keys.as<uint32_t>() + N * ((size_t)g + 1);
+    } else {
+        b.keys_in = s->tape_keys.as<uint32_t>() + N * qs;
+        b.keys_out = s->tape_keys.as<uint32_t>() + N * (qs + 1);
+    }
+    set_sort_slot(s, b, g >= 0 ? (size_t)g : jg);
+    b.grid_v = s->tape_gv.as<float4>() + nodes * jg;
+    b.grid_vpre = s->tape_gvpre.as<float4>() + nodes * jg;
     return b;
 }
 
 // Runs body(stream) under capture on the solver's capture stream and keeps
-// the instantiated graph in tape_exec[kind] (tagged with len).
+// the instantiated graph: in tape_exec[kind] (tagged with len) when base < 0,
+// else in seg_exec under (kind, len, base).  ex receives the graph.
 template <class Body>
-int tape_graph(pgmpm_solver s, int kind, int len, Body&& body) {
-    if (s->tape_exec[kind] && s->tape_exec_len[kind] == len) return PGMPM_OK;
-    if (s->tape_exec[kind]) cudaGraphExecDestroy(s->tape_exec[kind]);
-    s->tape_exec[kind] = nullptr;
-    s->tape_exec_len[kind] = -1;
+int tape_graph(pgmpm_solver s, int kind, int len, int base, cudaGraphExec_t& ex, Body&& body) {
+    cudaGraphExec_t* slot;
+    if (base >= 0 && s->seg_exec.size() >= 4096) s->drop_tape_graphs();  // bound the per-segment cache
+    if (base < 0) {
+        if (s->tape_exec[kind] && s->tape_exec_len[kind] != len) {
+            cudaGraphExecDestroy(s->tape_exec[kind]);
+            s->tape_exec[kind] = nullptr;
+            s->tape_exec_len[kind] = -1;
+        }
+        slot = &s->tape_exec[kind];
+    } else {
+        slot = &s->seg_exec[std::make_tuple(kind, len, base)];
+    }
+    if (*slot) {
+        ex = *slot;
+        return PGMPM_OK;
+    }
     CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
     int rc = body(s->cap_stream);
     cudaGraph_t g = nullptr;
@@ -124,10 +177,11 @@ int tape_graph(pgmpm_solver s, int kind, int len, Body&& body) {
         return rc;
     }
     CK(e);
-    e = cudaGraphInstantiate(&s->tape_exec[kind], g, 0);
+    e = cudaGraphInstantiate(slot, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    s->tape_exec_len[kind] = len;
+    if (base < 0) s->tape_exec_len[kind] = len;
+    ex = *slot;
     return PGMPM_OK;
 }
 
@@ -135,28 +189,63 @@ int tape_graph(pgmpm_solver s, int kind, int len, Body&& body) {
 // grid_mp clear).  With the fused kernel each slot's G2P2G does the next
 // slot's P2G; the last slot runs the split G2P, so nothing is left pending
 // in grid_mp and the payload buffer holds the final state's payload.
-int record_tape_forward(pgmpm_solver s, int len, cudaStream_t st, int t = 0) {
+// g0 >= 0: the slots are forward steps g0.. of the record; replay: they were
+// recorded already, so each step keeps its recorded sort (the first always,
+// the others unless the previous step's G2P changed a key).
+int record_tape_forward(pgmpm_solver s, int len, cudaStream_t st, int t = 0, int g0 = -1, bool replay = false) {
     for (int j = 0; j < len; ++j) {
-        int rc = record_step(s, tape_bufs(s, j, t), st, false, true, step_kind(s, j, len, false, true));
+        StepBufs b = tape_bufs(s, j, t, g0 < 0 ? -1 : g0 + j);
+        if (replay && g0 >= 0) {
+            b.resort = s->rec_resort.as<uint32_t>() + t;
+            b.sort_mode = j == 0 ? 1 : 2;
+        }
+        int rc = record_step(s, b, st, false, true, step_kind(s, j, len, false, true));
         if (rc) return rc;
     }
     return PGMPM_OK;
 }
 
 // Reverse kernels of slots len-1 .. 0 of tape set t.
-int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t st, int t = 0) {
+int record_tape_reverse(pgmpm_solver s, const AdjView& A0, int len, cudaStream_t st, int t = 0, int g0 = -1) {
     AdjView A = A0;
     for (int j = len - 1; j >= 0; --j) {
-        StepBufs b = tape_bufs(s, j, t);
+        StepBufs b = tape_bufs(s, j, t, g0 < 0 ? -1 : g0 + j);
         View V = s->view_for(b);
         V.grid_mp = A.grid_gv;  // scatter target of the G2P reverse
         A.q_next = b.q_out;
         // the slot's P2G work cursor is zero: the grid update of the slot's
-        // forward step cleared it after P2G
+        // forward step cleared it after P2G (and a previous reverse's grid
+        // adjoint after its scatter)
         CK(launch_adj_scatter(V, A, s->pf, s->tune, s->num_sms, st));
         CK(launch_adj_grid(V, A, s->tune, s->num_sms, st));
         CK(launch_adj_gather(V, A, s->pf, s->tune, st));
     }
+    return PGMPM_OK;
+}
+
+// Steps g0 .. g0 + len - 1 of a recorded forward on the live state: each
+// step's sort writes its slot of the record and its G2P the next state's
+// keys; the segment's last step stores v and C (the checkpoint that follows
+// copies the whole state).
+int run_recorded(pgmpm_solver s, int g0, int len, cudaStream_t st) {
+    cudaGraphExec_t ex = nullptr;
+    int rc = tape_graph(s, 7, len, g0, ex, [&](cudaStream_t c) -> int {
+        for (int j = 0; j < len; ++j) {
+            StepBufs b = s->live_bufs();
+            const size_t N = (size_t)std::max<int64_t>(s->N, 1);
+            b.keys_in = s->rec_keys.as<uint32_t>() + N * (size_t)(g0 + j);
+            b.keys_out = s->rec_keys.as<uint32_t>() + N * (size_t)(g0 + j + 1);
+            set_sort_slot(s, b, (size_t)(g0 + j));
+            int r = record_step(s, b, c, false, j + 1 == len, STEP_SPLIT);
+            if (r) return r;
+        }
+        CK(launch_merge_flags(s->tape_counters.as<uint32_t>() + (size_t)CNT_WORDS * g0, len,
+                              s->counters.as<uint32_t>(), c));
+        return PGMPM_OK;
+    });
+    if (rc) return rc;
+    CK(cudaGraphLaunch(ex, st));
+    s->met.total_steps += len;
     return PGMPM_OK;
 }
 
@@ -174,26 +263,41 @@ int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
     if (!s->ev_join) CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     cudaStream_t side = s->side_stream;
     auto seg_len = [&](int seg) { return std::min(k, s->ck_steps - seg * k); };
+    // with a recorded forward, segment seg's steps are forward steps
+    // seg k .. and keep their recorded sorts (graphs per segment).  Kernel
+    // variants changed to the fused step since the forward: replay every
+    // segment with its own sorts (the tape's segments hold the record's).
+    const bool rec = s->ck_rec && !s->fused();
+    if (s->ck_rec && !rec) {
+        s->tape_has_last = false;
+        s->tape_has_prev = false;
+    }
     auto replay = [&](int seg, int t, cudaStream_t cs) -> int {
         const int len = seg_len(seg);
-        const StepBufs b0 = tape_bufs(s, 0, t);
+        const int g0 = rec ? seg * k : -1;
+        const StepBufs b0 = tape_bufs(s, 0, t, g0);
         CK(cudaMemcpyAsync(b0.q, s->ck_q.as<float4>() + 6 * Nz * seg, sizeof(float4) * 6 * Nz,
                            cudaMemcpyDeviceToDevice, cs));
         CK(cudaMemcpyAsync(b0.keys_in, s->ck_keys.as<uint32_t>() + Nz * seg, sizeof(uint32_t) * Nz,
                            cudaMemcpyDeviceToDevice, cs));
-        int rc = tape_graph(s, 4 + t, len, [&](cudaStream_t c) -> int {
+        cudaGraphExec_t ex = nullptr;
+        int rc = tape_graph(s, 4 + t, len, g0, ex, [&](cudaStream_t c) -> int {
+            if (rec) CK(cudaMemsetAsync(s->rec_resort.as<uint32_t>() + t, 0, sizeof(uint32_t), c));
             CK(launch_payload(s->view_for(b0), s->pf, c));
-            return record_tape_forward(s, len, c, t);
+            return record_tape_forward(s, len, c, t, g0, true);
         });
         if (rc) return rc;
-        CK(cudaGraphLaunch(s->tape_exec[4 + t], cs));
+        CK(cudaGraphLaunch(ex, cs));
         return PGMPM_OK;
     };
     auto reverse = [&](int seg, int t, cudaStream_t cs) -> int {
         const int len = seg_len(seg);
-        int rc = tape_graph(s, 2 + t, len, [&](cudaStream_t c) { return record_tape_reverse(s, A, len, c, t); });
+        const int g0 = rec ? seg * k : -1;
+        cudaGraphExec_t ex = nullptr;
+        int rc = tape_graph(s, 2 + t, len, g0, ex,
+                            [&](cudaStream_t c) { return record_tape_reverse(s, A, len, c, t, g0); });
         if (rc) return rc;
-        CK(cudaGraphLaunch(s->tape_exec[2 + t], cs));
+        CK(cudaGraphLaunch(ex, cs));
         return PGMPM_OK;
     };
     const int last = s->ck_count - 1;
@@ -247,9 +351,31 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     const size_t N = (size_t)std::max<int64_t>(s->N, 1);
     CK(s->ck_q.ensure(sizeof(float4) * 6 * N * nseg));
     CK(s->ck_keys.ensure(sizeof(uint32_t) * N * nseg));
-    int rc = ensure_tape(s, k);
+    // Record the forward (every step's sort and keys) when the steps are
+    // split bin-sorted steps and the tape with the record is modest: at most
+    // 1/16 of the device's memory, with a quarter of it still free after it
+    // (other solvers of the process keep room for their tapes).  The
+    // backward's replays then keep the forward's sorts.  Otherwise (or when
+    // its allocation fails) the tape is the plain one and the replays sort.
+    int rec = 0;
+    if (s->rec_mode && s->tune.step_sort == 0 && s->bs_ccount.p && !s->fused() && s->N > 0) {
+        size_t fr = 0, tot = 0;
+        const size_t tape = (size_t)2 * (k + 1) * N * (96 + 4) + 64 * N + (size_t)2 * k * nodes_of(s) * 32;
+        const size_t need = tape + rec_step_bytes(s) * (size_t)n_steps;
+        if (s->tape_rec >= n_steps && s->tape_slots >= k)
+            rec = n_steps;
+        else if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need <= tot / 16 && fr >= need + tot / 4)
+            rec = n_steps;
+    }
+    int rc = ensure_tape(s, k, rec);
+    if (rc == PGMPM_ERR_OOM && rec) {
+        cudaGetLastError();  // clear the failed allocation
+        rec = 0;
+        rc = ensure_tape(s, k, 0);
+    }
     if (rc) return rc;
     s->ck_valid = false;
+    s->ck_rec = false;
     s->tape_has_last = false;
     s->tape_has_prev = false;
     rc = unprime(s, st);  // checkpoints and replays start from the state alone
@@ -257,18 +383,22 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     // Runs a segment in the slots of tape set t, so that the backward does
     // not replay it, then hands the final state back to the live buffers
     // (the tape starts from the state and its payload, with grid_mp clear).
-    auto run_in_tape = [&](int len, int t) -> int {
+    // g0 >= 0: the recorded forward's steps g0 .. (the record's keys g0 are
+    // the state's already)
+    auto run_in_tape = [&](int len, int t, int g0) -> int {
         int r = unprime(s, st);
         if (r) return r;
-        const StepBufs first = tape_bufs(s, 0, t);
+        const StepBufs first = tape_bufs(s, 0, t, g0);
         CK(cudaMemcpyAsync(first.q, s->q.p, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(first.keys_in, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
+        if (g0 < 0)
+            CK(cudaMemcpyAsync(first.keys_in, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_pay.p, s->pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
         const int kind = t == 0 ? 1 : 6;
-        r = tape_graph(s, kind, len, [&](cudaStream_t cs) { return record_tape_forward(s, len, cs, t); });
+        cudaGraphExec_t ex = nullptr;
+        r = tape_graph(s, kind, len, g0, ex, [&](cudaStream_t cs) { return record_tape_forward(s, len, cs, t, g0); });
         if (r) return r;
-        CK(cudaGraphLaunch(s->tape_exec[kind], st));
-        const StepBufs last = tape_bufs(s, len - 1, t);
+        CK(cudaGraphLaunch(ex, st));
+        const StepBufs last = tape_bufs(s, len - 1, t, g0);
         CK(cudaMemcpyAsync(s->q.p, last.q_out, sizeof(float4) * 6 * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->keys.p, last.keys_out, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->pay.p, s->tape_pay.p, sizeof(float4) * 4 * N, cudaMemcpyDeviceToDevice, st));
@@ -278,27 +408,31 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->counters.as<uint32_t>() + CNT_ACTIVE, last.counters + CNT_ACTIVE, 2 * sizeof(uint32_t),
                            cudaMemcpyDeviceToDevice, st));
-        CK(launch_merge_flags(s->tape_counters.as<uint32_t>() + (size_t)CNT_WORDS * s->tape_slots * t, len,
-                              s->counters.as<uint32_t>(), st));
+        CK(launch_merge_flags(s->tape_counters.as<uint32_t>() + (size_t)CNT_WORDS * (g0 >= 0 ? g0 : s->tape_slots * t),
+                              len, s->counters.as<uint32_t>(), st));
         s->met.total_steps += len;
         return PGMPM_OK;
     };
     // with two tape sets (the overlapped backward) the second-to-last
     // segment runs in set 1 as well, so the backward replays one segment less
     const bool prev_in_tape = s->tape_sets == 2 && s->tune.step_sort == 0 && nseg >= 2;
+    // recorded: the live keys stay as they are until the last segment; the
+    // steps read and write the record's
+    uint32_t* rk = rec ? s->rec_keys.as<uint32_t>() : nullptr;
+    if (rec) CK(cudaMemcpyAsync(rk, s->keys.p, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
     for (int seg = 0; seg < nseg; ++seg) {
         CK(cudaMemcpyAsync(s->ck_q.as<float4>() + 6 * N * seg, s->q.p, sizeof(float4) * 6 * N,
                            cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(s->ck_keys.as<uint32_t>() + N * seg, s->keys.p, sizeof(uint32_t) * N,
-                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(s->ck_keys.as<uint32_t>() + N * seg, rec ? rk + N * (size_t)seg * k : s->keys.as<uint32_t>(),
+                           sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, st));
         const int len = std::min(k, n_steps - seg * k);
         if (s->N == 0 || seg + 2 < nseg || (seg + 2 == nseg && !prev_in_tape)) {
-            rc = run_steps(s, len, st);
+            rc = rec ? run_recorded(s, seg * k, len, st) : run_steps(s, len, st);
             if (rc) return rc;
             continue;
         }
         const int t = seg + 1 == nseg ? 0 : 1;
-        rc = run_in_tape(len, t);
+        rc = run_in_tape(len, t, rec ? seg * k : -1);
         if (rc) return rc;
         if (t == 0)
             s->tape_has_last = true;
@@ -309,6 +443,7 @@ int pgmpm_forward_checkpointed(pgmpm_solver s, int32_t n_steps, int32_t checkpoi
     s->ck_every = k;
     s->ck_count = nseg;
     s->ck_valid = true;
+    s->ck_rec = rec > 0;
     return PGMPM_OK;
 }
 
@@ -366,9 +501,10 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
         const int len = std::min(k, s->ck_steps - seg * k);
         if (seg == s->ck_count - 1 && s->tape_has_last) {
             // the forward left this segment in the tape
-            rc = tape_graph(s, 2, len, [&](cudaStream_t cs) { return record_tape_reverse(s, A, len, cs); });
+            cudaGraphExec_t ex = nullptr;
+            rc = tape_graph(s, 2, len, -1, ex, [&](cudaStream_t cs) { return record_tape_reverse(s, A, len, cs); });
             if (rc) return rc;
-            CK(cudaGraphLaunch(s->tape_exec[2], st));
+            CK(cudaGraphLaunch(ex, st));
             s->tape_has_last = false;  // the replays below overwrite it
             continue;
         }
@@ -377,17 +513,18 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(s->tape_keys.p, s->ck_keys.as<uint32_t>() + Nz * seg, sizeof(uint32_t) * Nz,
                            cudaMemcpyDeviceToDevice, st));
-        rc = tape_graph(s, 0, len, [&](cudaStream_t cs) -> int {
+        cudaGraphExec_t ex = nullptr;
+        rc = tape_graph(s, 0, len, -1, ex, [&](cudaStream_t cs) -> int {
             CK(launch_payload(s->view_for(tape_bufs(s, 0)), s->pf, cs));
             int r = record_tape_forward(s, len, cs);
             if (r) return r;
             return record_tape_reverse(s, A, len, cs);
         });
         if (rc) return rc;
-        CK(cudaGraphLaunch(s->tape_exec[0], st));
+        CK(cudaGraphLaunch(ex, st));
     }
-    CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), s->tape_slots * s->tape_sets, s->counters.as<uint32_t>(),
-                          st));
+    CK(launch_merge_flags(s->tape_counters.as<uint32_t>(), std::max(s->tape_slots * s->tape_sets, s->tape_rec),
+                          s->counters.as<uint32_t>(), st));
     // physical planes -> caller's arrays (upload order)
     if (ptr_kind == PGMPM_PTR_DEVICE) {
         CK(launch_planes_to_state(A.g, s->phys_of_user.as<uint32_t>(), gx_in, gv_in, gC_in, gF_in, N, st));

@@ -43,6 +43,9 @@ struct View {
     const float2* mV;          // (mass, V0)
     const int32_t* mat;        // material id (null when M == 1)
     uint32_t* keys;            // cell key per particle (physical order), input of the next sort
+    uint32_t* resort;          // MLS G2P replaying recorded steps: V.keys holds the recorded next
+                               // keys; G2P overwrites only those that differ and then sets *resort
+                               // (the next step must sort again).  Null: G2P writes every key.
     const uint32_t* skeys;     // sorted keys
     const uint32_t* order;     // sorted position -> physical particle
     float4* grid_mp;           // (m, p) accumulator

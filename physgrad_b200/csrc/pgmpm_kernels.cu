@@ -1459,7 +1459,11 @@ __device__ __forceinline__ void mls_advance(const View& V, const SceneDev& sc, i
 // SPARSE (MLS, physical order, live solver only): the grid is the slot pool
 // of V.sp; the particle's tile is the slot of the key it was sorted by (read
 // before the new key overwrites it).
-template <int PHYS, bool MULTI, bool FLUID, bool PLASTIC, class Fetch, bool SPARSE = false>
+// CHECK (MLS, dense, replaying recorded steps): V.keys holds the keys the
+// forward recorded for the next step; a new key that differs replaces it and
+// sets *V.resort, so that the next step sorts again instead of keeping the
+// recorded sort.
+template <int PHYS, bool MULTI, bool FLUID, bool PLASTIC, class Fetch, bool SPARSE = false, bool CHECK = false>
 __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, uint32_t p, const Fetch& fetch,
                                              uint32_t& flags) {
     const int64_t N = V.N;
@@ -1550,6 +1554,12 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
                                       : sp_find_or_insert(V.sp, sp_code(tx, ty, tz), flags);
             V.keys[p] = slot == SP_NONE ? SP_NONE
                                         : slot * 64u + (uint32_t)((so[2] & 3) * 16 + (so[1] & 3) * 4 + (so[0] & 3));
+        } else if (CHECK) {
+            const uint32_t nk = cell_key(sc, so);
+            if (V.keys[p] != nk) {  // rare: the replay rounded across a cell face
+                V.keys[p] = nk;
+                atomicOr(V.resort, 1u);
+            }
         } else {
             V.keys[p] = cell_key(sc, so);
         }
@@ -1609,7 +1619,7 @@ __device__ __forceinline__ void g2p_particle(const View& V, const SceneDev& sc, 
 // sorted at upload and particles drift less than a cell per step, so
 // neighbouring threads still share grid nodes, and the state loads are fully
 // coalesced with no dependent load of the order array.
-template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER, bool PLASTIC, bool SPARSE = false>
+template <int PHYS, bool MULTI, bool FLUID, bool PHYS_ORDER, bool PLASTIC, bool SPARSE = false, bool CHECK = false>
 __device__ __forceinline__ void k_g2p_impl(const View& V) {
     const int64_t N = V.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1624,7 +1634,7 @@ __device__ __forceinline__ void k_g2p_impl(const View& V) {
         const SceneDev& sc = scene_ref(V, s);
         const float4* gv = V.grid_v;
         auto fetch = [&](int, int, int, int idx) { return __ldg(&gv[idx]); };
-        g2p_particle<PHYS, MULTI, FLUID, PLASTIC, decltype(fetch), SPARSE>(V, sc, p, fetch, flags);
+        g2p_particle<PHYS, MULTI, FLUID, PLASTIC, decltype(fetch), SPARSE, CHECK>(V, sc, p, fetch, flags);
     }
     if (flags) atomicOr(&V.counters[CNT_FLAGS], flags);
 }
@@ -1643,6 +1653,12 @@ __global__ void __launch_bounds__(512, 2) k_g2p_phys(View V) {
 template <int PHYS, bool MULTI, bool FLUID>
 __global__ void __launch_bounds__(512, 2) k_g2p_phys_vm(View V) {
     k_g2p_impl<PHYS, MULTI, FLUID, true, true>(V);
+}
+// replay of recorded steps (MLS, dense): the new keys are checked against
+// the recorded ones (see g2p_particle's CHECK)
+template <bool MULTI, bool FLUID, bool PLASTIC>
+__global__ void __launch_bounds__(512, 2) k_g2p_check(View V) {
+    k_g2p_impl<PHYS_MLS, MULTI, FLUID, true, PLASTIC, false, true>(V);
 }
 // sparse grids (MLS)
 template <bool MULTI, bool FLUID, bool PLASTIC>
@@ -2351,6 +2367,26 @@ cudaError_t launch_g2p(const View& V, const PhysFlags& pf, const Tuning& t, int 
             }
         }
 #undef PGMPM_G2PS
+        return cudaGetLastError();
+    }
+    if (V.resort) {  // a replay of recorded steps: physical order, keys checked
+        if (pf.physics != PHYS_MLS) return cudaErrorNotSupported;
+        const int nb = grid_for(V.N, t.g2p_block, 1 << 30);
+#define PGMPM_G2PC(M_, F_, P_) k_g2p_check<M_, F_, P_><<<nb, t.g2p_block, 0, st>>>(V)
+        if (pf.multi_mat) {
+            if (pf.has_fluid) {
+                if (pf.has_plastic) PGMPM_G2PC(true, true, true); else PGMPM_G2PC(true, true, false);
+            } else {
+                if (pf.has_plastic) PGMPM_G2PC(true, false, true); else PGMPM_G2PC(true, false, false);
+            }
+        } else {
+            if (pf.has_fluid) {
+                if (pf.has_plastic) PGMPM_G2PC(false, true, true); else PGMPM_G2PC(false, true, false);
+            } else {
+                if (pf.has_plastic) PGMPM_G2PC(false, false, true); else PGMPM_G2PC(false, false, false);
+            }
+        }
+#undef PGMPM_G2PC
         return cudaGetLastError();
     }
     if (t.g2p_variant == 0) {

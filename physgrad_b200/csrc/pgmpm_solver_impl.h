@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/pgmpm.h"
@@ -72,6 +74,13 @@ struct StepBufs {
     uint2* cell_range;     // per-cell ranges written by the bin sort (null: not kept)
     uint32_t* ptile_list;  // occupied tiles largest first, built by the bin sort (null: not kept)
     uint32_t* counters;
+    // Replay of a recorded step (bin sort only): the sort's outputs above are
+    // the forward's, valid while keys_in equals the forward's keys.  The step
+    // runs its sort only when *resort is set (a conditional graph node; the
+    // step must be captured), and its G2P compares the new keys with the
+    // recorded ones in keys_out and sets *resort when one differs.
+    uint32_t* resort = nullptr;
+    int sort_mode = 0;  // 0: sort keys_in; 1: keep the recorded sort; 2: keep it unless *resort
 };
 
 struct DeviceGuard {
@@ -166,7 +175,19 @@ struct pgmpm_solver_s {
     static constexpr int kTapeGraphs = 7;
     cudaGraphExec_t tape_exec[kTapeGraphs] = {};
     int tape_exec_len[kTapeGraphs] = {-1, -1, -1, -1, -1, -1, -1};
+    // Recorded forward (the bin sort, split steps): the per-step sort outputs
+    // of the tape (tape_sk .. tape_ptile) hold one slot per forward step,
+    // rec_keys the keys of every state, so that a replay keeps the forward's
+    // sort.  Its graphs are per segment: (kind, length, first step) -> graph,
+    // kind as tape_exec plus [7], a recorded live segment of the forward.
+    int rec_mode = 1;           // pgmpm_set_sort_record: 0 off, 1 on, 2 on with replays that always sort
+    int tape_rec = 0;           // forward steps the per-step arrays hold (0: slots only)
+    bool ck_rec = false;        // the valid checkpointed forward was recorded
+    pgmpm::DevBuf rec_keys;     // (tape_rec + 1) x N
+    pgmpm::DevBuf rec_resort;   // one flag per tape set (a replayed key changed)
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> seg_exec;
     cudaStream_t side_stream = nullptr;  // the replay that overlaps a segment's reverse
+    cudaStream_t body_stream = nullptr;  // captures the bodies of conditional graph nodes
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     pgmpm::DevBuf adj_g, adj_grid_gv, adj_grid_gpm, adj_gE, adj_stage;
 
@@ -209,6 +230,7 @@ struct pgmpm_solver_s {
         V.mV = mV.as<float2>();
         V.mat = pf.multi_mat ? mat.as<int32_t>() : nullptr;
         V.keys = b.keys_out;
+        V.resort = b.resort;
         V.skeys = b.which ? b.kb : b.ka;
         V.order = b.which ? b.vb : b.va;
         V.grid_mp = grid_mp.as<float4>();
@@ -240,6 +262,9 @@ struct pgmpm_solver_s {
             tape_exec[i] = nullptr;
             tape_exec_len[i] = -1;
         }
+        for (auto& kv : seg_exec)
+            if (kv.second) cudaGraphExecDestroy(kv.second);
+        seg_exec.clear();
     }
 
     void drop_graph() {
@@ -266,6 +291,7 @@ struct pgmpm_solver_s {
         if (cpl_grid) pgmpm_hashgrid_destroy(cpl_grid);
         if (cap_stream) cudaStreamDestroy(cap_stream);
         if (side_stream) cudaStreamDestroy(side_stream);
+        if (body_stream) cudaStreamDestroy(body_stream);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         for (auto& e : ev)

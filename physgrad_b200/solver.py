@@ -298,6 +298,18 @@ class Simulator:
         """C.SORT_BINS (default) or C.SORT_RADIX (stable order within a cell)."""
         check(lib().pgmpm_set_step_sort(self._h, int(kind)))
 
+    def set_sort_record(self, on):
+        """Record every step's sort in forward_checkpointed (default on), so
+        that backward's replays keep it instead of sorting again; 2: record,
+        but every replayed step after a segment's first sorts again."""
+        check(lib().pgmpm_set_sort_record(self._h, int(on)))
+
+    def replay_resorts(self) -> int:
+        """Replayed steps that sorted again because a key changed."""
+        n = ctypes.c_int64(0)
+        check(lib().pgmpm_get_replay_resorts(self._h, ctypes.byref(n)))
+        return int(n.value)
+
     def autotune(self, reps: int = 3, stream=None) -> dict:
         check(lib().pgmpm_autotune(self._h, int(reps), _stream_handle(stream)))
         m = self.metrics()

@@ -69,7 +69,7 @@ int main(void){
 def test_header_compiles_as_c_and_cxx(tmp_path):
     for comp, ext in (("gcc", "c"), ("g++", "cpp")):
         f = tmp_path / f"h.{ext}"
-        f.write_text('#include "pgmpm.h"\nint main(void){ return PGMPM_ABI_VERSION == 3 ? 0 : 1; }\n')
+        f.write_text('#include "pgmpm.h"\nint main(void){ return PGMPM_ABI_VERSION == 5 ? 0 : 1; }\n')
         subprocess.run([comp, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(f), "-o",
                         str(tmp_path / f"h_{ext}")], check=True)
 
@@ -101,7 +101,7 @@ def test_argument_validation_without_gpu(built_lib):
     assert b"scene" in L.pgmpm_last_error()
     assert L.pgmpm_step(None, 1, None) == C.PGMPM_ERR_ARG
     assert L.pgmpm_radix_sort_pairs(None, None, None, None, 10, 8, None) == C.PGMPM_ERR_ARG
-    assert L.pgmpm_abi_version() == 4
+    assert L.pgmpm_abi_version() == 5
     # sparse grids: one MLS scene, at most 4091 nodes per axis (refused before any device work)
     sd = (C.SceneDesc * 2)()
     for d in sd:

@@ -549,3 +549,64 @@ def test_two_rollouts_on_one_simulator_refuse_a_stale_backward(gpu):
     xb = simulate(sim2, x0, vb, E, m, V0, 8, 4)[0]
     (xa.sum() + xb.sum()).backward()
     assert va.grad is not None and vb.grad is not None
+
+
+def _grads(gpu, scenes, counts, mats, st, steps, k, record):
+    """Gradients of a COM-and-velocity loss with the sort recording in mode
+    `record`; with a recording also a second backward over it."""
+    sim = gpu.Simulator(scenes, counts, mats)
+    sim.set_sort_record(record)
+    sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st.get("mat"))
+    sim.forward_checkpointed(steps, k)
+    out = sim.download()
+    N = int(sum(counts))
+    go = {"x": (out["x"] - 0.5).astype(np.float32) / N, "v": (out["v"] / N).astype(np.float32)}
+    g = sim.backward(go)
+    g2 = sim.backward(go) if record else None
+    return g, g2, sim.replay_resorts()
+
+
+def test_recorded_sorts_give_the_gradients_of_sorting_replays(gpu):
+    """With the bin sort, pgmpm_forward_checkpointed records every step's sort
+    and the backward's replays keep it.  The gradients equal those of replays
+    that sort every step (recording off) to FP32 rounding, and a second
+    backward over the same recording gives them again."""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.two_material_drop(n_particles=20000, n=32, seed=31)
+    ga, ga2, _ = _grads(gpu, scenes, counts, mats, st, 40, 8, True)
+    gb, _, _ = _grads(gpu, scenes, counts, mats, st, 40, 8, False)
+    for key in ("x", "v", "C", "F", "E"):
+        a, a2, b = (np.asarray(g[key]).ravel() for g in (ga, ga2, gb))
+        scale = np.abs(b).max()
+        print(f"d/d{key}: recorded vs sorting replays {np.abs(a - b).max() / scale:.2e}, "
+              f"second backward {np.abs(a2 - a).max() / scale:.2e}")
+        assert scale > 0.0, key
+        assert np.abs(a - b).max() <= 1e-4 * scale, key
+        assert np.abs(a2 - a).max() <= 1e-4 * scale, key
+
+
+def test_replayed_steps_that_sort_again_give_the_same_gradients(gpu):
+    """The conditional sort of a replayed step: with the recording in mode 2
+    every replayed step after a segment's first runs it (counted by
+    pgmpm_get_replay_resorts), and the gradients equal those of replays that
+    sort every step.  (In mode 1 a step runs it only after a G2P put a
+    particle in another cell than the forward did, which rounding makes
+    rare.)"""
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.config3(n_particles=65536, steps=64)
+    ga, ga2, resorts = _grads(gpu, scenes, counts, mats, st, 64, 16, 2)
+    gb, _, none = _grads(gpu, scenes, counts, mats, st, 64, 16, 0)
+    # two backwards; each replays 2 of the 4 segments the first time and all
+    # 4 the second (the forward's tape is overwritten), 15 steps each
+    print(f"replayed steps that sorted again: {resorts}")
+    assert none == 0
+    assert resorts == (2 + 4) * 15
+    for key in ("x", "v", "C", "F", "E"):
+        a, a2, b = (np.asarray(g[key]).ravel() for g in (ga, ga2, gb))
+        scale = np.abs(b).max()
+        print(f"d/d{key}: re-sorting replays vs sorting replays {np.abs(a - b).max() / scale:.2e}")
+        assert scale > 0.0, key
+        assert np.abs(a - b).max() <= 1e-4 * scale, key
+        assert np.abs(a2 - b).max() <= 1e-4 * scale, key
