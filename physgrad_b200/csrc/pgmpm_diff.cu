@@ -271,6 +271,7 @@ int backward_overlapped(pgmpm_solver s, const AdjView& A, cudaStream_t st) {
     if (s->ck_rec && !rec) {
         s->tape_has_last = false;
         s->tape_has_prev = false;
+        s->ck_rec = false;
     }
     auto replay = [&](int seg, int t, cudaStream_t cs) -> int {
         const int len = seg_len(seg);
@@ -493,6 +494,14 @@ int pgmpm_backward(pgmpm_solver s, const float* gx_out, const float* gv_out, con
     A.gE = s->adj_gE.as<float>();
     const int k = s->ck_every;
     const bool overlapped = s->tape_sets == 2 && s->tune.step_sort == 0;
+    if (s->ck_rec && !overlapped) {
+        // the step sort changed to the radix sort since a recorded forward:
+        // the tape's segments hold the record's sorts, which the one-set
+        // path does not index, so every segment is replayed with its sorts
+        s->tape_has_last = false;
+        s->tape_has_prev = false;
+        s->ck_rec = false;
+    }
     if (overlapped && N > 0) {
         rc = backward_overlapped(s, A, st);
         if (rc) return rc;

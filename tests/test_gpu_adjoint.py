@@ -551,9 +551,10 @@ def test_two_rollouts_on_one_simulator_refuse_a_stale_backward(gpu):
     assert va.grad is not None and vb.grad is not None
 
 
-def _grads(gpu, scenes, counts, mats, st, steps, k, record):
+def _grads(gpu, scenes, counts, mats, st, steps, k, record, between=None):
     """Gradients of a COM-and-velocity loss with the sort recording in mode
-    `record`; with a recording also a second backward over it."""
+    `record`; with a recording also a second backward over it.  between(sim)
+    runs after the forward."""
     sim = gpu.Simulator(scenes, counts, mats)
     sim.set_sort_record(record)
     sim.upload(st["x"], st["v"], None, None, st["m"], st["V0"], st.get("mat"))
@@ -561,6 +562,8 @@ def _grads(gpu, scenes, counts, mats, st, steps, k, record):
     out = sim.download()
     N = int(sum(counts))
     go = {"x": (out["x"] - 0.5).astype(np.float32) / N, "v": (out["v"] / N).astype(np.float32)}
+    if between is not None:
+        between(sim)
     g = sim.backward(go)
     g2 = sim.backward(go) if record else None
     return g, g2, sim.replay_resorts()
@@ -608,5 +611,28 @@ def test_replayed_steps_that_sort_again_give_the_same_gradients(gpu):
         scale = np.abs(b).max()
         print(f"d/d{key}: re-sorting replays vs sorting replays {np.abs(a - b).max() / scale:.2e}")
         assert scale > 0.0, key
+        assert np.abs(a - b).max() <= 1e-4 * scale, key
+        assert np.abs(a2 - b).max() <= 1e-4 * scale, key
+
+
+@pytest.mark.parametrize("change", ["radix_sort", "fused_kernel"])
+def test_backward_after_a_sort_or_kernel_change_replays_every_segment(gpu, change):
+    """A recorded forward, then the step sort switched to the radix sort or
+    P2G to the fused kernel: the backward cannot keep the recorded sorts
+    (the radix path does not index them, the fused steps sort their own), so
+    it replays every segment, the ones the forward left on the tape too, with
+    their own sorts.  The gradients equal those of an unrecorded run."""
+    from physgrad_b200 import _capi as C
+    from physgrad_b200 import workloads as W
+
+    scenes, counts, mats, st, _ = W.two_material_drop(n_particles=20000, n=32, seed=31)
+    act = {"radix_sort": lambda s: s.set_step_sort(C.SORT_RADIX),
+           "fused_kernel": lambda s: s.set_variants(p2g_variant=5)}[change]
+    ga, ga2, _ = _grads(gpu, scenes, counts, mats, st, 40, 8, 1, between=act)
+    gb, _, _ = _grads(gpu, scenes, counts, mats, st, 40, 8, 0)
+    for key in ("x", "v", "C", "F", "E"):
+        a, a2, b = (np.asarray(g[key]).ravel() for g in (ga, ga2, gb))
+        scale = np.abs(b).max()
+        print(f"{change} d/d{key}: {np.abs(a - b).max() / scale:.2e}, second backward {np.abs(a2 - b).max() / scale:.2e}")
         assert np.abs(a - b).max() <= 1e-4 * scale, key
         assert np.abs(a2 - b).max() <= 1e-4 * scale, key
