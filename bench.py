@@ -509,7 +509,11 @@ def run_adjoint(args, device=0):
             "loss": L, "grad_check": {"direction": "uniform v0_y shift", "fd": fd, "adjoint": ad,
                                       "rel_err": abs(fd - ad) / abs(fd)},
             "dL_dE": float(g["E"][0].item()),
-            "note": "dL/dE of a centre-of-mass loss is ~0: momentum-conserving transfers, no wall contact"}
+            "note": "dL/dE of a centre-of-mass loss is ~0: momentum-conserving transfers, no wall contact",
+            # the forward records every step's sort; a replayed step sorts
+            # again only after a G2P that moved a particle into another cell
+            # than the forward did (counted over all the runs above)
+            "replays": {"sort_record": True, "replayed_steps_sorted_again": sim.replay_resorts()}}
     sim.close()
     return line
 
@@ -666,6 +670,7 @@ def run_targets(args, device=0):
                 "ratio_vs_plain_forward": round(adj["ratio_vs_plain_forward"], 4), "target_ratio": 3.0,
                 "timing": adj["config"]["timing"],
                 "grad_check": adj["grad_check"],
+                "replays": adj["replays"],
                 "forward_adjoint_particle_steps_per_s": adj["value"]},
             "batched_forward_64_scenes": {
                 "n_particles": b4["config"]["n_particles"], "steps": b4["steps"],
