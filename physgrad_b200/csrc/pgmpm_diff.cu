@@ -16,6 +16,13 @@
 // occupancy.  With the radix step sort (whose ping-pong buffers the replay
 // shares) a segment's replay and reverse run in turn.  Each piece is one
 // CUDA graph (captured once per segment length; checkpoint copies outside).
+//
+// Sort record (bin sort, split steps, when it fits): the forward also keeps
+// every step's sort outputs and every state's keys, indexed by forward step,
+// so a replay keeps the forward's sorts.  Its first step always can (the
+// checkpoint is the forward's state bit for bit); a later step sorts again
+// through a conditional graph node only when the previous replayed G2P wrote
+// a key that differs from the recorded one.  These graphs are per segment.
 #include <cuda_runtime.h>
 
 #include <algorithm>
